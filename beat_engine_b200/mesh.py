@@ -1,0 +1,230 @@
+"""Boundary meshes and observation sets for the exterior Burton-Miller path.
+
+Host-side mirror of the reference's mesh handling (paths relative to
+``src/beat_engine/julia_local/``):
+
+* :class:`BoundaryMesh` -- ``BoundaryMesh`` and its constructor
+  (``src/BeatEngineCore.jl:224-232,344-364``): centroids, unit normals
+  ``(v2-v1) x (v3-v1)`` normalised, areas.  Faces are stored 0-based here; the
+  reference is 1-based.
+* :func:`load_gmsh22_with_tags` -- ``src/BeatEngineCore.jl:301-342``.
+* :func:`reference_sphere` -- the icosphere of
+  ``tests/analytical_exterior_tests.jl:4-66`` (outward winding enforced).
+* :func:`oscillating_sphere` -- the octahedron sphere of
+  ``tests/axial_source_tests.jl:71-88``.
+* :func:`fibonacci_sphere` -- ``src/BeatEngineCore.jl:828-840``.
+
+All arrays are numpy; nothing here touches the GPU.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class BoundaryMesh:
+    """Triangle surface mesh with P1 (vertex) and DP0 (face) dofs.
+
+    ``vertices`` is ``V x 3`` float64, ``faces`` ``F x 3`` int32 (0-based),
+    ``physical_tags`` ``F`` int32.  The P1 space has ``V`` dofs numbered like
+    the vertices; the DP0 space has ``F`` dofs numbered like the faces
+    (``build_p1_space`` / ``build_dp0_space``, ``src/BeatEngineCore.jl:445-446``).
+    """
+
+    vertices: np.ndarray
+    faces: np.ndarray
+    physical_tags: np.ndarray
+
+    def __post_init__(self):
+        self.vertices = np.ascontiguousarray(self.vertices, dtype=np.float64).reshape(-1, 3)
+        self.faces = np.ascontiguousarray(self.faces, dtype=np.int32).reshape(-1, 3)
+        if self.physical_tags is None:
+            self.physical_tags = np.ones(len(self.faces), dtype=np.int32)
+        self.physical_tags = np.ascontiguousarray(self.physical_tags, dtype=np.int32).reshape(-1)
+        if len(self.physical_tags) != len(self.faces):
+            raise ValueError("one physical tag per face is required")
+        if len(self.faces) and (self.faces.min() < 0 or self.faces.max() >= len(self.vertices)):
+            raise ValueError("face vertex index out of range")
+        v1 = self.vertices[self.faces[:, 0]]
+        v2 = self.vertices[self.faces[:, 1]]
+        v3 = self.vertices[self.faces[:, 2]]
+        cross = np.cross(v2 - v1, v3 - v1)
+        norm = np.linalg.norm(cross, axis=1)
+        if np.any(norm == 0):
+            raise ValueError("degenerate triangle in mesh")
+        self.centroids = (v1 + v2 + v3) / 3.0
+        self.areas = norm / 2.0
+        self.normals = cross / norm[:, None]
+
+    @property
+    def num_vertices(self) -> int:
+        return int(self.vertices.shape[0])
+
+    @property
+    def num_faces(self) -> int:
+        return int(self.faces.shape[0])
+
+    # P1 / DP0 dof counts, as P1Space.global_dof_count / DP0Space.global_dof_count
+    @property
+    def p1_dofs(self) -> int:
+        return self.num_vertices
+
+    @property
+    def dp0_dofs(self) -> int:
+        return self.num_faces
+
+
+def load_gmsh22_with_tags(path: str, scale: float = 1.0) -> BoundaryMesh:
+    """Read a Gmsh 2.2 ASCII mesh: nodes and triangle (type 2) elements with
+    their physical tag (``src/BeatEngineCore.jl:301-342``)."""
+    with open(path, "r", encoding="utf-8") as fh:
+        lines = [ln.rstrip("\n") for ln in fh]
+    try:
+        ns, ne = lines.index("$Nodes"), lines.index("$EndNodes")
+        es, ee = lines.index("$Elements"), lines.index("$EndElements")
+    except ValueError as exc:
+        raise ValueError("Only Gmsh 2.2 ASCII meshes with Nodes and Elements sections are supported.") from exc
+    index = {}
+    verts = []
+    for ln in lines[ns + 2:ne]:
+        parts = ln.split()
+        if len(parts) < 4:
+            continue
+        index[int(parts[0])] = len(verts)
+        verts.append([float(parts[1]) * scale, float(parts[2]) * scale, float(parts[3]) * scale])
+    faces, tags = [], []
+    for ln in lines[es + 2:ee]:
+        parts = ln.split()
+        if len(parts) < 8 or int(parts[1]) != 2:
+            continue
+        tri = [index.get(int(parts[-3]), -1), index.get(int(parts[-2]), -1), index.get(int(parts[-1]), -1)]
+        if min(tri) < 0:
+            continue
+        faces.append(tri)
+        tags.append(int(parts[3]))
+    return BoundaryMesh(np.array(verts), np.array(faces), np.array(tags))
+
+
+def write_gmsh22(path: str, mesh: BoundaryMesh) -> None:
+    """Write a Gmsh 2.2 ASCII file that :func:`load_gmsh22_with_tags` (and the
+    reference's loader) reads back, so generated meshes feed either path."""
+    with open(path, "w", encoding="utf-8") as fh:
+        fh.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n")
+        fh.write(f"{mesh.num_vertices}\n")
+        for i, v in enumerate(mesh.vertices):
+            fh.write(f"{i + 1} {v[0]:.17e} {v[1]:.17e} {v[2]:.17e}\n")
+        fh.write("$EndNodes\n$Elements\n")
+        fh.write(f"{mesh.num_faces}\n")
+        for i, (f, t) in enumerate(zip(mesh.faces, mesh.physical_tags)):
+            fh.write(f"{i + 1} 2 2 {int(t)} {int(t)} {f[0] + 1} {f[1] + 1} {f[2] + 1}\n")
+        fh.write("$EndElements\n")
+
+
+_ICO_FACES = np.array([
+    (1, 12, 6), (1, 6, 2), (1, 2, 8), (1, 8, 11), (1, 11, 12),
+    (2, 6, 10), (6, 12, 5), (12, 11, 3), (11, 8, 7), (8, 2, 9),
+    (4, 10, 5), (4, 5, 3), (4, 3, 7), (4, 7, 9), (4, 9, 10),
+    (5, 10, 6), (3, 5, 12), (7, 3, 11), (9, 7, 8), (10, 9, 2),
+], dtype=np.int64) - 1
+
+
+def reference_sphere(radius: float, subdivisions: int, centre=(0.0, 0.0, 0.0), tag: int = 1) -> BoundaryMesh:
+    """Icosphere: unit icosahedron, midpoint subdivision ``subdivisions``
+    times, vertices projected to ``radius`` about ``centre``, every winding
+    oriented outward (``tests/analytical_exterior_tests.jl:4-66``).
+
+    ``subdivisions=3`` gives 1,280 faces / 642 vertices; ``5`` gives
+    20,480 faces / 10,242 vertices.
+    """
+    if subdivisions < 0:
+        raise ValueError("Icosphere subdivision level must be >= 0.")
+    phi = (1.0 + math.sqrt(5.0)) / 2.0
+    verts = [np.array(v, dtype=np.float64) for v in (
+        (-1, phi, 0), (1, phi, 0), (-1, -phi, 0), (1, -phi, 0),
+        (0, -1, phi), (0, 1, phi), (0, -1, -phi), (0, 1, -phi),
+        (phi, 0, -1), (phi, 0, 1), (-phi, 0, -1), (-phi, 0, 1))]
+    faces = [tuple(int(x) for x in f) for f in _ICO_FACES]
+    for _ in range(subdivisions):
+        mids: dict = {}
+
+        def midpoint(a: int, b: int) -> int:
+            key = (a, b) if a < b else (b, a)
+            idx = mids.get(key)
+            if idx is not None:
+                return idx
+            verts.append((verts[a] + verts[b]) / 2.0)
+            mids[key] = len(verts) - 1
+            return len(verts) - 1
+
+        nxt = []
+        for a, b, c in faces:
+            ab, bc, ca = midpoint(a, b), midpoint(b, c), midpoint(c, a)
+            nxt.extend([(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)])
+        faces = nxt
+    centre = np.asarray(centre, dtype=np.float64)
+    V = np.array(verts)
+    V = centre + radius * (V / np.linalg.norm(V, axis=1)[:, None])
+    Fa = np.array(faces, dtype=np.int64)
+    v1, v2, v3 = V[Fa[:, 0]], V[Fa[:, 1]], V[Fa[:, 2]]
+    outward = (v1 + v2 + v3) / 3.0 - centre
+    flip = np.einsum("ij,ij->i", np.cross(v2 - v1, v3 - v1), outward) < 0
+    Fa[flip] = Fa[flip][:, [0, 2, 1]]
+    mesh = BoundaryMesh(V, Fa, np.full(len(Fa), tag))
+    if np.any(np.einsum("ij,ij->i", mesh.normals, mesh.centroids - centre) <= 0):
+        raise RuntimeError("icosphere has an inward normal")
+    return mesh
+
+
+def oscillating_sphere(refinements: int, radius: float, tag: int = 2) -> BoundaryMesh:
+    """Octahedron refined by normalised midpoints ``refinements`` times
+    (``tests/axial_source_tests.jl:71-88``): 128 faces at 2, 512 at 3."""
+    verts = [np.array(v, dtype=np.float64) for v in
+             ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1))]
+    faces = [(0, 2, 4), (2, 1, 4), (1, 3, 4), (3, 0, 4), (2, 0, 5), (1, 2, 5), (3, 1, 5), (0, 3, 5)]
+    for _ in range(refinements):
+        mids: dict = {}
+
+        def midpoint(a: int, b: int) -> int:
+            key = (min(a, b), max(a, b))
+            if key not in mids:
+                v = verts[a] + verts[b]
+                verts.append(v / np.linalg.norm(v))
+                mids[key] = len(verts) - 1
+            return mids[key]
+
+        ref = []
+        for a, b, c in faces:
+            ab, bc, ca = midpoint(a, b), midpoint(b, c), midpoint(c, a)
+            ref.extend([(a, ab, ca), (ab, b, bc), (ca, bc, c), (ab, bc, ca)])
+        faces = ref
+    return BoundaryMesh(radius * np.array(verts), np.array(faces), np.full(len(faces), tag))
+
+
+def fibonacci_sphere(n_points: int, radius: float) -> np.ndarray:
+    """``fibonacci_sphere`` of ``src/BeatEngineCore.jl:828-840`` (``n x 3``)."""
+    golden = math.pi * (3.0 - math.sqrt(5.0))
+    i = np.arange(n_points, dtype=np.float64)
+    z = 1.0 - (2.0 * i + 1.0) / n_points
+    r = np.sqrt(1.0 - z * z)
+    phi = i * golden
+    return np.stack([r * np.cos(phi) * radius, r * np.sin(phi) * radius, z * radius], axis=1)
+
+
+def arc_points(n: int, radius: float) -> np.ndarray:
+    """``n`` points on a meridian arc of ``radius``, theta from 0 to 180 deg
+    (x-z plane)."""
+    th = np.linspace(0.0, math.pi, n)
+    return np.stack([radius * np.sin(th), np.zeros(n), radius * np.cos(th)], axis=1)
+
+
+def equator_meridian_directions(n_equator: int = 360, n_meridian: int = 181) -> np.ndarray:
+    """Unit far-field directions: ``n_equator`` on the equator (1 deg steps for
+    360) followed by ``n_meridian`` on the x-z meridian, theta 0..180 deg."""
+    ph = np.arange(n_equator) * (2.0 * math.pi / n_equator)
+    eq = np.stack([np.cos(ph), np.sin(ph), np.zeros(n_equator)], axis=1)
+    th = np.linspace(0.0, math.pi, n_meridian)
+    me = np.stack([np.sin(th), np.zeros(n_meridian), np.cos(th)], axis=1)
+    return np.concatenate([eq, me], axis=0)
