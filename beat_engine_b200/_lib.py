@@ -1,0 +1,224 @@
+"""ctypes binding of libbeatb200.so (C ABI in include/beat_b200.h).
+
+The library is built in-tree (``beat_engine_b200/libbeatb200.so``).  Loading
+fails loudly when it is missing: there is no CPU fallback for the solver.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbeatb200.so")
+
+OK, INVALID_ARG, OOM, CUDA_ERROR, NOT_CONVERGED, TIMEOUT, NO_DEVICE, STATE, SINGULAR = range(9)
+FP64, MIXED_FP32_IR = 0, 1
+STATUS_NAMES = {OK: "OK", INVALID_ARG: "INVALID_ARG", OOM: "OOM", CUDA_ERROR: "CUDA_ERROR",
+                NOT_CONVERGED: "NOT_CONVERGED", TIMEOUT: "TIMEOUT", NO_DEVICE: "NO_DEVICE", STATE: "STATE",
+                SINGULAR: "SINGULAR"}
+
+# every symbol include/beat_b200.h declares
+EXPORTS = (
+    "beat_b200_abi_version", "beat_b200_default_opts", "beat_b200_create", "beat_b200_destroy",
+    "beat_b200_last_error", "beat_b200_set_mesh", "beat_b200_solve", "beat_b200_solve_device",
+    "beat_b200_field", "beat_b200_farfield", "beat_b200_farfield_device", "beat_b200_assemble",
+    "beat_b200_release_workspace", "beat_b200_device_bytes",
+)
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int32), ("ir_restart", ctypes.c_int32), ("ir_max_iters", ctypes.c_int32),
+                ("lu_split_terms", ctypes.c_int32), ("ir_rtol", ctypes.c_double), ("lu_block", ctypes.c_int32),
+                ("flags", ctypes.c_int32)]
+
+
+class Diag(ctypes.Structure):
+    _fields_ = [("assembly_ms", ctypes.c_double), ("singular_ms", ctypes.c_double), ("lu_ms", ctypes.c_double),
+                ("solve_ms", ctypes.c_double), ("ir_ms", ctypes.c_double), ("field_ms", ctypes.c_double),
+                ("ir_iterations", ctypes.c_int32), ("ir_converged", ctypes.c_int32),
+                ("ir_residual", ctypes.c_double), ("regular_pairs", ctypes.c_int64),
+                ("singular_pairs", ctypes.c_int64), ("precision", ctypes.c_int32), ("lu_block", ctypes.c_int32),
+                ("lu_split_terms", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+
+
+class BeatB200Error(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the shared library and declare its prototypes."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            f"{path} is missing: build it with `python -m beat_engine_b200.build` (nvcc, sm_100a). "
+            "The exterior solver has no CPU fallback.")
+    L = ctypes.CDLL(path)
+    vp, dp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)
+    i32, f64 = ctypes.c_int32, ctypes.c_double
+    L.beat_b200_abi_version.restype = i32
+    L.beat_b200_default_opts.argtypes = [ctypes.POINTER(Opts)]
+    L.beat_b200_default_opts.restype = None
+    L.beat_b200_create.argtypes = [i32, ctypes.POINTER(vp)]
+    L.beat_b200_create.restype = i32
+    L.beat_b200_destroy.argtypes = [vp]
+    L.beat_b200_destroy.restype = i32
+    L.beat_b200_last_error.argtypes = [vp]
+    L.beat_b200_last_error.restype = ctypes.c_char_p
+    L.beat_b200_set_mesh.argtypes = [vp, i32, dp, i32, ip, i32, i32]
+    L.beat_b200_set_mesh.restype = i32
+    L.beat_b200_solve.argtypes = [vp, f64, f64, i32, dp, ctypes.POINTER(Opts), dp, ctypes.POINTER(Diag)]
+    L.beat_b200_solve.restype = i32
+    L.beat_b200_solve_device.argtypes = [vp, f64, f64, i32, vp, ctypes.POINTER(Opts), vp, ctypes.POINTER(Diag)]
+    L.beat_b200_solve_device.restype = i32
+    L.beat_b200_field.argtypes = [vp, f64, i32, dp, i32, dp, dp, dp]
+    L.beat_b200_field.restype = i32
+    L.beat_b200_farfield.argtypes = [vp, f64, i32, dp, i32, dp, dp, dp]
+    L.beat_b200_farfield.restype = i32
+    L.beat_b200_farfield_device.argtypes = [vp, f64, i32, dp, i32, vp, vp, vp]
+    L.beat_b200_farfield_device.restype = i32
+    L.beat_b200_assemble.argtypes = [vp, f64, f64, i32, dp, i32, dp, dp]
+    L.beat_b200_assemble.restype = i32
+    L.beat_b200_release_workspace.argtypes = [vp]
+    L.beat_b200_release_workspace.restype = i32
+    L.beat_b200_device_bytes.argtypes = [vp]
+    L.beat_b200_device_bytes.restype = ctypes.c_int64
+    _lib = L
+    return L
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _c128_f(a, rows: int) -> np.ndarray:
+    """Column-major complex128 view with ``rows`` rows (1-d input -> 1 column)."""
+    a = np.asarray(a, dtype=np.complex128)
+    if a.ndim == 1:
+        a = a[:, None]
+    if a.shape[0] != rows:
+        raise ValueError(f"expected {rows} rows, got {a.shape[0]}")
+    return np.asfortranarray(a)
+
+
+class Context:
+    """One device context per mesh (``beat_b200_create`` .. ``beat_b200_destroy``)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        h = ctypes.c_void_p()
+        st = self.lib.beat_b200_create(device, ctypes.byref(h))
+        if st != OK:
+            raise BeatB200Error(st, "beat_b200_create failed")
+        self.handle = h
+        self.V = self.F = 0
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.beat_b200_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, st: int):
+        if st != OK:
+            raise BeatB200Error(st, self.lib.beat_b200_last_error(self.handle).decode(errors="replace"))
+
+    def set_mesh(self, vertices, faces0, quad_order: int = 4, singular_order: int = 4):
+        v = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 3)
+        f = np.ascontiguousarray(np.asarray(faces0, dtype=np.int32).reshape(-1, 3) + 1, dtype=np.int32)
+        self._check(self.lib.beat_b200_set_mesh(self.handle, v.shape[0], _dp(v), f.shape[0],
+                                                f.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                                quad_order, singular_order))
+        self.V, self.F = v.shape[0], f.shape[0]
+
+    @staticmethod
+    def opts(precision: int = MIXED_FP32_IR, **kw) -> Opts:
+        o = Opts()
+        load().beat_b200_default_opts(ctypes.byref(o))
+        o.precision = precision
+        for k, v in kw.items():
+            setattr(o, k, v)
+        return o
+
+    def solve(self, k_signed: float, eta: float, q, opts: Opts | None = None):
+        qf = _c128_f(q, self.F)
+        R = qf.shape[1]
+        p = np.zeros((self.V, R), dtype=np.complex128, order="F")
+        d = Diag()
+        self._check(self.lib.beat_b200_solve(self.handle, float(k_signed), float(eta), R, _dp(qf),
+                                             ctypes.byref(opts) if opts is not None else None,
+                                             _dp(p), ctypes.byref(d)))
+        return p, d.as_dict()
+
+    def solve_device(self, k_signed: float, eta: float, d_q_ptr: int, R: int, d_p_ptr: int,
+                     opts: Opts | None = None) -> dict:
+        d = Diag()
+        self._check(self.lib.beat_b200_solve_device(self.handle, float(k_signed), float(eta), R,
+                                                    ctypes.c_void_p(d_q_ptr),
+                                                    ctypes.byref(opts) if opts is not None else None,
+                                                    ctypes.c_void_p(d_p_ptr), ctypes.byref(d)))
+        return d.as_dict()
+
+    def assemble(self, k_signed: float, eta: float, q=None, precision: int = FP64, want_matrix: bool = True):
+        if q is None:
+            qf = np.zeros((self.F, 0), dtype=np.complex128, order="F")
+        else:
+            qf = _c128_f(q, self.F)
+        R = qf.shape[1]
+        A = np.zeros((self.V, self.V), dtype=np.complex128, order="F") if want_matrix else None
+        b = np.zeros((self.V, max(R, 1)), dtype=np.complex128, order="F")
+        self._check(self.lib.beat_b200_assemble(self.handle, float(k_signed), float(eta), R,
+                                                _dp(qf) if R else None, precision,
+                                                _dp(A) if A is not None else None,
+                                                _dp(b)))
+        return A, b[:, :R]
+
+    def _eval(self, fn, k_signed, pts, p, q):
+        pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        pf, qf = _c128_f(p, self.V), _c128_f(q, self.F)
+        if pf.shape[1] != qf.shape[1]:
+            raise ValueError("p and q need the same number of columns")
+        out = np.zeros((pts.shape[0], pf.shape[1]), dtype=np.complex128, order="F")
+        self._check(fn(self.handle, float(k_signed), pts.shape[0], _dp(pts), pf.shape[1], _dp(pf),
+                       _dp(qf), _dp(out)))
+        return out
+
+    def field(self, k_signed, points, p, q):
+        return self._eval(self.lib.beat_b200_field, k_signed, points, p, q)
+
+    def farfield(self, k_signed, dirs, p, q):
+        return self._eval(self.lib.beat_b200_farfield, k_signed, dirs, p, q)
+
+    def farfield_device(self, k_signed, dirs, R, d_p_ptr, d_q_ptr, d_out_ptr):
+        dirs = np.ascontiguousarray(dirs, dtype=np.float64).reshape(-1, 3)
+        self._check(self.lib.beat_b200_farfield_device(self.handle, float(k_signed), dirs.shape[0], _dp(dirs), R,
+                                                       ctypes.c_void_p(d_p_ptr), ctypes.c_void_p(d_q_ptr),
+                                                       ctypes.c_void_p(d_out_ptr)))
+
+    def release_workspace(self):
+        self._check(self.lib.beat_b200_release_workspace(self.handle))
+
+    def device_bytes(self) -> int:
+        return int(self.lib.beat_b200_device_bytes(self.handle))

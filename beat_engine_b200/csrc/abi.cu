@@ -1,0 +1,342 @@
+// abi.cu -- the extern "C" entry points of libbeatb200.so (include/beat_b200.h).
+//
+// The solve entry replaces solve_exterior_direct_cuda
+// (BeatEngineCompiledDriver.jl:870-915): assemble the fused Burton-Miller
+// system for all R excitations, factor once, solve every column; the field
+// entries replace evaluate_galerkin_field_cuda (src/BeatEngineCudaField.jl:329-389).
+// Every entry converts exceptions to a status code and keeps the message for
+// beat_b200_last_error; nothing here aborts.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "internal.cuh"
+
+using namespace bb;
+
+namespace {
+
+template <typename F> int32_t guarded(beat_b200_ctx *c, F &&fn) {
+    if (!c) return BEAT_B200_INVALID_ARG;
+    try {
+        BB_CUDA(cudaSetDevice(c->device));
+        fn();
+        c->last_error.clear();
+        return BEAT_B200_OK;
+    } catch (const Error &e) {
+        c->last_error = e.msg;
+        cudaGetLastError();
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        c->last_error = "host allocation failed";
+        return BEAT_B200_OOM;
+    } catch (...) {
+        c->last_error = "unexpected exception";
+        return BEAT_B200_CUDA_ERROR;
+    }
+}
+
+beat_b200_opts resolve_opts(const beat_b200_opts *o) {
+    beat_b200_opts r;
+    beat_b200_default_opts(&r);
+    if (o) r = *o;
+    if (r.ir_restart <= 0) r.ir_restart = 20;
+    if (r.ir_max_iters <= 0) r.ir_max_iters = 200;
+    if (!(r.ir_rtol > 0)) r.ir_rtol = 1e-10;
+    if (r.lu_split_terms != 1 && r.lu_split_terms != 3) r.lu_split_terms = 3;
+    BB_REQUIRE(r.precision == BEAT_B200_FP64 || r.precision == BEAT_B200_MIXED_FP32_IR, BEAT_B200_INVALID_ARG,
+               "unknown precision form");
+    if (r.lu_block <= 0) r.lu_block = r.precision == BEAT_B200_FP64 ? 64 : 128;
+    BB_REQUIRE(r.lu_block == 32 || r.lu_block == 64 || r.lu_block == 128, BEAT_B200_INVALID_ARG,
+               "lu_block must be 32, 64 or 128");
+    return r;
+}
+
+__global__ void f32_to_f64_copy(const float2 *src, double2 *dst, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = make_double2(src[i].x, src[i].y);
+}
+
+// row-major (ld) -> column-major N x N FP64
+template <typename T>
+__global__ void export_matrix_kernel(const Cx<T> *A, int64_t ld, int n, double2 *out) {
+    __shared__ double2 tile[32][33];
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int r = by + i, cc = bx + threadIdx.x;
+        if (r < n && cc < n) {
+            const Cx<T> v = A[(int64_t)r * ld + cc];
+            tile[i][threadIdx.x] = make_double2((double)v.re, (double)v.im);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int cc = bx + i, r = by + threadIdx.x;
+        if (r < n && cc < n) out[(size_t)cc * n + r] = tile[threadIdx.x][i];
+    }
+}
+
+void solve_core(beat_b200_ctx *c, double k, double eta, int R, const double *d_q, const beat_b200_opts &o,
+                double *d_x, beat_b200_diag *diag) {
+    BB_REQUIRE(c->F > 0, BEAT_B200_STATE, "no mesh: call beat_b200_set_mesh first");
+    BB_REQUIRE(R >= 1, BEAT_B200_INVALID_ARG, "R must be >= 1");
+    BB_REQUIRE(std::isfinite(k) && k != 0.0 && std::isfinite(eta), BEAT_B200_INVALID_ARG,
+               "wavenumber must be finite and nonzero");
+    ensure_workspace(c, o.precision, R);
+    Workspace &w = c->ws;
+    const int n = c->V;
+    float ms_asm = 0, ms_sing = 0, ms_lu = 0, ms_solve = 0, ms_ir = 0;
+    assemble(c, k, eta, o.precision, R, d_q, &ms_asm, &ms_sing);
+    if (o.precision != BEAT_B200_FP64)
+        BB_CUDA(cudaMemcpyAsync(w.Aop.p, w.A.p, (size_t)n * w.ld * 8, cudaMemcpyDeviceToDevice, c->stream));
+    BB_CUDA(cudaEventRecord(c->ev[4], c->stream));
+    lu_factor(c, o.precision, o.lu_block, o.lu_split_terms);
+    BB_CUDA(cudaEventRecord(c->ev[5], c->stream));
+    const int st = read_status(c);
+    BB_REQUIRE(!(st & DEV_BARRIER_TIMEOUT), BEAT_B200_TIMEOUT, "LU panel: grid barrier ran out of its wait budget");
+    BB_REQUIRE(!(st & DEV_ZERO_PIVOT), BEAT_B200_SINGULAR, "LU: exact zero pivot (singular system)");
+    IrResult ir{0, 1, 0.0};
+    if (o.precision == BEAT_B200_FP64) {
+        BB_CUDA(cudaMemcpyAsync(d_x, w.b.p, (size_t)n * R * 16, cudaMemcpyDeviceToDevice, c->stream));
+        lu_solve_fp64(c, R, d_x);
+        BB_CUDA(cudaEventRecord(c->ev[6], c->stream));
+        BB_CUDA(cudaEventRecord(c->ev[7], c->stream));
+    } else {
+        lu_precond_fp32(c, R, w.b.as<double>(), d_x);
+        BB_CUDA(cudaEventRecord(c->ev[6], c->stream));
+        ir = gmres_refine(c, R, d_x, w.b.as<double>(), o.ir_restart, o.ir_max_iters, o.ir_rtol);
+        BB_CUDA(cudaEventRecord(c->ev[7], c->stream));
+    }
+    BB_CUDA(cudaEventSynchronize(c->ev[7]));
+    BB_CUDA(cudaEventElapsedTime(&ms_lu, c->ev[4], c->ev[5]));
+    BB_CUDA(cudaEventElapsedTime(&ms_solve, c->ev[5], c->ev[6]));
+    BB_CUDA(cudaEventElapsedTime(&ms_ir, c->ev[6], c->ev[7]));
+    if (diag) {
+        diag->assembly_ms = ms_asm;
+        diag->singular_ms = ms_sing;
+        diag->lu_ms = ms_lu;
+        diag->solve_ms = ms_solve;
+        diag->ir_ms = ms_ir;
+        diag->field_ms = 0;
+        diag->ir_iterations = ir.iterations;
+        diag->ir_converged = ir.converged;
+        diag->ir_residual = ir.residual;
+        diag->regular_pairs = c->regular_pairs;
+        diag->singular_pairs = c->npairs;
+        diag->precision = o.precision;
+        diag->lu_block = o.lu_block;
+        diag->lu_split_terms = o.lu_split_terms;
+        diag->reserved = 0;
+    }
+    BB_REQUIRE(ir.converged || o.precision == BEAT_B200_FP64, BEAT_B200_NOT_CONVERGED,
+               "GMRES refinement missed its tolerance (worst relative residual " + std::to_string(ir.residual) + ")");
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t beat_b200_abi_version(void) { return BEAT_B200_ABI_VERSION; }
+
+void beat_b200_default_opts(beat_b200_opts *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->precision = BEAT_B200_MIXED_FP32_IR;
+    o->ir_restart = 20;
+    o->ir_max_iters = 200;
+    o->lu_split_terms = 3;
+    o->ir_rtol = 1e-10;
+    o->lu_block = 0;
+    o->flags = 0;
+}
+
+int32_t beat_b200_create(int32_t device, beat_b200_ctx **out) {
+    if (!out) return BEAT_B200_INVALID_ARG;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+        cudaGetLastError();
+        return BEAT_B200_NO_DEVICE;
+    }
+    if (device < 0 || device >= count) return BEAT_B200_INVALID_ARG;
+    beat_b200_ctx *c = new (std::nothrow) beat_b200_ctx();
+    if (!c) return BEAT_B200_OOM;
+    c->device = device;
+    const int32_t st = guarded(c, [&] {
+        cudaDeviceProp prop;
+        BB_CUDA(cudaGetDeviceProperties(&prop, device));
+        BB_REQUIRE(prop.major >= 10, BEAT_B200_NO_DEVICE,
+                   std::string("libbeatb200 is built for sm_100a; device is ") + prop.name);
+        c->sm_count = prop.multiProcessorCount;
+        BB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        for (auto &e : c->ev) BB_CUDA(cudaEventCreate(&e));
+        c->status.alloc(256);
+        BB_CUDA(cudaMemset(c->status.p, 0, 256));
+        c->barrier.alloc(sizeof(unsigned) * 4096);
+        BB_CUDA(cudaMemset(c->barrier.p, 0, sizeof(unsigned) * 4096));
+    });
+    if (st != BEAT_B200_OK) {
+        beat_b200_destroy(c);
+        return st;
+    }
+    *out = c;
+    return BEAT_B200_OK;
+}
+
+int32_t beat_b200_destroy(beat_b200_ctx *c) {
+    if (!c) return BEAT_B200_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    release_workspace(c);
+    for (DevBuf *b : {&c->pos_face, &c->pos_qpts64, &c->pos_qpts32, &c->pos_normal64, &c->pos_normal32,
+                      &c->pos_curl64, &c->pos_curl32, &c->pos_area64, &c->pos_area32, &c->pos_gvert, &c->d_verts,
+                      &c->d_faces, &c->d_normals, &c->d_areas, &c->d_curls, &c->d_qpts, &c->sp_test, &c->sp_trial,
+                      &c->sp_rule, &c->sp_jac, &c->sp_nn, &c->rule_start, &c->rule_data, &c->status, &c->barrier})
+        b->free_();
+    for (Tiling *t : {&c->test_tiles, &c->trial_tiles}) {
+        t->face_start.free_();
+        t->vert_start.free_();
+        t->verts.free_();
+        t->local_vert.free_();
+    }
+    for (auto &e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    cudaGetLastError();
+    delete c;
+    return BEAT_B200_OK;
+}
+
+const char *beat_b200_last_error(const beat_b200_ctx *c) { return c ? c->last_error.c_str() : "null context"; }
+
+int32_t beat_b200_set_mesh(beat_b200_ctx *c, int32_t V, const double *vertices, int32_t F, const int32_t *faces,
+                           int32_t quad_order, int32_t singular_order) {
+    return guarded(c, [&] { set_mesh(c, V, vertices, F, faces, quad_order, singular_order); });
+}
+
+int32_t beat_b200_solve_device(beat_b200_ctx *c, double k, double eta, int32_t R, const void *d_q,
+                               const beat_b200_opts *opts, void *d_p, beat_b200_diag *diag) {
+    return guarded(c, [&] {
+        BB_REQUIRE(d_q && d_p, BEAT_B200_INVALID_ARG, "null device pointer");
+        const beat_b200_opts o = resolve_opts(opts);
+        solve_core(c, k, eta, R, (const double *)d_q, o, (double *)d_p, diag);
+    });
+}
+
+int32_t beat_b200_solve(beat_b200_ctx *c, double k, double eta, int32_t R, const double *q,
+                        const beat_b200_opts *opts, double *p_out, beat_b200_diag *diag) {
+    return guarded(c, [&] {
+        BB_REQUIRE(q && p_out && R >= 1, BEAT_B200_INVALID_ARG, "null pointer or R < 1");
+        BB_REQUIRE(c->F > 0, BEAT_B200_STATE, "no mesh: call beat_b200_set_mesh first");
+        const beat_b200_opts o = resolve_opts(opts);
+        ensure_workspace(c, o.precision, R);
+        Workspace &w = c->ws;
+        BB_CUDA(cudaMemcpyAsync(w.q.p, q, (size_t)c->F * R * 16, cudaMemcpyHostToDevice, c->stream));
+        DevBuf out;
+        out.alloc((size_t)c->V * R * 16);
+        try {
+            solve_core(c, k, eta, R, w.q.as<double>(), o, out.as<double>(), diag);
+            BB_CUDA(cudaMemcpyAsync(p_out, out.p, (size_t)c->V * R * 16, cudaMemcpyDeviceToHost, c->stream));
+            BB_CUDA(cudaStreamSynchronize(c->stream));
+        } catch (...) {
+            if (c->stream) cudaStreamSynchronize(c->stream);
+            out.free_();
+            throw;
+        }
+        out.free_();
+    });
+}
+
+static int32_t field_common(beat_b200_ctx *c, double k, int32_t M, const double *pts, int32_t R, const double *p,
+                            const double *q, double *out, bool far) {
+    return guarded(c, [&] {
+        BB_REQUIRE(c->F > 0, BEAT_B200_STATE, "no mesh: call beat_b200_set_mesh first");
+        BB_REQUIRE(M >= 0 && R >= 1 && (M == 0 || (pts && p && q && out)), BEAT_B200_INVALID_ARG,
+                   "field: bad arguments");
+        if (M == 0) return;
+        DevBuf buf;
+        buf.alloc(16 * ((size_t)c->V * R + (size_t)c->F * R + (size_t)M * R));
+        try {
+            double *dp = buf.as<double>(), *dq = dp + 2 * (size_t)c->V * R, *dout = dq + 2 * (size_t)c->F * R;
+            BB_CUDA(cudaMemcpyAsync(dp, p, (size_t)c->V * R * 16, cudaMemcpyHostToDevice, c->stream));
+            BB_CUDA(cudaMemcpyAsync(dq, q, (size_t)c->F * R * 16, cudaMemcpyHostToDevice, c->stream));
+            farfield(c, k, M, pts, R, dp, dq, dout, far);
+            BB_CUDA(cudaMemcpyAsync(out, dout, (size_t)M * R * 16, cudaMemcpyDeviceToHost, c->stream));
+            BB_CUDA(cudaStreamSynchronize(c->stream));
+        } catch (...) {
+            buf.free_();
+            throw;
+        }
+        buf.free_();
+    });
+}
+
+int32_t beat_b200_field(beat_b200_ctx *c, double k, int32_t M, const double *points, int32_t R, const double *p,
+                        const double *q, double *out) {
+    return field_common(c, k, M, points, R, p, q, out, false);
+}
+
+int32_t beat_b200_farfield(beat_b200_ctx *c, double k, int32_t M, const double *dirs, int32_t R, const double *p,
+                           const double *q, double *out) {
+    return field_common(c, k, M, dirs, R, p, q, out, true);
+}
+
+int32_t beat_b200_farfield_device(beat_b200_ctx *c, double k, int32_t M, const double *dirs, int32_t R,
+                                  const void *d_p, const void *d_q, void *d_out) {
+    return guarded(c, [&] {
+        BB_REQUIRE(dirs && d_p && d_q && d_out, BEAT_B200_INVALID_ARG, "null pointer");
+        farfield(c, k, M, dirs, R, (const double *)d_p, (const double *)d_q, (double *)d_out, true);
+    });
+}
+
+int32_t beat_b200_assemble(beat_b200_ctx *c, double k, double eta, int32_t R, const double *q, int32_t precision,
+                           double *A_out, double *b_out) {
+    return guarded(c, [&] {
+        BB_REQUIRE(c->F > 0, BEAT_B200_STATE, "no mesh: call beat_b200_set_mesh first");
+        BB_REQUIRE(R >= 0 && (R == 0 || q), BEAT_B200_INVALID_ARG, "assemble: bad arguments");
+        BB_REQUIRE(precision == BEAT_B200_FP64 || precision == BEAT_B200_MIXED_FP32_IR, BEAT_B200_INVALID_ARG,
+                   "unknown precision form");
+        const int Rr = std::max(R, 1);
+        ensure_workspace(c, precision, Rr);
+        Workspace &w = c->ws;
+        const int n = c->V;
+        if (R > 0)
+            BB_CUDA(cudaMemcpyAsync(w.q.p, q, (size_t)c->F * R * 16, cudaMemcpyHostToDevice, c->stream));
+        else
+            BB_CUDA(cudaMemsetAsync(w.q.p, 0, (size_t)c->F * 16, c->stream));
+        assemble(c, k, eta, precision, Rr, w.q.p, nullptr, nullptr);
+        w.lu_valid = 0;
+        if (A_out) {
+            DevBuf tmp;
+            tmp.alloc((size_t)n * n * 16);
+            dim3 grid((n + 31) / 32, (n + 31) / 32), block(32, 8);
+            if (precision == BEAT_B200_FP64)
+                export_matrix_kernel<double><<<grid, block, 0, c->stream>>>(w.A.as<Cx<double>>(), w.ld, n,
+                                                                            tmp.as<double2>());
+            else
+                export_matrix_kernel<float><<<grid, block, 0, c->stream>>>(w.A.as<Cx<float>>(), w.ld, n,
+                                                                           tmp.as<double2>());
+            BB_CUDA(cudaGetLastError());
+            BB_CUDA(cudaMemcpyAsync(A_out, tmp.p, (size_t)n * n * 16, cudaMemcpyDeviceToHost, c->stream));
+            BB_CUDA(cudaStreamSynchronize(c->stream));
+            tmp.free_();
+        }
+        if (b_out && R > 0) {
+            BB_CUDA(cudaMemcpyAsync(b_out, w.b.p, (size_t)n * R * 16, cudaMemcpyDeviceToHost, c->stream));
+        }
+        BB_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int32_t beat_b200_release_workspace(beat_b200_ctx *c) {
+    return guarded(c, [&] {
+        BB_CUDA(cudaStreamSynchronize(c->stream));
+        release_workspace(c);
+    });
+}
+
+int64_t beat_b200_device_bytes(const beat_b200_ctx *c) { return c ? device_bytes(c) : 0; }
+
+}  // extern "C"

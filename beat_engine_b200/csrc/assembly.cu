@@ -1,0 +1,557 @@
+// assembly.cu -- fused Burton-Miller system assembly on sm_100a.
+//
+//   A = 0.5 M_p1p1 - D + eta H            (N x N, row = test vertex)
+//   B = -S - eta (K' + 0.5 M_p1dp0)       (N x F, column = trial face)
+//   b = B q                               (N x R, FP64)
+//
+// Reference (paths relative to src/beat_engine/julia_local/src/):
+//   per point pair combination   BeatEngineCpuBurtonMiller.jl:53-112 (regular),
+//                                :116-167 (Duffy), green BeatEngineCpuAssembly.jl:1-6
+//   CUDA element-pair kernel      BeatEngineCudaRegular.jl:18-383
+//   Duffy block kernel + scatter  BeatEngineCudaSingular.jl:359-588,
+//                                 BeatEngineCudaBurtonMiller.jl:97-162,273-329
+//   identity kernel               BeatEngineCudaBurtonMiller.jl:21-69
+//   cached RHS operator  b = B Q  BeatEngineCudaBurtonMiller.jl:774-830
+//
+// Design (no reference counterpart): elements are sorted along a Morton curve
+// and cut into tiles of consecutive elements with few distinct vertices.  One
+// CTA integrates a (test tile x trial tile) block of element pairs; each
+// pair's 3x3 block and 3-vector land in shared-memory accumulators indexed by
+// tile-local vertex numbers, and the CTA flushes them to HBM once with
+// red.global.add.  The Duffy kernel runs one warp per touching pair, lanes
+// over the Duffy points, in FP64 in both precision forms.
+#include <cuda_runtime.h>
+
+#include "internal.cuh"
+
+namespace bb {
+
+constexpr int TT = 64, VT = 80;  // test tile: faces, distinct vertices (context.cu)
+constexpr int TS = 16, VS = 32;  // trial tile
+constexpr int REG_THREADS = 256;
+
+// rule tables: index 0 -> 1-point, 1 -> 3-point, 2 -> 6-point (order 4)
+__constant__ double c_rw64[3][6];
+__constant__ double c_rb64[3][6][3];
+__constant__ float c_rw32[3][6];
+__constant__ float c_rb32[3][6][3];
+
+template <typename T> struct RuleRef;
+template <> struct RuleRef<double> {
+    static __device__ __forceinline__ double w(int r, int q) { return c_rw64[r][q]; }
+    static __device__ __forceinline__ double b(int r, int q, int a) { return c_rb64[r][q][a]; }
+};
+template <> struct RuleRef<float> {
+    static __device__ __forceinline__ float w(int r, int q) { return c_rw32[r][q]; }
+    static __device__ __forceinline__ float b(int r, int q, int a) { return c_rb32[r][q][a]; }
+};
+
+void upload_rule_tables(const std::vector<double> &pts, const std::vector<double> &w, int Q) {
+    double w64[3][6] = {}, b64[3][6][3] = {};
+    float w32[3][6] = {}, b32[3][6][3] = {};
+    BB_CUDA(cudaMemcpyFromSymbol(w64, c_rw64, sizeof(w64)));
+    BB_CUDA(cudaMemcpyFromSymbol(b64, c_rb64, sizeof(b64)));
+    const int r = Q == 1 ? 0 : Q == 3 ? 1 : 2;
+    for (int q = 0; q < Q; ++q) {
+        w64[r][q] = w[q];
+        b64[r][q][0] = 1.0 - pts[2 * q] - pts[2 * q + 1];
+        b64[r][q][1] = pts[2 * q];
+        b64[r][q][2] = pts[2 * q + 1];
+    }
+    for (int i = 0; i < 3; ++i)
+        for (int q = 0; q < 6; ++q) {
+            w32[i][q] = (float)w64[i][q];
+            for (int a = 0; a < 3; ++a) b32[i][q][a] = (float)b64[i][q][a];
+        }
+    BB_CUDA(cudaMemcpyToSymbol(c_rw64, w64, sizeof(w64)));
+    BB_CUDA(cudaMemcpyToSymbol(c_rb64, b64, sizeof(b64)));
+    BB_CUDA(cudaMemcpyToSymbol(c_rw32, w32, sizeof(w32)));
+    BB_CUDA(cudaMemcpyToSymbol(c_rb32, b32, sizeof(b32)));
+}
+
+__device__ __forceinline__ void sincos_t(double x, double *s, double *c) { sincos(x, s, c); }
+__device__ __forceinline__ void sincos_t(float x, float *s, float *c) { sincosf(x, s, c); }
+__device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
+__device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
+
+__device__ __forceinline__ void red_add(double *p, double v) { atomicAdd(p, v); }
+__device__ __forceinline__ void red_add(float *p, float v) { atomicAdd(p, v); }
+__device__ __forceinline__ void red_add_cx(Cx<double> *p, double re, double im) {
+    atomicAdd(&p->re, re);
+    atomicAdd(&p->im, im);
+}
+__device__ __forceinline__ void red_add_cx(Cx<float> *p, float re, float im) {
+    atomicAdd(reinterpret_cast<float2 *>(p), make_float2(re, im));
+}
+
+template <typename T> struct RegArgs {
+    const T *qpts;      // by position: F x Q x 3
+    const T *normal;    // F x 3
+    const T *curl;      // F x 9
+    const T *area;      // F
+    const int *gvert;   // F x 3
+    const int *face_id; // F
+    const int *t_fstart, *t_vstart, *t_verts, *t_local;
+    const int *s_fstart, *s_vstart, *s_verts, *s_local;
+    Cx<T> *A;
+    Cx<T> *B;
+    int64_t ld;         // row stride of A (complex entries)
+    int F;
+    T k, eta, k2;
+};
+
+// Element-pair kernel.  grid = (trial tiles, test tiles), 256 threads.
+template <typename T, int Q>
+__global__ void __launch_bounds__(REG_THREADS) regular_pairs_kernel(RegArgs<T> g) {
+    constexpr int RI = Q == 1 ? 0 : Q == 3 ? 1 : 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cx<T> *sA = reinterpret_cast<Cx<T> *>(smem_raw);  // VT x VS
+    Cx<T> *sB = sA + VT * VS;                         // VT x TS
+    T *tq = reinterpret_cast<T *>(sB + VT * TS);      // TT x Q x 3
+    T *tn = tq + TT * Q * 3;                          // TT x 3
+    T *tc = tn + TT * 3;                              // TT x 9
+    T *ta = tc + TT * 9;                              // TT
+    T *sq = ta + TT;                                  // (Q*3) x TS (trial, transposed)
+    T *sn = sq + TS * Q * 3;                          // 3 x TS
+    T *sc = sn + TS * 3;                              // 9 x TS
+    T *sa = sc + TS * 9;                              // TS
+    int *tgv = reinterpret_cast<int *>(sa + TS);      // TT x 3
+    int *tlv = tgv + TT * 3;                          // TT x 3
+    int *sgv = tlv + TT * 3;                          // 3 x TS
+    int *slv = sgv + TS * 3;                          // 3 x TS
+
+    const int tid = threadIdx.x;
+    const int t0 = g.t_fstart[blockIdx.y], nt = g.t_fstart[blockIdx.y + 1] - t0;
+    const int s0 = g.s_fstart[blockIdx.x], ns = g.s_fstart[blockIdx.x + 1] - s0;
+    const int tv0 = g.t_vstart[blockIdx.y], nvt = g.t_vstart[blockIdx.y + 1] - tv0;
+    const int sv0 = g.s_vstart[blockIdx.x], nvs = g.s_vstart[blockIdx.x + 1] - sv0;
+
+    for (int i = tid; i < VT * VS; i += REG_THREADS) sA[i] = Cx<T>{T(0), T(0)};
+    for (int i = tid; i < VT * TS; i += REG_THREADS) sB[i] = Cx<T>{T(0), T(0)};
+    for (int i = tid; i < nt * Q * 3; i += REG_THREADS) tq[i] = g.qpts[(size_t)t0 * Q * 3 + i];
+    for (int i = tid; i < nt * 3; i += REG_THREADS) {
+        tn[i] = g.normal[(size_t)t0 * 3 + i];
+        tgv[i] = g.gvert[(size_t)t0 * 3 + i];
+        tlv[i] = g.t_local[(size_t)t0 * 3 + i];
+    }
+    for (int i = tid; i < nt * 9; i += REG_THREADS) tc[i] = g.curl[(size_t)t0 * 9 + i];
+    for (int i = tid; i < nt; i += REG_THREADS) ta[i] = g.area[t0 + i];
+    for (int i = tid; i < ns * Q * 3; i += REG_THREADS) {
+        int s = i / (Q * 3), j = i % (Q * 3);
+        sq[j * TS + s] = g.qpts[(size_t)s0 * Q * 3 + i];
+    }
+    for (int i = tid; i < ns * 3; i += REG_THREADS) {
+        int s = i / 3, j = i % 3;
+        sn[j * TS + s] = g.normal[(size_t)s0 * 3 + i];
+        sgv[j * TS + s] = g.gvert[(size_t)s0 * 3 + i];
+        slv[j * TS + s] = g.s_local[(size_t)s0 * 3 + i];
+    }
+    for (int i = tid; i < ns * 9; i += REG_THREADS) {
+        int s = i / 9, j = i % 9;
+        sc[j * TS + s] = g.curl[(size_t)s0 * 9 + i];
+    }
+    for (int i = tid; i < ns; i += REG_THREADS) sa[i] = g.area[s0 + i];
+    __syncthreads();
+
+    const T k = g.k, eta = g.eta;
+    const T inv4pi = T(0.07957747154594767);  // 1 / (4 pi)
+    const int npairs = nt * TS;
+    for (int p = tid; p < npairs; p += REG_THREADS) {
+        const int tl = p / TS, sl = p % TS;
+        if (sl >= ns) continue;
+        const int ga = tgv[3 * tl], gb = tgv[3 * tl + 1], gc = tgv[3 * tl + 2];
+        const int ha = sgv[sl], hb = sgv[TS + sl], hc = sgv[2 * TS + sl];
+        if (ga == ha || ga == hb || ga == hc || gb == ha || gb == hb || gb == hc || gc == ha || gc == hb ||
+            gc == hc)
+            continue;  // touching pair: the Duffy kernel integrates it
+        const T ntx = tn[3 * tl], nty = tn[3 * tl + 1], ntz = tn[3 * tl + 2];
+        const T nsx = sn[sl], nsy = sn[TS + sl], nsz = sn[2 * TS + sl];
+        const T k2n = eta * g.k2 * (ntx * nsx + nty * nsy + ntz * nsz);
+        T L[9][2], Rv[3][2], cr = T(0), ci = T(0);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) L[i][0] = L[i][1] = T(0);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) Rv[i][0] = Rv[i][1] = T(0);
+#pragma unroll 1
+        for (int qt = 0; qt < Q; ++qt) {
+            const T x0 = tq[(tl * Q + qt) * 3], x1 = tq[(tl * Q + qt) * 3 + 1], x2 = tq[(tl * Q + qt) * 3 + 2];
+            const T wt = RuleRef<T>::w(RI, qt) * inv4pi;
+            T S0r = 0, S0i = 0, S1r = 0, S1i = 0, S2r = 0, S2i = 0, Ur = 0, Ui = 0;
+#pragma unroll
+            for (int qs = 0; qs < Q; ++qs) {
+                const T rx = sq[(qs * 3) * TS + sl] - x0;
+                const T ry = sq[(qs * 3 + 1) * TS + sl] - x1;
+                const T rz = sq[(qs * 3 + 2) * TS + sl] - x2;
+                const T r2 = rx * rx + ry * ry + rz * rz;
+                const T ir = rsqrt_t(r2);
+                const T rad = r2 * ir;
+                T sn_, cs_;
+                sincos_t(k * rad, &sn_, &cs_);
+                const T scl = ir * (wt * RuleRef<T>::w(RI, qs));
+                const T gr = cs_ * scl, gi = sn_ * scl;           // weighted green
+                const T gsr = -gr * ir - gi * k;                  // weighted grad scale
+                const T gsi = gr * k - gi * ir;
+                const T dns = (rx * nsx + ry * nsy + rz * nsz) * ir;
+                const T dnt = -(rx * ntx + ry * nty + rz * ntz) * ir;
+                const T lr = -gsr * dns + k2n * gi;               // -grad*dn_s - i k2n g
+                const T li = -gsi * dns - k2n * gr;
+                const T rr = -gr + eta * (gsi * dnt);             // -g - i eta grad*dn_t
+                const T ri = -gi - eta * (gsr * dnt);
+                cr += gr;
+                ci += gi;
+                Ur += rr;
+                Ui += ri;
+                const T b0 = RuleRef<T>::b(RI, qs, 0), b1 = RuleRef<T>::b(RI, qs, 1), b2 = RuleRef<T>::b(RI, qs, 2);
+                S0r += b0 * lr;
+                S0i += b0 * li;
+                S1r += b1 * lr;
+                S1i += b1 * li;
+                S2r += b2 * lr;
+                S2i += b2 * li;
+            }
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const T ba = RuleRef<T>::b(RI, qt, a);
+                L[3 * a + 0][0] += ba * S0r;
+                L[3 * a + 0][1] += ba * S0i;
+                L[3 * a + 1][0] += ba * S1r;
+                L[3 * a + 1][1] += ba * S1i;
+                L[3 * a + 2][0] += ba * S2r;
+                L[3 * a + 2][1] += ba * S2i;
+                Rv[a][0] += ba * Ur;
+                Rv[a][1] += ba * Ui;
+            }
+        }
+        // hypersingular curl term: eta * sum(g w) * curl_t . curl_s
+        const T ccr = -eta * ci, cci = eta * cr;
+        const T jac = T(4) * ta[tl] * sa[sl];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int row = tlv[3 * tl + a];
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const T d = tc[9 * tl + 3 * a] * sc[(3 * b) * TS + sl] +
+                            tc[9 * tl + 3 * a + 1] * sc[(3 * b + 1) * TS + sl] +
+                            tc[9 * tl + 3 * a + 2] * sc[(3 * b + 2) * TS + sl];
+                const int col = slv[b * TS + sl];
+                Cx<T> *dst = &sA[row * VS + col];
+                red_add(&dst->re, (L[3 * a + b][0] + d * ccr) * jac);
+                red_add(&dst->im, (L[3 * a + b][1] + d * cci) * jac);
+            }
+            Cx<T> *db = &sB[row * TS + sl];
+            red_add(&db->re, Rv[a][0] * jac);
+            red_add(&db->im, Rv[a][1] * jac);
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < nvt * nvs; i += REG_THREADS) {
+        const int lt = i / nvs, ls = i % nvs;
+        const Cx<T> v = sA[lt * VS + ls];
+        if (v.re != T(0) || v.im != T(0))
+            red_add_cx(&g.A[(int64_t)g.t_verts[tv0 + lt] * g.ld + g.s_verts[sv0 + ls]], v.re, v.im);
+    }
+    for (int i = tid; i < nvt * ns; i += REG_THREADS) {
+        const int lt = i / ns, sl = i % ns;
+        const Cx<T> v = sB[lt * TS + sl];
+        if (v.re != T(0) || v.im != T(0))
+            red_add_cx(&g.B[(int64_t)g.t_verts[tv0 + lt] * g.F + g.face_id[s0 + sl]], v.re, v.im);
+    }
+}
+
+template <typename T, int Q> static size_t regular_smem_bytes() {
+    return sizeof(Cx<T>) * (VT * VS + VT * TS) + sizeof(T) * (TT * (Q * 3 + 3 + 9 + 1) + TS * (Q * 3 + 3 + 9 + 1)) +
+           sizeof(int) * (TT * 6 + TS * 6);
+}
+
+// ---------------------------------------------------------------------------
+// touching pairs: one warp per pair, FP64, Duffy points over the lanes
+// ---------------------------------------------------------------------------
+template <typename T> struct SingArgs {
+    const int *test, *trial, *rule;
+    const double *jac, *nn;
+    const int *rule_start;
+    const double *rule_data;  // 5 per point
+    const double *verts;      // V x 3
+    const int *faces;         // F x 3
+    const double *normals;    // F x 3
+    const double *curls;      // F x 9
+    Cx<T> *A;
+    Cx<T> *B;
+    int64_t ld;
+    int F;
+    int64_t npairs;
+    double k, eta;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) singular_pairs_kernel(SingArgs<T> g) {
+    const int lane = threadIdx.x & 31;
+    const int64_t pair = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    if (pair >= g.npairs) return;
+    const int t = g.test[pair], s = g.trial[pair], r = g.rule[pair];
+    const int *ft = g.faces + 3 * t, *fs = g.faces + 3 * s;
+    double tv[3][3], sv[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            tv[a][c] = g.verts[3 * ft[a] + c];
+            sv[a][c] = g.verts[3 * fs[a] + c];
+        }
+    const double ntx = g.normals[3 * t], nty = g.normals[3 * t + 1], ntz = g.normals[3 * t + 2];
+    const double nsx = g.normals[3 * s], nsy = g.normals[3 * s + 1], nsz = g.normals[3 * s + 2];
+    const double k = g.k, eta = g.eta;
+    const double k2n = eta * (k * k * g.nn[pair]);
+    double acc[26];
+#pragma unroll
+    for (int i = 0; i < 26; ++i) acc[i] = 0.0;  // L[9] re/im, R[3] re/im, curl re/im
+    const int q1 = g.rule_start[r + 1];
+    for (int q = g.rule_start[r] + lane; q < q1; q += 32) {
+        const double *d = g.rule_data + 5 * (size_t)q;
+        const double xi = d[0], et = d[1], yi = d[2], ye = d[3], w = d[4];
+        const double bt[3] = {1.0 - xi - et, xi, et}, bs[3] = {1.0 - yi - ye, yi, ye};
+        double x[3], y[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            x[c] = bt[0] * tv[0][c] + bt[1] * tv[1][c] + bt[2] * tv[2][c];
+            y[c] = bs[0] * sv[0][c] + bs[1] * sv[1][c] + bs[2] * sv[2][c];
+        }
+        const double rx = y[0] - x[0], ry = y[1] - x[1], rz = y[2] - x[2];
+        const double r2 = rx * rx + ry * ry + rz * rz;
+        if (r2 == 0.0) continue;
+        const double rad = sqrt(r2), ir = 1.0 / rad;
+        double sn_, cs_;
+        sincos(k * rad, &sn_, &cs_);
+        const double scl = ir * (0.07957747154594767 * w);
+        const double gr = cs_ * scl, gi = sn_ * scl;
+        const double gsr = -gr * ir - gi * k, gsi = gr * k - gi * ir;
+        const double dns = (rx * nsx + ry * nsy + rz * nsz) * ir;
+        const double dnt = -(rx * ntx + ry * nty + rz * ntz) * ir;
+        const double lr = -gsr * dns + k2n * gi, li = -gsi * dns - k2n * gr;
+        const double rr = -gr + eta * (gsi * dnt), ri = -gi - eta * (gsr * dnt);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const double bp = bt[a] * bs[b];
+                acc[2 * (3 * a + b)] += bp * lr;
+                acc[2 * (3 * a + b) + 1] += bp * li;
+            }
+            acc[18 + 2 * a] += bt[a] * rr;
+            acc[18 + 2 * a + 1] += bt[a] * ri;
+        }
+        acc[24] += gr;
+        acc[25] += gi;
+    }
+#pragma unroll
+    for (int i = 0; i < 26; ++i) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
+    }
+    const double jac = g.jac[pair];
+    const double ccr = -eta * acc[25], cci = eta * acc[24];
+    if (lane < 9) {
+        const int a = lane / 3, b = lane % 3;
+        const double *cta = g.curls + 9 * t + 3 * a, *csb = g.curls + 9 * s + 3 * b;
+        const double d = cta[0] * csb[0] + cta[1] * csb[1] + cta[2] * csb[2];
+        double vr = 0, vi = 0;
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+            if (i == lane) {
+                vr = acc[2 * i];
+                vi = acc[2 * i + 1];
+            }
+        red_add_cx(&g.A[(int64_t)ft[a] * g.ld + fs[b]], (T)((vr + d * ccr) * jac), (T)((vi + d * cci) * jac));
+    } else if (lane < 12) {
+        const int a = lane - 9;
+        double vr = 0, vi = 0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            if (i == a) {
+                vr = acc[18 + 2 * i];
+                vi = acc[18 + 2 * i + 1];
+            }
+        red_add_cx(&g.B[(int64_t)ft[a] * g.F + s], (T)(vr * jac), (T)(vi * jac));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// identity terms: A += 0.5 M_p1p1, B += -0.5 eta M_p1dp0
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void identity_kernel(const int *faces, const double *areas, int F, int Q, double eta, Cx<T> *A,
+                                int64_t ld, Cx<T> *B) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= F) return;
+    const int ri = Q == 1 ? 0 : Q == 3 ? 1 : 2;
+    const double jac = 2.0 * areas[f];
+    double blk[9] = {0}, col[3] = {0};
+    for (int q = 0; q < Q; ++q) {
+        const double w = c_rw64[ri][q];
+        for (int a = 0; a < 3; ++a) {
+            const double pa = c_rb64[ri][q][a];
+            col[a] += pa * w * jac;
+            for (int b = 0; b < 3; ++b) blk[3 * a + b] += pa * c_rb64[ri][q][b] * w * jac;
+        }
+    }
+    const int *fc = faces + 3 * f;
+    for (int a = 0; a < 3; ++a) {
+        for (int b = 0; b < 3; ++b) red_add(&A[(int64_t)fc[a] * ld + fc[b]].re, (T)(0.5 * blk[3 * a + b]));
+        red_add(&B[(int64_t)fc[a] * F + f].im, (T)(-0.5 * eta * col[a]));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// b = B q: one warp per row, up to 16 columns per pass, q chunk in smem
+// ---------------------------------------------------------------------------
+constexpr int BQ_ROWS = 8, BQ_CHUNK = 128, BQ_RC = 16;
+
+template <typename T>
+__global__ void __launch_bounds__(256) rhs_apply_kernel(const Cx<T> *B, int N, int F, const Cx<double> *q, int R,
+                                                        int r0, Cx<double> *b) {
+    __shared__ Cx<double> sq[BQ_RC][BQ_CHUNK];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int row = blockIdx.x * BQ_ROWS + warp;
+    const int rc = min(BQ_RC, R - r0);
+    double ar[BQ_RC], ai[BQ_RC];
+#pragma unroll
+    for (int r = 0; r < BQ_RC; ++r) ar[r] = ai[r] = 0.0;
+    for (int f0 = 0; f0 < F; f0 += BQ_CHUNK) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < BQ_RC * BQ_CHUNK; i += blockDim.x) {
+            const int r = i / BQ_CHUNK, f = f0 + i % BQ_CHUNK;
+            sq[r][i % BQ_CHUNK] = (r < rc && f < F) ? q[(size_t)(r0 + r) * F + f] : Cx<double>{0.0, 0.0};
+        }
+        __syncthreads();
+        if (row < N) {
+            for (int j = lane; j < BQ_CHUNK && f0 + j < F; j += 32) {
+                const Cx<T> bv = B[(int64_t)row * F + f0 + j];
+                const double br = (double)bv.re, bi = (double)bv.im;
+#pragma unroll
+                for (int r = 0; r < BQ_RC; ++r) {
+                    const Cx<double> qv = sq[r][j];
+                    ar[r] += br * qv.re - bi * qv.im;
+                    ai[r] += br * qv.im + bi * qv.re;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < BQ_RC; ++r) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ar[r] += __shfl_xor_sync(0xffffffffu, ar[r], o);
+            ai[r] += __shfl_xor_sync(0xffffffffu, ai[r], o);
+        }
+    }
+    if (row < N && lane < rc) {
+        double vr = 0, vi = 0;
+#pragma unroll
+        for (int r = 0; r < BQ_RC; ++r)
+            if (r == lane) {
+                vr = ar[r];
+                vi = ai[r];
+            }
+        b[(size_t)(r0 + lane) * N + row] = Cx<double>{vr, vi};
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host driver
+// ---------------------------------------------------------------------------
+template <typename T, int Q> static void launch_regular(beat_b200_ctx *c, double k, double eta) {
+    RegArgs<T> g;
+    const bool d = sizeof(T) == 8;
+    g.qpts = (const T *)(d ? c->pos_qpts64.p : c->pos_qpts32.p);
+    g.normal = (const T *)(d ? c->pos_normal64.p : c->pos_normal32.p);
+    g.curl = (const T *)(d ? c->pos_curl64.p : c->pos_curl32.p);
+    g.area = (const T *)(d ? c->pos_area64.p : c->pos_area32.p);
+    g.gvert = c->pos_gvert.as<int>();
+    g.face_id = c->pos_face.as<int>();
+    g.t_fstart = c->test_tiles.face_start.as<int>();
+    g.t_vstart = c->test_tiles.vert_start.as<int>();
+    g.t_verts = c->test_tiles.verts.as<int>();
+    g.t_local = c->test_tiles.local_vert.as<int>();
+    g.s_fstart = c->trial_tiles.face_start.as<int>();
+    g.s_vstart = c->trial_tiles.vert_start.as<int>();
+    g.s_verts = c->trial_tiles.verts.as<int>();
+    g.s_local = c->trial_tiles.local_vert.as<int>();
+    g.A = c->ws.A.as<Cx<T>>();
+    g.B = c->ws.B.as<Cx<T>>();
+    g.ld = c->ws.ld;
+    g.F = c->F;
+    g.k = (T)k;
+    g.eta = (T)eta;
+    g.k2 = (T)(k * k);
+    const size_t smem = regular_smem_bytes<T, Q>();
+    BB_CUDA(cudaFuncSetAttribute(regular_pairs_kernel<T, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid(c->trial_tiles.ntiles, c->test_tiles.ntiles);
+    regular_pairs_kernel<T, Q><<<grid, REG_THREADS, smem, c->stream>>>(g);
+    BB_CUDA(cudaGetLastError());
+}
+
+template <typename T> static void assemble_t(beat_b200_ctx *c, double k, double eta, int R, const Cx<double> *q,
+                                             float *ms_total, float *ms_singular) {
+    Workspace &w = c->ws;
+    const int N = c->V, F = c->F;
+    BB_CUDA(cudaEventRecord(c->ev[0], c->stream));
+    BB_CUDA(cudaMemsetAsync(w.A.p, 0, (size_t)N * w.ld * sizeof(Cx<T>), c->stream));
+    BB_CUDA(cudaMemsetAsync(w.B.p, 0, (size_t)N * F * sizeof(Cx<T>), c->stream));
+    switch (c->Q) {
+        case 1: launch_regular<T, 1>(c, k, eta); break;
+        case 3: launch_regular<T, 3>(c, k, eta); break;
+        default: launch_regular<T, 6>(c, k, eta); break;
+    }
+    BB_CUDA(cudaEventRecord(c->ev[1], c->stream));
+    if (c->npairs > 0) {
+        SingArgs<T> s;
+        s.test = c->sp_test.as<int>();
+        s.trial = c->sp_trial.as<int>();
+        s.rule = c->sp_rule.as<int>();
+        s.jac = c->sp_jac.as<double>();
+        s.nn = c->sp_nn.as<double>();
+        s.rule_start = c->rule_start.as<int>();
+        s.rule_data = c->rule_data.as<double>();
+        s.verts = c->d_verts.as<double>();
+        s.faces = c->d_faces.as<int>();
+        s.normals = c->d_normals.as<double>();
+        s.curls = c->d_curls.as<double>();
+        s.A = w.A.as<Cx<T>>();
+        s.B = w.B.as<Cx<T>>();
+        s.ld = w.ld;
+        s.F = F;
+        s.npairs = c->npairs;
+        s.k = k;
+        s.eta = eta;
+        const int wpb = 8;
+        singular_pairs_kernel<T><<<(unsigned)((c->npairs + wpb - 1) / wpb), 32 * wpb, 0, c->stream>>>(s);
+        BB_CUDA(cudaGetLastError());
+    }
+    BB_CUDA(cudaEventRecord(c->ev[2], c->stream));
+    identity_kernel<T><<<(F + 255) / 256, 256, 0, c->stream>>>(c->d_faces.as<int>(), c->d_areas.as<double>(), F,
+                                                               c->Q, eta, w.A.as<Cx<T>>(), w.ld, w.B.as<Cx<T>>());
+    BB_CUDA(cudaGetLastError());
+    for (int r0 = 0; r0 < R; r0 += BQ_RC)
+        rhs_apply_kernel<T><<<(N + BQ_ROWS - 1) / BQ_ROWS, 256, 0, c->stream>>>(w.B.as<Cx<T>>(), N, F, q, R, r0,
+                                                                                 w.b.as<Cx<double>>());
+    BB_CUDA(cudaGetLastError());
+    BB_CUDA(cudaEventRecord(c->ev[3], c->stream));
+    if (ms_total || ms_singular) {
+        BB_CUDA(cudaEventSynchronize(c->ev[3]));
+        if (ms_total) BB_CUDA(cudaEventElapsedTime(ms_total, c->ev[0], c->ev[3]));
+        if (ms_singular) BB_CUDA(cudaEventElapsedTime(ms_singular, c->ev[1], c->ev[2]));
+    }
+}
+
+void assemble(beat_b200_ctx *c, double k, double eta, int precision, int R, const void *q_dev, float *ms_total,
+              float *ms_singular) {
+    BB_REQUIRE(c->F > 0, BEAT_B200_STATE, "no mesh: call beat_b200_set_mesh first");
+    BB_REQUIRE(std::isfinite(k) && k != 0.0 && std::isfinite(eta), BEAT_B200_INVALID_ARG,
+               "assemble: wavenumber must be finite and nonzero");
+    if (precision == BEAT_B200_FP64)
+        assemble_t<double>(c, k, eta, R, (const Cx<double> *)q_dev, ms_total, ms_singular);
+    else
+        assemble_t<float>(c, k, eta, R, (const Cx<double> *)q_dev, ms_total, ms_singular);
+}
+
+}  // namespace bb

@@ -1,0 +1,191 @@
+// internal.cuh -- shared declarations of libbeatb200 (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/beat_b200.h"
+
+namespace bb {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+struct Error {
+    int32_t code;
+    std::string msg;
+};
+
+#define BB_CUDA(call)                                                                       \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            throw ::bb::Error{e_ == cudaErrorMemoryAllocation ? BEAT_B200_OOM               \
+                                                              : BEAT_B200_CUDA_ERROR,       \
+                              std::string(#call) + ": " + cudaGetErrorString(e_)};          \
+    } while (0)
+
+#define BB_REQUIRE(cond, code, text)                    \
+    do {                                                \
+        if (!(cond)) throw ::bb::Error{(code), (text)}; \
+    } while (0)
+
+// device-side status words (one int per context, read by the host after a
+// stage that can give up)
+enum DeviceStatus : int {
+    DEV_OK = 0,
+    DEV_BARRIER_TIMEOUT = 1,  // a grid barrier ran out of its spin budget
+    DEV_ZERO_PIVOT = 2,
+    DEV_BAD_INDEX = 4,
+};
+
+// ---------------------------------------------------------------------------
+// device buffers (plain cudaMalloc, owned by the context)
+// ---------------------------------------------------------------------------
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    void alloc(size_t n);
+    void free_();
+    template <typename T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+// ---------------------------------------------------------------------------
+// complex helpers
+// ---------------------------------------------------------------------------
+template <typename T> struct alignas(2 * sizeof(T)) Cx {
+    T re, im;
+};
+
+template <typename T> __host__ __device__ __forceinline__ Cx<T> cmul(Cx<T> a, Cx<T> b) {
+    return Cx<T>{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+
+// ---------------------------------------------------------------------------
+// mesh-derived tables for the element-pair kernel
+// ---------------------------------------------------------------------------
+struct Tiling {
+    int tile_faces = 0;   // max faces per tile
+    int tile_verts = 0;   // max distinct vertices per tile
+    int ntiles = 0;
+    DevBuf face_start;    // ntiles + 1 (positions in the sorted face order)
+    DevBuf vert_start;    // ntiles + 1
+    DevBuf verts;         // concatenated global vertex ids per tile
+    DevBuf local_vert;    // F x 3 (by sorted position): index of each face vertex in its tile
+};
+
+struct Workspace {
+    int precision = -1;
+    int N = 0, F = 0, R = 0;
+    int64_t ld = 0;       // leading dimension (row stride, in complex entries) of A
+    DevBuf A;             // N x ld system matrix (row-major); FP64 or FP32 complex
+    DevBuf Aop;           // mixed form: FP32 copy kept as the refinement operator
+    DevBuf B;             // N x F RHS operator (row-major), same precision as A
+    DevBuf b;             // N x R FP64 right-hand sides (column-major)
+    DevBuf x;             // N x R FP64 solution (column-major)
+    DevBuf ipiv;          // N int
+    DevBuf perm;          // N int (row permutation of the factorisation)
+    DevBuf panel_scratch; // pivot candidates, published rows
+    DevBuf stage;         // tensor-core staging (expanded operands)
+    DevBuf krylov;        // GMRES bases
+    DevBuf small;         // GMRES small vectors
+    DevBuf q;             // F x R FP64 Neumann data (column-major)
+    int lu_valid = 0;     // factors match the current operator
+};
+
+}  // namespace bb
+
+// ---------------------------------------------------------------------------
+// the opaque context
+// ---------------------------------------------------------------------------
+struct beat_b200_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+
+    // mesh (host copies)
+    int V = 0, F = 0, Q = 0, quad_order = 4, sing_order = 4;
+    std::vector<double> verts;    // V x 3
+    std::vector<int> faces;       // F x 3, 0-based
+    std::vector<double> normals;  // F x 3
+    std::vector<double> areas;    // F
+    std::vector<double> rule_pts; // Q x 2
+    std::vector<double> rule_w;   // Q
+
+    // device mesh data indexed by sorted position (Morton order of centroids)
+    bb::DevBuf pos_face;          // F: original face id at each position
+    bb::DevBuf pos_qpts64;        // F x Q x 3
+    bb::DevBuf pos_qpts32;
+    bb::DevBuf pos_normal64;      // F x 3
+    bb::DevBuf pos_normal32;
+    bb::DevBuf pos_curl64;        // F x 9
+    bb::DevBuf pos_curl32;
+    bb::DevBuf pos_area64;        // F
+    bb::DevBuf pos_area32;
+    bb::DevBuf pos_gvert;         // F x 3 global vertex ids
+    bb::Tiling test_tiles, trial_tiles;
+
+    // device mesh data by original face id
+    bb::DevBuf d_verts;           // V x 3 double
+    bb::DevBuf d_faces;           // F x 3 int (0-based)
+    bb::DevBuf d_normals;         // F x 3 double
+    bb::DevBuf d_areas;           // F double
+    bb::DevBuf d_curls;           // F x 9 double
+    bb::DevBuf d_qpts;            // F x Q x 3 double (field sources)
+
+    // singular (touching) pairs
+    int64_t npairs = 0;
+    int nrules = 0;
+    bb::DevBuf sp_test, sp_trial, sp_rule;  // int per pair (original face ids)
+    bb::DevBuf sp_jac, sp_nn;               // double per pair
+    bb::DevBuf rule_start;                  // nrules + 1
+    bb::DevBuf rule_data;                   // per point: test xi, eta, trial xi, eta, weight
+
+    int64_t regular_pairs = 0;
+    bb::DevBuf status;            // device status word(s)
+    bb::DevBuf barrier;           // grid-barrier counters
+    bb::Workspace ws;
+
+    cudaEvent_t ev[8] = {};
+};
+
+namespace bb {
+
+// context.cu
+void set_mesh(beat_b200_ctx *c, int V, const double *verts, int F, const int32_t *faces,
+              int quad_order, int sing_order);
+void ensure_workspace(beat_b200_ctx *c, int precision, int R);
+void release_workspace(beat_b200_ctx *c);
+int64_t device_bytes(const beat_b200_ctx *c);
+int read_status(beat_b200_ctx *c);
+
+// assembly.cu: rule tables in constant memory (fixed per rule size)
+void upload_rule_tables(const std::vector<double> &pts, const std::vector<double> &w, int Q);
+// assembly.cu: A (row-major N x ld) and B (N x F) in the workspace precision,
+// then b = B q (FP64, N x R column-major).  q_dev is F x R FP64 complex.
+void assemble(beat_b200_ctx *c, double k, double eta, int precision, int R, const void *q_dev,
+              float *ms_total, float *ms_singular);
+
+// lu.cu
+void lu_factor(beat_b200_ctx *c, int precision, int nb, int split_terms);
+void lu_solve_fp64(beat_b200_ctx *c, int R, double *x_dev);          // in place, N x R col-major
+void lu_precond_fp32(beat_b200_ctx *c, int R, const double *in, double *out);
+
+// gmres.cu
+struct IrResult {
+    int iterations;
+    int converged;
+    double residual;
+};
+IrResult gmres_refine(beat_b200_ctx *c, int R, double *x_dev, const double *b_dev, int restart,
+                      int max_iters, double rtol);
+
+// field.cu
+void farfield(beat_b200_ctx *c, double k, int M, const double *dirs_host, int R, const double *p_dev,
+              const double *q_dev, double *out_dev, bool far);
+
+}  // namespace bb

@@ -1,0 +1,575 @@
+// lu.cu -- blocked right-looking complex LU with partial pivoting, and the
+// multi-right-hand-side triangular solves, on one B200.
+//
+// Replaces the reference's lu!(system.matrix) / factorization \ rhs
+// (BeatEngineCompiledDriver.jl:902-903 -> cuSOLVER getrf/getrs through
+// CUDA.jl, and OpenBLAS zgetrf on the CPU path, BeatEngineDenseSolve.jl:1104-1110).
+// Pivoting is the partial pivoting LAPACK uses (first maximum of |re| + |im|
+// in the column), so the factorisation is P A = L U with unit-lower L.
+//
+// Layout: A is row-major complex, row stride ld (complex entries).  Row
+// interchanges are then contiguous copies.
+//
+// Per panel of nb columns:
+//   1. panel_kernel: a cooperative kernel; the panel rows are split over the
+//      CTAs and held in shared memory.  Per column every CTA publishes its
+//      best candidate row, one grid barrier, every CTA picks the same winner,
+//      swaps and eliminates locally.  Candidate slots are double-buffered by
+//      column parity so one barrier per column suffices.
+//   2. laswp_kernel: the panel's interchanges on all other columns (and on
+//      the running row permutation).
+//   3. trsm_kernel: U12 = L11^-1 A12.
+//   4. trailing update A22 -= L21 U12: SIMT complex GEMM here (FP64 form),
+//      tcgen05 TF32 tensor-core GEMM for the FP32 form (tc_gemm.cu).
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "internal.cuh"
+
+namespace bb {
+
+// device-side wait with a budget; gives up by setting a status bit
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void grid_barrier(unsigned *ctr, unsigned target, int *status, unsigned limit) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(ctr, 1u);
+        unsigned it = 0;
+        while (ld_acquire_u32(ctr) < target) {
+            if (*(volatile int *)status & DEV_BARRIER_TIMEOUT) break;
+            if (++it > limit) {
+                atomicOr(status, (int)DEV_BARRIER_TIMEOUT);
+                break;
+            }
+            __nanosleep(64);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+template <typename T> __device__ __forceinline__ T cabs1(Cx<T> v) { return fabs(v.re) + fabs(v.im); }
+
+// L2-coherent loads of values other CTAs published before a grid barrier
+__device__ __forceinline__ Cx<double> ldcg(const Cx<double> *p) {
+    const double2 v = __ldcg(reinterpret_cast<const double2 *>(p));
+    return Cx<double>{v.x, v.y};
+}
+__device__ __forceinline__ Cx<float> ldcg(const Cx<float> *p) {
+    const float2 v = __ldcg(reinterpret_cast<const float2 *>(p));
+    return Cx<float>{v.x, v.y};
+}
+__device__ __forceinline__ double ldcg(const double *p) { return __ldcg(p); }
+__device__ __forceinline__ float ldcg(const float *p) { return __ldcg(p); }
+__device__ __forceinline__ int ldcg(const int *p) { return __ldcg(p); }
+
+template <typename T> struct PanelArgs {
+    Cx<T> *A;
+    int64_t ld;
+    int n, k, nb;
+    int rpc;            // rows per CTA
+    int *ipiv;
+    Cx<T> *pub_rows;    // [2][G][nb]
+    Cx<T> *pub_diag;    // [2][nb]
+    T *pub_val;         // [2][G]
+    int *pub_idx;       // [2][G]
+    unsigned *barrier;
+    int *status;
+    unsigned spin_limit;
+};
+
+constexpr int PANEL_THREADS = 256;
+
+template <typename T> __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(PanelArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nb = a.nb, G = gridDim.x, cta = blockIdx.x, tid = threadIdx.x;
+    Cx<T> *P = reinterpret_cast<Cx<T> *>(smem_raw);  // rpc x nb
+    Cx<T> *prow = P + (size_t)a.rpc * nb;             // nb
+    Cx<T> *drow = prow + nb;                          // nb
+    Cx<T> *lcol = drow + nb;                          // rpc
+    __shared__ T red_v[PANEL_THREADS / 32];
+    __shared__ int red_i[PANEL_THREADS / 32];
+    __shared__ int s_piv;
+    __shared__ T s_pv;
+
+    const int gr0 = a.k + cta * a.rpc;
+    const int nrows = max(0, min(a.rpc, a.n - gr0));
+    for (int i = tid; i < nrows * nb; i += PANEL_THREADS) {
+        const int r = i / nb, c = i % nb;
+        P[i] = a.A[(int64_t)(gr0 + r) * a.ld + a.k + c];
+    }
+    __syncthreads();
+
+    for (int j = 0; j < nb && a.k + j < a.n; ++j) {
+        const int jr = a.k + j, par = j & 1;
+        // local candidate: first maximum of |re|+|im| among own rows >= jr
+        T bv = T(-1);
+        int bi = -1;
+        for (int i = tid; i < nrows; i += PANEL_THREADS) {
+            if (gr0 + i < jr) continue;
+            const T v = cabs1(P[i * nb + j]);
+            if (v > bv) {
+                bv = v;
+                bi = gr0 + i;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const T ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ov > bv || (ov == bv && oi >= 0 && (bi < 0 || oi < bi))) {
+                bv = ov;
+                bi = oi;
+            }
+        }
+        if ((tid & 31) == 0) {
+            red_v[tid >> 5] = bv;
+            red_i[tid >> 5] = bi;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            for (int w = 1; w < PANEL_THREADS / 32; ++w)
+                if (red_v[w] > bv || (red_v[w] == bv && red_i[w] >= 0 && (bi < 0 || red_i[w] < bi))) {
+                    bv = red_v[w];
+                    bi = red_i[w];
+                }
+            a.pub_val[par * G + cta] = bv;
+            a.pub_idx[par * G + cta] = bi;
+            s_piv = bi;
+        }
+        __syncthreads();
+        const int mine = s_piv;
+        if (mine >= 0)
+            for (int c = tid; c < nb; c += PANEL_THREADS)
+                a.pub_rows[((size_t)par * G + cta) * nb + c] = P[(mine - gr0) * nb + c];
+        if (jr >= gr0 && jr < gr0 + nrows)
+            for (int c = tid; c < nb; c += PANEL_THREADS) a.pub_diag[(size_t)par * nb + c] = P[(jr - gr0) * nb + c];
+        grid_barrier(a.barrier, (unsigned)(j + 1) * G, a.status, a.spin_limit);
+
+        // every CTA picks the same winner
+        if (tid < 32) {
+            T wv = T(-1);
+            int wi = -1, wc = -1;
+            for (int g = tid; g < G; g += 32) {
+                const T v = ldcg(&a.pub_val[par * G + g]);
+                const int i = ldcg(&a.pub_idx[par * G + g]);
+                if (i >= 0 && (v > wv || (v == wv && (wi < 0 || i < wi)))) {
+                    wv = v;
+                    wi = i;
+                    wc = g;
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const T ov = __shfl_xor_sync(0xffffffffu, wv, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, wi, o);
+                const int oc = __shfl_xor_sync(0xffffffffu, wc, o);
+                if (oi >= 0 && (ov > wv || (ov == wv && (wi < 0 || oi < wi)))) {
+                    wv = ov;
+                    wi = oi;
+                    wc = oc;
+                }
+            }
+            if (tid == 0) {
+                s_piv = wi < 0 ? jr : wi;
+                s_pv = wv;
+                red_i[0] = wc;
+                if (wv <= T(0)) atomicOr(a.status, (int)DEV_ZERO_PIVOT);
+                if (cta == 0) a.ipiv[jr] = s_piv;
+            }
+        }
+        __syncthreads();
+        const int p = s_piv, wc = red_i[0];
+        for (int c = tid; c < nb; c += PANEL_THREADS) {
+            prow[c] = wc >= 0 ? ldcg(&a.pub_rows[((size_t)par * G + wc) * nb + c]) : Cx<T>{T(0), T(0)};
+            drow[c] = ldcg(&a.pub_diag[(size_t)par * nb + c]);
+        }
+        __syncthreads();
+        if (p != jr) {
+            if (jr >= gr0 && jr < gr0 + nrows)
+                for (int c = tid; c < nb; c += PANEL_THREADS) P[(jr - gr0) * nb + c] = prow[c];
+            if (p >= gr0 && p < gr0 + nrows)
+                for (int c = tid; c < nb; c += PANEL_THREADS) P[(p - gr0) * nb + c] = drow[c];
+        }
+        __syncthreads();
+        // eliminate below the pivot
+        const Cx<T> pv = prow[j];
+        const T den = pv.re * pv.re + pv.im * pv.im;
+        const Cx<T> inv = den > T(0) ? Cx<T>{pv.re / den, -pv.im / den} : Cx<T>{T(0), T(0)};
+        const int first = max(0, jr + 1 - gr0);
+        for (int i = first + tid; i < nrows; i += PANEL_THREADS) lcol[i] = cmul(P[i * nb + j], inv);
+        __syncthreads();
+        const int w = nb - j - 1;
+        if (w > 0) {
+            for (int idx = tid; idx < (nrows - first) * w; idx += PANEL_THREADS) {
+                const int i = first + idx / w, c = j + 1 + idx % w;
+                const Cx<T> l = lcol[i], u = prow[c];
+                Cx<T> &d = P[i * nb + c];
+                d.re -= l.re * u.re - l.im * u.im;
+                d.im -= l.re * u.im + l.im * u.re;
+            }
+        }
+        for (int i = first + tid; i < nrows; i += PANEL_THREADS) P[i * nb + j] = lcol[i];
+        __syncthreads();
+    }
+    for (int i = tid; i < nrows * nb; i += PANEL_THREADS) {
+        const int r = i / nb, c = i % nb;
+        a.A[(int64_t)(gr0 + r) * a.ld + a.k + c] = P[i];
+    }
+}
+
+// row interchanges of one panel on all columns outside it; the extra
+// "column" -1 applies them to the running permutation perm[]
+template <typename T>
+__global__ void laswp_kernel(Cx<T> *A, int64_t ld, int n, int k, int nb, const int *ipiv, int *perm) {
+    __shared__ int sp[256];
+    for (int j = threadIdx.x; j < nb; j += blockDim.x) sp[j] = ipiv[k + j];
+    __syncthreads();
+    const int c = (int)(blockIdx.x * blockDim.x + threadIdx.x) - 1;
+    const int jmax = min(nb, n - k);
+    if (c == -1) {
+        for (int j = 0; j < jmax; ++j) {
+            const int p = sp[j];
+            if (p != k + j) {
+                const int t = perm[k + j];
+                perm[k + j] = perm[p];
+                perm[p] = t;
+            }
+        }
+        return;
+    }
+    if (c >= n || (c >= k && c < k + nb)) return;
+    for (int j = 0; j < jmax; ++j) {
+        const int p = sp[j];
+        if (p != k + j) {
+            const Cx<T> t = A[(int64_t)(k + j) * ld + c];
+            A[(int64_t)(k + j) * ld + c] = A[(int64_t)p * ld + c];
+            A[(int64_t)p * ld + c] = t;
+        }
+    }
+}
+
+__global__ void iota_kernel(int *perm, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) perm[i] = i;
+}
+
+// U12 = L11^-1 A12 for columns [k+nb, n); 32 columns per CTA
+constexpr int TRSM_COLS = 32;
+template <typename T> __global__ void __launch_bounds__(256) trsm_kernel(Cx<T> *A, int64_t ld, int n, int k, int nb) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cx<T> *L = reinterpret_cast<Cx<T> *>(smem_raw);  // nb x nb
+    Cx<T> *X = L + nb * nb;                           // nb x TRSM_COLS
+    const int c0 = k + nb + blockIdx.x * TRSM_COLS;
+    const int nc = min(TRSM_COLS, n - c0);
+    const int kb = min(nb, n - k);
+    for (int i = threadIdx.x; i < kb * kb; i += blockDim.x) {
+        const int r = i / kb, c = i % kb;
+        L[r * nb + c] = A[(int64_t)(k + r) * ld + k + c];
+    }
+    for (int i = threadIdx.x; i < kb * TRSM_COLS; i += blockDim.x) {
+        const int r = i / TRSM_COLS, c = i % TRSM_COLS;
+        X[r * TRSM_COLS + c] = c < nc ? A[(int64_t)(k + r) * ld + c0 + c] : Cx<T>{T(0), T(0)};
+    }
+    __syncthreads();
+    for (int j = 0; j < kb - 1; ++j) {
+        for (int idx = threadIdx.x; idx < (kb - 1 - j) * TRSM_COLS; idx += blockDim.x) {
+            const int i = j + 1 + idx / TRSM_COLS, c = idx % TRSM_COLS;
+            const Cx<T> l = L[i * nb + j], x = X[j * TRSM_COLS + c];
+            Cx<T> &d = X[i * TRSM_COLS + c];
+            d.re -= l.re * x.re - l.im * x.im;
+            d.im -= l.re * x.im + l.im * x.re;
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < kb * TRSM_COLS; i += blockDim.x) {
+        const int r = i / TRSM_COLS, c = i % TRSM_COLS;
+        if (c < nc) A[(int64_t)(k + r) * ld + c0 + c] = X[r * TRSM_COLS + c];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// SIMT complex GEMM for the trailing update: C[m0.., n0..] -= L U
+// L = A[r, k:k+kk], U = A[k:k+kk, c]; 64 x 64 output tile, 256 threads,
+// 4 x 4 complex accumulators per thread.
+// ---------------------------------------------------------------------------
+constexpr int GT = 64, GKC = 16;
+template <typename T>
+__global__ void __launch_bounds__(256) gemm_update_kernel(Cx<T> *A, int64_t ld, int n, int k, int kk, int row0,
+                                                          int col0) {
+    __shared__ Cx<T> sL[GKC][GT + 1];
+    __shared__ Cx<T> sU[GKC][GT];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int r0 = row0 + blockIdx.y * GT, c0 = col0 + blockIdx.x * GT;
+    T acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = T(0);
+    for (int kc = 0; kc < kk; kc += GKC) {
+        for (int idx = threadIdx.x; idx < GT * GKC; idx += 256) {
+            const int i = idx / GKC, q = idx % GKC;
+            const int r = r0 + i, kq = kc + q;
+            sL[q][i] = (r < n && kq < kk) ? A[(int64_t)r * ld + k + kq] : Cx<T>{T(0), T(0)};
+            const int q2 = idx / GT, j = idx % GT;
+            const int c = c0 + j, kq2 = kc + q2;
+            sU[q2][j] = (c < n && kq2 < kk) ? A[(int64_t)(k + kq2) * ld + c] : Cx<T>{T(0), T(0)};
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int q = 0; q < GKC; ++q) {
+            Cx<T> a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = sL[q][ty + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = sU[q][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    acc[i][j][0] += a[i].re * b[j].re - a[i].im * b[j].im;
+                    acc[i][j][1] += a[i].re * b[j].im + a[i].im * b[j].re;
+                }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int r = r0 + ty + 16 * i, c = c0 + tx + 16 * j;
+            if (r < n && c < n) {
+                Cx<T> &d = A[(int64_t)r * ld + c];
+                d.re -= acc[i][j][0];
+                d.im -= acc[i][j][1];
+            }
+        }
+}
+
+// FP32 form trailing update on the tensor cores (tc_gemm.cu); returns false
+// when the shape is not supported, in which case the SIMT kernel runs.
+bool tc_trailing_update(beat_b200_ctx *c, int k, int nb, int split_terms);
+
+// ---------------------------------------------------------------------------
+// host driver
+// ---------------------------------------------------------------------------
+template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int split_terms) {
+    Workspace &w = c->ws;
+    const int n = c->V;
+    const int64_t ld = w.ld;
+    Cx<T> *A = w.A.as<Cx<T>>();
+    int G = c->sm_count;
+    // shared memory per CTA for the panel: rows x nb + 2 nb + rows
+    const size_t smem_cap = 200 * 1024;
+    int rpc = (n + G - 1) / G;
+    size_t smem = sizeof(Cx<T>) * ((size_t)rpc * nb + 2 * nb + rpc);
+    BB_REQUIRE(smem <= smem_cap, BEAT_B200_INVALID_ARG,
+               "LU: system of order " + std::to_string(n) + " exceeds the shared-memory panel limit");
+    // scratch: [2][G][nb] rows + [2][nb] diag + [2][G] vals + [2][G] idx
+    const size_t scratch = sizeof(Cx<T>) * (2 * (size_t)G * nb + 2 * nb) + sizeof(T) * 2 * G + sizeof(int) * 2 * G;
+    w.panel_scratch.alloc(scratch + 256);
+    Cx<T> *pub_rows = w.panel_scratch.as<Cx<T>>();
+    Cx<T> *pub_diag = pub_rows + 2 * (size_t)G * nb;
+    T *pub_val = reinterpret_cast<T *>(pub_diag + 2 * nb);
+    int *pub_idx = reinterpret_cast<int *>(pub_val + 2 * G);
+    c->barrier.alloc(sizeof(unsigned) * 4096);
+    BB_CUDA(cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+    const size_t trsm_smem = sizeof(Cx<T>) * ((size_t)nb * nb + (size_t)nb * TRSM_COLS);
+    BB_CUDA(cudaFuncSetAttribute(trsm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
+    iota_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(w.perm.as<int>(), n);
+    BB_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream));
+    for (int k = 0; k < n; k += nb) {
+        const int m = n - k;
+        int g = std::min(G, std::max(1, (m + 15) / 16));
+        int rows = (m + g - 1) / g;
+        PanelArgs<T> a;
+        a.A = A;
+        a.ld = ld;
+        a.n = n;
+        a.k = k;
+        a.nb = nb;
+        a.rpc = rows;
+        a.ipiv = w.ipiv.as<int>();
+        a.pub_rows = pub_rows;
+        a.pub_diag = pub_diag;
+        a.pub_val = pub_val;
+        a.pub_idx = pub_idx;
+        a.barrier = c->barrier.as<unsigned>();
+        a.status = c->status.as<int>();
+        a.spin_limit = 1u << 22;
+        const size_t ps = sizeof(Cx<T>) * ((size_t)rows * nb + 2 * nb + rows);
+        BB_CUDA(cudaMemsetAsync(c->barrier.p, 0, sizeof(unsigned), c->stream));
+        void *args[] = {&a};
+        BB_CUDA(cudaLaunchCooperativeKernel((void *)panel_kernel<T>, dim3(g), dim3(PANEL_THREADS), args, ps,
+                                            c->stream));
+        laswp_kernel<T><<<(n + 1 + 255) / 256, 256, 0, c->stream>>>(A, ld, n, k, nb, w.ipiv.as<int>(),
+                                                                    w.perm.as<int>());
+        BB_CUDA(cudaGetLastError());
+        const int rest = n - k - nb;
+        if (rest > 0) {
+            trsm_kernel<T><<<(rest + TRSM_COLS - 1) / TRSM_COLS, 256, trsm_smem, c->stream>>>(A, ld, n, k, nb);
+            BB_CUDA(cudaGetLastError());
+            if (!(sizeof(T) == 4 && tc_trailing_update(c, k, nb, split_terms))) {
+                dim3 grid((rest + GT - 1) / GT, (rest + GT - 1) / GT);
+                gemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(A, ld, n, k, nb, k + nb, k + nb);
+                BB_CUDA(cudaGetLastError());
+            }
+        }
+    }
+}
+
+void lu_factor(beat_b200_ctx *c, int precision, int nb, int split_terms) {
+    if (precision == BEAT_B200_FP64)
+        lu_factor_t<double>(c, nb, split_terms);
+    else
+        lu_factor_t<float>(c, nb, split_terms);
+    c->ws.lu_valid = 1;
+}
+
+// ---------------------------------------------------------------------------
+// triangular solves with R right-hand sides (X column-major N x R, FP64)
+// ---------------------------------------------------------------------------
+__global__ void permute_rows_kernel(const double2 *in, double2 *out, const int *perm, int n, int R) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int src = perm[i];
+    for (int r = 0; r < R; ++r) out[(size_t)r * n + i] = in[(size_t)r * n + src];
+}
+
+constexpr int SB = 64;  // solve block
+// solve the diagonal block [kb, kb+bs) in place (unit lower or upper)
+template <typename T, bool LOWER>
+__global__ void __launch_bounds__(256) diag_solve_kernel(const Cx<T> *A, int64_t ld, int n, int kb, int bs,
+                                                         double2 *X, int R) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cx<double>(*D)[SB + 1] = reinterpret_cast<Cx<double>(*)[SB + 1]>(smem_raw);
+    Cx<double>(*Y)[17] = reinterpret_cast<Cx<double>(*)[17]>(smem_raw + sizeof(Cx<double>) * SB * (SB + 1));
+    const int r0 = blockIdx.x * 16;
+    const int rc = min(16, R - r0);
+    for (int i = threadIdx.x; i < bs * bs; i += blockDim.x) {
+        const int a = i / bs, b = i % bs;
+        const Cx<T> v = A[(int64_t)(kb + a) * ld + kb + b];
+        D[a][b] = Cx<double>{(double)v.re, (double)v.im};
+    }
+    for (int i = threadIdx.x; i < bs * 16; i += blockDim.x) {
+        const int a = i / 16, r = i % 16;
+        const double2 v = r < rc ? X[(size_t)(r0 + r) * n + kb + a] : make_double2(0, 0);
+        Y[a][r] = Cx<double>{v.x, v.y};
+    }
+    __syncthreads();
+    const int r = threadIdx.x;  // one thread per RHS column
+    if (r < 16) {
+        if (LOWER) {
+            for (int j = 0; j < bs; ++j) {
+                const Cx<double> y = Y[j][r];
+                for (int i = j + 1; i < bs; ++i) {
+                    const Cx<double> l = D[i][j];
+                    Y[i][r].re -= l.re * y.re - l.im * y.im;
+                    Y[i][r].im -= l.re * y.im + l.im * y.re;
+                }
+            }
+        } else {
+            for (int j = bs - 1; j >= 0; --j) {
+                const Cx<double> u = D[j][j];
+                const double den = u.re * u.re + u.im * u.im;
+                const Cx<double> v = Y[j][r];
+                const Cx<double> y = {(v.re * u.re + v.im * u.im) / den, (v.im * u.re - v.re * u.im) / den};
+                Y[j][r] = y;
+                for (int i = 0; i < j; ++i) {
+                    const Cx<double> l = D[i][j];
+                    Y[i][r].re -= l.re * y.re - l.im * y.im;
+                    Y[i][r].im -= l.re * y.im + l.im * y.re;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < bs * 16; i += blockDim.x) {
+        const int a = i / 16, rr = i % 16;
+        if (rr < rc) X[(size_t)(r0 + rr) * n + kb + a] = make_double2(Y[a][rr].re, Y[a][rr].im);
+    }
+}
+
+// X[rows] -= A[rows, kb:kb+bs] X[kb:kb+bs]; 16 rows per CTA, 16 RHS per CTA
+template <typename T>
+__global__ void __launch_bounds__(256) block_update_kernel(const Cx<T> *A, int64_t ld, int n, int kb, int bs,
+                                                           int row_begin, int row_end, double2 *X, int R) {
+    __shared__ Cx<double> Lt[16][SB + 1];
+    __shared__ Cx<double> Y[SB][17];
+    const int i0 = row_begin + blockIdx.x * 16, r0 = blockIdx.y * 16;
+    const int rc = min(16, R - r0);
+    for (int i = threadIdx.x; i < 16 * bs; i += blockDim.x) {
+        const int a = i / bs, b = i % bs;
+        Cx<T> v = (i0 + a < row_end) ? A[(int64_t)(i0 + a) * ld + kb + b] : Cx<T>{T(0), T(0)};
+        Lt[a][b] = Cx<double>{(double)v.re, (double)v.im};
+    }
+    for (int i = threadIdx.x; i < bs * 16; i += blockDim.x) {
+        const int a = i / 16, r = i % 16;
+        const double2 v = r < rc ? X[(size_t)(r0 + r) * n + kb + a] : make_double2(0, 0);
+        Y[a][r] = Cx<double>{v.x, v.y};
+    }
+    __syncthreads();
+    const int a = threadIdx.x >> 4, r = threadIdx.x & 15;
+    if (i0 + a < row_end && r < rc) {
+        double sr = 0, si = 0;
+        for (int b = 0; b < bs; ++b) {
+            const Cx<double> l = Lt[a][b], y = Y[b][r];
+            sr += l.re * y.re - l.im * y.im;
+            si += l.re * y.im + l.im * y.re;
+        }
+        double2 &d = X[(size_t)(r0 + r) * n + i0 + a];
+        d.x -= sr;
+        d.y -= si;
+    }
+}
+
+template <typename T> static void lu_solve_t(beat_b200_ctx *c, int R, const double *in, double *out) {
+    Workspace &w = c->ws;
+    const int n = c->V;
+    const Cx<T> *A = w.A.as<Cx<T>>();
+    double2 *X = reinterpret_cast<double2 *>(out);
+    const size_t dsm = sizeof(Cx<double>) * (SB * (SB + 1) + SB * 17);
+    BB_CUDA(cudaFuncSetAttribute(diag_solve_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
+    BB_CUDA(cudaFuncSetAttribute(diag_solve_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
+    permute_rows_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(reinterpret_cast<const double2 *>(in), X,
+                                                                w.perm.as<int>(), n, R);
+    const int rg = (R + 15) / 16;
+    for (int kb = 0; kb < n; kb += SB) {
+        const int bs = std::min(SB, n - kb);
+        diag_solve_kernel<T, true><<<rg, 256, dsm, c->stream>>>(A, w.ld, n, kb, bs, X, R);
+        if (kb + bs < n) {
+            dim3 grid((n - kb - bs + 15) / 16, rg);
+            block_update_kernel<T><<<grid, 256, 0, c->stream>>>(A, w.ld, n, kb, bs, kb + bs, n, X, R);
+        }
+    }
+    for (int kb = ((n - 1) / SB) * SB; kb >= 0; kb -= SB) {
+        const int bs = std::min(SB, n - kb);
+        diag_solve_kernel<T, false><<<rg, 256, dsm, c->stream>>>(A, w.ld, n, kb, bs, X, R);
+        if (kb > 0) {
+            dim3 grid((kb + 15) / 16, rg);
+            block_update_kernel<T><<<grid, 256, 0, c->stream>>>(A, w.ld, n, kb, bs, 0, kb, X, R);
+        }
+    }
+    BB_CUDA(cudaGetLastError());
+}
+
+void lu_solve_fp64(beat_b200_ctx *c, int R, double *x_dev) {
+    // x_dev holds b on entry (N x R), solution on exit; uses ws.x as scratch
+    BB_CUDA(cudaMemcpyAsync(c->ws.x.p, x_dev, (size_t)c->V * R * 16, cudaMemcpyDeviceToDevice, c->stream));
+    lu_solve_t<double>(c, R, c->ws.x.as<double>(), x_dev);
+}
+
+void lu_precond_fp32(beat_b200_ctx *c, int R, const double *in, double *out) {
+    lu_solve_t<float>(c, R, in, out);
+}
+
+}  // namespace bb

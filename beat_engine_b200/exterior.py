@@ -1,0 +1,135 @@
+"""Host-side mirror of the reference's exterior direct-system interface.
+
+Paths relative to ``src/beat_engine/julia_local/``:
+
+* :func:`solve_exterior_direct_b200` mirrors ``solve_exterior_direct_cuda``
+  (``BeatEngineCompiledDriver.jl:870-915``): Neumann values per excitation in,
+  boundary pressures per excitation out, one factorisation for all of them,
+  plus the assembly and solve seconds.
+* :func:`evaluate_galerkin_field_b200` mirrors ``evaluate_galerkin_field_cuda``
+  (``src/BeatEngineCudaField.jl:329-389``).
+* :func:`exterior_neumann` mirrors ``exterior_neumann``
+  (``BeatEngineCompiledDriver.jl:825-839``) for tag-driven excitations,
+  including the rigid-translation motion factor ``n_f . axis``.
+* ``BURTON_MILLER_ASSEMBLY = "b200_direct"`` is the new value of the
+  ``burton_miller_assembly`` solver option that selects this path
+  (the reference accepts ``direct_system`` / ``operator_matrices``,
+  ``BeatEngineCompiledDriver.jl:1066-1069``).
+
+Wavenumbers are passed unsigned, as the reference passes them; the phasor
+convention is an argument instead of the reference's global.  Errors raise
+:class:`~beat_engine_b200._lib.BeatB200Error` (the reference raises through
+``error(...)`` into a ``failed`` worker event).
+"""
+from __future__ import annotations
+
+import time
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib
+from .mesh import BoundaryMesh
+from .phasor import (NEGATIVE_TIME_PHASOR, burton_miller_coupling, neumann_scale, outgoing_wavenumber)
+
+BURTON_MILLER_ASSEMBLY = "b200_direct"
+PRECISIONS = {"float64": _lib.FP64, "mixed_fp32_ir": _lib.MIXED_FP32_IR}
+
+
+class ExteriorB200Cache:
+    """Per-mesh device context: the analogue of the reference's
+    ``device_cache`` / ``device_singular_cache`` pair built once per request
+    (``BeatEngineCompiledDriver.jl:1133-1176``) and reused over frequencies."""
+
+    def __init__(self, mesh: BoundaryMesh, quadrature_order: int = 4, singular_order: int = 4, device: int = 0):
+        self.mesh = mesh
+        self.quadrature_order = quadrature_order
+        self.singular_order = singular_order
+        self.ctx = _lib.Context(device)
+        self.ctx.set_mesh(mesh.vertices, mesh.faces, quadrature_order, singular_order)
+
+    def close(self):
+        self.ctx.close()
+
+
+def solver_options_precision(options: dict) -> int:
+    """``b200_precision`` solver option -> precision form (default mixed)."""
+    name = str(options.get("b200_precision", "mixed_fp32_ir")).lower()
+    if name not in PRECISIONS:
+        raise ValueError(f"b200_precision must be one of {sorted(PRECISIONS)}; got {name!r}")
+    return PRECISIONS[name]
+
+
+def solve_exterior_direct_b200(mesh: BoundaryMesh, neumann_values: Sequence[np.ndarray], wavenumber: float, *,
+                               cache: ExteriorB200Cache | None = None, precision: str = "mixed_fp32_ir",
+                               phasor_convention: str = NEGATIVE_TIME_PHASOR, ir_restart: int = 20,
+                               ir_rtol: float = 1e-10, lu_split_terms: int = 3, quadrature_order: int = 4,
+                               singular_order: int = 4):
+    """Assemble the Burton-Miller system for every excitation, factor once,
+    solve all columns.  Returns ``(pressures, assembly_s, solve_s, report)``
+    with ``pressures`` a list of length-N complex vectors, like the reference."""
+    if precision not in PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+    own = cache is None
+    if own:
+        cache = ExteriorB200Cache(mesh, quadrature_order, singular_order)
+    try:
+        q = np.stack([np.asarray(v, dtype=np.complex128) for v in neumann_values], axis=1)
+        k = outgoing_wavenumber(wavenumber, phasor_convention)
+        eta = burton_miller_coupling(wavenumber, phasor_convention).imag
+        opts = _lib.Context.opts(PRECISIONS[precision], ir_restart=ir_restart, ir_rtol=ir_rtol,
+                                 lu_split_terms=lu_split_terms)
+        t0 = time.perf_counter()
+        p, diag = cache.ctx.solve(k, eta, q, opts)
+        wall = time.perf_counter() - t0
+        assembly_s = diag["assembly_ms"] / 1e3
+        solve_s = max(wall - assembly_s, 0.0)
+        report = dict(diag, burton_miller_assembly=BURTON_MILLER_ASSEMBLY, factorization_count=1,
+                      linear_solver="b200_lu" if precision == "float64" else "b200_lu_gmres_ir",
+                      b200_precision=precision)
+        return [p[:, i].copy() for i in range(p.shape[1])], assembly_s, solve_s, report
+    finally:
+        if own:
+            cache.close()
+
+
+def evaluate_galerkin_field_b200(points, mesh: BoundaryMesh, pressure, q, wavenumber: float,
+                                 cache: ExteriorB200Cache, phasor_convention: str = NEGATIVE_TIME_PHASOR):
+    """Pressure at observation points (``M`` or ``M x R``)."""
+    k = outgoing_wavenumber(wavenumber, phasor_convention)
+    out = cache.ctx.field(k, points, pressure, q)
+    return out[:, 0] if np.asarray(pressure).ndim == 1 else out
+
+
+def evaluate_far_field_b200(directions, mesh: BoundaryMesh, pressure, q, wavenumber: float,
+                            cache: ExteriorB200Cache, phasor_convention: str = NEGATIVE_TIME_PHASOR):
+    """Far-field pattern ``lim r exp(-i k r) p(r d)`` (no reference counterpart)."""
+    k = outgoing_wavenumber(wavenumber, phasor_convention)
+    out = cache.ctx.farfield(k, directions, pressure, q)
+    return out[:, 0] if np.asarray(pressure).ndim == 1 else out
+
+
+def exterior_neumann(mesh: BoundaryMesh, tags, amplitudes, density: float, omega: float,
+                     phasor_convention: str = NEGATIVE_TIME_PHASOR, motion_axis=None):
+    """Per-face Neumann data ``q_f = neumann_scale(rho, omega) * amplitude``
+    on faces carrying one of ``tags`` (times ``n_f . axis`` for a rigid
+    translation), zero elsewhere."""
+    values = np.zeros(mesh.num_faces, dtype=np.complex128)
+    scale = neumann_scale(density, omega, phasor_convention)
+    factor = np.ones(mesh.num_faces)
+    if motion_axis is not None:
+        ax = np.asarray(motion_axis, dtype=np.float64)
+        ax = ax / np.max(np.abs(ax))
+        ax = ax / np.linalg.norm(ax)
+        factor = mesh.normals @ ax
+    for tag, amp in zip(tags, amplitudes):
+        sel = mesh.physical_tags == tag
+        values[sel] = scale * amp * factor[sel]
+    return values
+
+
+def bem_normal_velocity_neumann(velocity, density: float, omega: float,
+                                phasor_convention: str = NEGATIVE_TIME_PHASOR):
+    """``neumann_scale .* motion`` for explicit per-face velocities
+    (the ``bem_normal_velocity`` branch of ``exterior_neumann``)."""
+    return neumann_scale(density, omega, phasor_convention) * np.asarray(velocity, dtype=np.complex128)

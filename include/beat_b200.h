@@ -1,0 +1,148 @@
+/*
+ * beat_b200.h -- C ABI of libbeatb200.so, the B200 (sm_100a) exterior
+ * Burton-Miller direct-system solver.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and returns
+ * an int32 status (BEAT_B200_OK = 0).  Nothing here traps or aborts; on error
+ * beat_b200_last_error() describes what failed.  A context is not thread safe:
+ * one context per request/mesh, called from one host thread (the reference's
+ * worker runs one job at a time).
+ *
+ * Layout conventions (Julia's, so the reference can pass its arrays as is):
+ *   vertices  V x 3 float64, one (x,y,z) triple per vertex
+ *             (Vector{SVector{3,Float64}} in memory)
+ *   faces     F x 3 int32, 1-based vertex numbers, one triple per face
+ *   complex   interleaved (re, im) float64 pairs (ComplexF64)
+ *   q, p, out column-major: q[f + r*F], p[i + r*N], out[m + r*M]
+ *
+ * Reference interfaces replaced (paths relative to src/beat_engine/julia_local/):
+ *   solve_exterior_direct_cuda            BeatEngineCompiledDriver.jl:870-915
+ *   assemble_burton_miller_neumann_system_cuda  src/BeatEngineCudaBurtonMiller.jl:396-580
+ *   lu!(system.matrix); factorization \ rhs     BeatEngineCompiledDriver.jl:902-903
+ *   evaluate_galerkin_field_cuda          src/BeatEngineCudaField.jl:329-389
+ *   build_cuda_regular_assembly_cache /
+ *   build_singular_correction_cache       src/BeatEngineCudaRegular.jl:827-893,
+ *                                         src/BeatEngineCore.jl:994-1089
+ *   reclaim_accelerator_memory!           BeatEngineCompiledDriver.jl:3951
+ */
+#ifndef BEAT_B200_H
+#define BEAT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BEAT_B200_ABI_VERSION 1
+
+/* status codes */
+#define BEAT_B200_OK 0
+#define BEAT_B200_INVALID_ARG 1
+#define BEAT_B200_OOM 2
+#define BEAT_B200_CUDA_ERROR 3
+#define BEAT_B200_NOT_CONVERGED 4 /* iterative refinement missed its tolerance */
+#define BEAT_B200_TIMEOUT 5       /* a device-side wait ran out of its budget */
+#define BEAT_B200_NO_DEVICE 6
+#define BEAT_B200_STATE 7         /* call order (e.g. solve before set_mesh) */
+#define BEAT_B200_SINGULAR 8      /* exact zero pivot */
+
+/* precision forms */
+#define BEAT_B200_FP64 0          /* FP64 assembly, FP64 LU, FP64 solve */
+#define BEAT_B200_MIXED_FP32_IR 1 /* FP32 regular assembly (FP64 singular),
+                                     FP32 complex LU with TF32 tensor-core
+                                     trailing updates, FP64 GMRES refinement */
+
+typedef struct beat_b200_ctx beat_b200_ctx;
+
+typedef struct {
+    int32_t precision;      /* BEAT_B200_FP64 or BEAT_B200_MIXED_FP32_IR */
+    int32_t ir_restart;     /* GMRES restart length (20) */
+    int32_t ir_max_iters;   /* total GMRES iterations allowed (200) */
+    int32_t lu_split_terms; /* TF32 products per trailing update: 1 or 3 (3) */
+    double ir_rtol;         /* relative residual target of the refinement (1e-10) */
+    int32_t lu_block;       /* LU panel width; 0 = tuned default */
+    int32_t flags;          /* reserved, pass 0 */
+} beat_b200_opts;
+
+typedef struct {
+    double assembly_ms;     /* regular + singular + identity + RHS */
+    double singular_ms;     /* Duffy pass alone (part of assembly_ms) */
+    double lu_ms;
+    double solve_ms;        /* triangular solves of the direct solve */
+    double ir_ms;           /* GMRES refinement (mixed form) */
+    double field_ms;
+    int32_t ir_iterations;
+    int32_t ir_converged;
+    double ir_residual;     /* final max over columns of ||b - A x|| / ||b|| */
+    int64_t regular_pairs;
+    int64_t singular_pairs;
+    int32_t precision;
+    int32_t lu_block;
+    int32_t lu_split_terms;
+    int32_t reserved;
+} beat_b200_diag;
+
+/* ABI check: returns BEAT_B200_ABI_VERSION. */
+int32_t beat_b200_abi_version(void);
+
+/* Fill opts with the defaults listed above. */
+void beat_b200_default_opts(beat_b200_opts *opts);
+
+/* One context per mesh: device buffers, streams, tuned tile choices. */
+int32_t beat_b200_create(int32_t device, beat_b200_ctx **out);
+int32_t beat_b200_destroy(beat_b200_ctx *ctx);
+const char *beat_b200_last_error(const beat_b200_ctx *ctx);
+
+/* Upload a mesh and build everything that depends only on it: element
+ * geometry, the order-`quad_order` triangle rule (triangle_rule), touching
+ * pairs with orientation-remapped Duffy rules of order `singular_order`
+ * (build_singular_correction_cache), tiles for the element-pair kernel and
+ * the field source cache.  Host arrays are copied. */
+int32_t beat_b200_set_mesh(beat_b200_ctx *ctx, int32_t V, const double *vertices, int32_t F,
+                           const int32_t *faces, int32_t quad_order, int32_t singular_order);
+
+/* Assemble, factor once, solve all R right-hand sides (and refine in the
+ * mixed form).  k_signed = outgoing_wavenumber(k), eta_im = imag of
+ * burton_miller_coupling(k).  q: F x R Neumann data; p_out: N x R pressures.
+ * opts may be NULL (defaults), diag may be NULL.  The factors and the
+ * operator stay on the device for beat_b200_field / beat_b200_farfield. */
+int32_t beat_b200_solve(beat_b200_ctx *ctx, double k_signed, double eta_im, int32_t R,
+                        const double *q, const beat_b200_opts *opts, double *p_out,
+                        beat_b200_diag *diag);
+
+/* As beat_b200_solve with q and p_out in device memory (same layouts). */
+int32_t beat_b200_solve_device(beat_b200_ctx *ctx, double k_signed, double eta_im, int32_t R,
+                               const void *d_q, const beat_b200_opts *opts, void *d_p_out,
+                               beat_b200_diag *diag);
+
+/* Pressure at M observation points (M x 3) for R columns of boundary
+ * pressure p (N x R) and Neumann data q (F x R): out is M x R. */
+int32_t beat_b200_field(beat_b200_ctx *ctx, double k_signed, int32_t M, const double *points,
+                        int32_t R, const double *p, const double *q, double *out);
+
+/* Far-field pattern p_inf(d) = lim r exp(-i k r) p(r d) at M directions. */
+int32_t beat_b200_farfield(beat_b200_ctx *ctx, double k_signed, int32_t M, const double *dirs,
+                           int32_t R, const double *p, const double *q, double *out);
+
+/* Device-pointer variants of the two evaluators (points/dirs stay host). */
+int32_t beat_b200_farfield_device(beat_b200_ctx *ctx, double k_signed, int32_t M,
+                                  const double *dirs, int32_t R, const void *d_p,
+                                  const void *d_q, void *d_out);
+
+/* Assemble only and copy the system out (N x N column-major A, N x R b) in
+ * FP64, whatever the precision form; A_out or b_out may be NULL. */
+int32_t beat_b200_assemble(beat_b200_ctx *ctx, double k_signed, double eta_im, int32_t R,
+                           const double *q, int32_t precision, double *A_out, double *b_out);
+
+/* Free the per-solve workspaces (system matrix, factors, Krylov vectors);
+ * the mesh stays.  The next solve reallocates them. */
+int32_t beat_b200_release_workspace(beat_b200_ctx *ctx);
+
+/* Bytes of device memory the context holds right now. */
+int64_t beat_b200_device_bytes(const beat_b200_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BEAT_B200_H */

@@ -1,0 +1,224 @@
+"""GPU parity of libbeatb200 (through its C ABI) against the FP64 CPU oracle.
+
+Tolerances (written per test):
+  * FP64 assembly: entrywise within 1e-12 of the largest |A| entry, and
+    ||A - A_oracle||_F / ||A_oracle||_F <= 1e-12 (round-off of FP64
+    accumulation order only);
+  * FP32 regular assembly: ||dA||_F / ||A||_F <= 2e-6 (the reference CUDA gate
+    for FP32 direct assembly is rtol 2e-5, julia_local/tests/runtests.jl:1646);
+  * FP64 solve: relative L2 per column <= 1e-10;
+  * mixed FP32 + FP64 GMRES refinement: relative L2 per column <= 1e-6 vs the
+    FP64 oracle (the target of the mixed form);
+  * field / far field: relative L2 <= 1e-11.
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from beat_engine_b200 import _lib
+from beat_engine_b200 import mesh as M
+from beat_engine_b200 import phasor as P
+from beat_engine_b200.exterior import (ExteriorB200Cache, evaluate_galerkin_field_b200,
+                                       solve_exterior_direct_b200)
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def col_rel(a, b):
+    return np.linalg.norm(a - b, axis=0) / np.linalg.norm(b, axis=0)
+
+
+def random_q(F, R, seed):
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal((F, R)) + 1j * rng.standard_normal((F, R))
+
+
+@pytest.fixture(scope="module")
+def sphere3():
+    return M.reference_sphere(0.1, 3)
+
+
+@pytest.fixture(scope="module")
+def ctx3(sphere3):
+    c = _lib.Context(0)
+    c.set_mesh(sphere3.vertices, sphere3.faces, 4, 4)
+    yield c
+    c.close()
+
+
+def tetrahedron():
+    v = np.array([(0, 0, 0), (.23, 0, 0), (.02, .17, 0), (.03, .04, .13)], float)
+    f = np.array([(0, 2, 1), (0, 1, 3), (0, 3, 2), (1, 2, 3)])
+    return M.BoundaryMesh(v, f, np.array([1, 1, 1, 2]))
+
+
+@pytest.mark.parametrize("k", [7.0, 36.6, 110.0])
+def test_fp64_assembly_matches_oracle(ctx3, sphere3, k):
+    q = random_q(sphere3.num_faces, 3, 11)
+    eta = 1.0 / k
+    A, b = ctx3.assemble(k, eta, q, precision=_lib.FP64)
+    Ao, bo = oracle.assemble(sphere3, k, eta, q)
+    scale = np.abs(Ao).max()
+    assert np.abs(A - Ao).max() <= 1e-12 * scale
+    assert rel(A, Ao) <= 1e-12
+    assert rel(b, bo) <= 1e-12
+
+
+def test_fp64_assembly_negative_phasor_sign(ctx3, sphere3):
+    k, eta = -20.0, -1.0 / 20.0
+    q = random_q(sphere3.num_faces, 1, 12)
+    A, b = ctx3.assemble(k, eta, q, precision=_lib.FP64)
+    Ao, bo = oracle.assemble(sphere3, k, eta, q)
+    assert rel(A, Ao) <= 1e-12 and rel(b, bo) <= 1e-12
+
+
+def test_fp32_assembly_close_to_oracle(ctx3, sphere3):
+    k = 36.6
+    q = random_q(sphere3.num_faces, 2, 13)
+    A, b = ctx3.assemble(k, 1.0 / k, q, precision=_lib.MIXED_FP32_IR)
+    Ao, bo = oracle.assemble(sphere3, k, 1.0 / k, q)
+    assert rel(A, Ao) <= 2e-6
+    assert rel(b, bo) <= 2e-6
+
+
+@pytest.mark.parametrize("order,sorder", [(2, 2), (1, 3), (4, 2)])
+def test_other_quadrature_orders(order, sorder):
+    mesh = M.reference_sphere(0.1, 2)
+    k = 15.0
+    q = random_q(mesh.num_faces, 2, 14)
+    with _lib.Context(0) as c:
+        c.set_mesh(mesh.vertices, mesh.faces, order, sorder)
+        A, b = c.assemble(k, 1.0 / k, q, precision=_lib.FP64)
+    Ao, bo = oracle.assemble(mesh, k, 1.0 / k, q, quad_order=order, sing_order=sorder)
+    assert rel(A, Ao) <= 1e-12 and rel(b, bo) <= 1e-12
+
+
+def test_tiny_tetrahedron_all_pairs_touch():
+    mesh = tetrahedron()
+    q = random_q(4, 2, 15)
+    with _lib.Context(0) as c:
+        c.set_mesh(mesh.vertices, mesh.faces, 4, 4)
+        A, b = c.assemble(9.0, 1 / 9.0, q, precision=_lib.FP64)
+        p, d = c.solve(9.0, 1 / 9.0, q, _lib.Context.opts(_lib.FP64))
+    Ao, bo = oracle.assemble(mesh, 9.0, 1 / 9.0, q)
+    assert rel(A, Ao) <= 1e-12 and rel(b, bo) <= 1e-12
+    assert d["regular_pairs"] == 0 and d["singular_pairs"] == 16
+    assert np.all(col_rel(p, oracle.lu_solve(Ao, bo)) <= 1e-10)
+
+
+@pytest.mark.parametrize("R", [1, 5, 17])
+def test_fp64_solve_matches_oracle(ctx3, sphere3, R):
+    k = 36.6
+    q = random_q(sphere3.num_faces, R, 16 + R)
+    p, d = ctx3.solve(k, 1 / k, q, _lib.Context.opts(_lib.FP64))
+    Ao, bo = oracle.assemble(sphere3, k, 1 / k, q)
+    po = oracle.lu_solve(Ao, bo)
+    assert np.all(col_rel(p, po) <= 1e-10), col_rel(p, po)
+    assert d["precision"] == _lib.FP64
+
+
+@pytest.mark.parametrize("split", [1, 3])
+def test_mixed_solve_within_1e6_of_fp64_oracle(ctx3, sphere3, split):
+    k = 110.0
+    q = random_q(sphere3.num_faces, 4, 30)
+    p, d = ctx3.solve(k, 1 / k, q, _lib.Context.opts(_lib.MIXED_FP32_IR, lu_split_terms=split))
+    Ao, bo = oracle.assemble(sphere3, k, 1 / k, q)
+    po = oracle.lu_solve(Ao, bo)
+    err = col_rel(p, po)
+    assert d["ir_converged"] == 1 and d["ir_residual"] <= 1e-10
+    assert np.all(err <= 1e-6), err
+
+
+def test_field_and_farfield_match_oracle(ctx3, sphere3):
+    k = 36.6
+    rng = np.random.default_rng(40)
+    p = random_q(sphere3.num_vertices, 3, 41)
+    q = random_q(sphere3.num_faces, 3, 42)
+    pts = M.arc_points(181, 2.0) + rng.normal(0, 0.01, (181, 3))
+    f = ctx3.field(k, pts, p, q)
+    fo = oracle.field(sphere3, k, pts, p, q)
+    assert rel(f, fo) <= 1e-11
+    dirs = M.equator_meridian_directions(36, 19)
+    ff = ctx3.farfield(k, dirs, p, q)
+    ffo = oracle.farfield(sphere3, k, dirs, p, q)
+    assert rel(ff, ffo) <= 1e-11
+
+
+@pytest.mark.parametrize("precision", ["float64", "mixed_fp32_ir"])
+def test_analytic_pulsating_sphere_through_reference_interface(sphere3, precision):
+    """Config 0: pulsating sphere, exp(+i omega t), 181 points on a 2 m arc,
+    against p = rho c u (a/r) (ika/(1+ika)) exp(-ik(r-a)) at 0.05 dB / 0.5 deg."""
+    f, a, rho, c = 1000.0, 0.1, 1.21, 343.0
+    om = 2 * math.pi * f
+    k = om / c
+    conv = P.POSITIVE_TIME_PHASOR
+    q = np.full(sphere3.num_faces, P.neumann_scale(rho, om, conv))
+    cache = ExteriorB200Cache(sphere3)
+    try:
+        ps, asm_s, sol_s, rep = solve_exterior_direct_b200(sphere3, [q], k, cache=cache, precision=precision,
+                                                           phasor_convention=conv)
+        pts = M.arc_points(181, 2.0)
+        fld = evaluate_galerkin_field_b200(pts, sphere3, ps[0], q, k, cache, phasor_convention=conv)
+    finally:
+        cache.close()
+    r = np.linalg.norm(pts, axis=1)
+    ref = rho * c * (a / r) * (1j * k * a / (1 + 1j * k * a)) * np.exp(-1j * k * (r - a))
+    ratio = fld / ref
+    assert np.max(np.abs(20 * np.log10(np.abs(ratio)))) <= 0.05
+    assert np.max(np.abs(np.degrees(np.angle(ratio)))) <= 0.5
+    assert rep["burton_miller_assembly"] == "b200_direct" and rep["factorization_count"] == 1
+
+
+def test_golden_sweep_norms_on_gpu():
+    """Julia-produced norms of the reference's CPU sweep (sample.msh, order
+    2/2) through the FP64 GPU path, at the reference CI's 1e-3 (observed
+    agreement is ~1e-5, set by the reference's Float32 run)."""
+    gold = json.load(open(os.path.join(GOLD, "baseline_sweep_cpu.json")))
+    w = gold["workload"]
+    d = np.load(os.path.join(GOLD, "sample_msh.npz"))
+    mesh = M.BoundaryMesh(d["vertices"] * w["scale"], d["faces"], d["tags"])
+    pts = M.fibonacci_sphere(w["eval_points"], w["distance"])
+    with _lib.Context(0) as c:
+        c.set_mesh(mesh.vertices, mesh.faces, w["quadrature_order"], w["singular_order"])
+        for row in gold["frequencies"]:
+            om = 2 * math.pi * row["frequency_hz"]
+            k = om / w["sound_speed"]
+            q = np.zeros(mesh.num_faces, complex)
+            q[mesh.physical_tags == w["tag_throat"]] = 1j * w["rho"] * om
+            for prec in (_lib.FP64, _lib.MIXED_FP32_IR):
+                p, _ = c.solve(k, 1 / k, q, _lib.Context.opts(prec))
+                fld = c.field(k, pts, p, q)
+                assert abs(np.linalg.norm(p) / row["pressure_norm"] - 1) < 2e-5
+                assert abs(np.linalg.norm(fld) / row["field_norm"] - 1) < 2e-5
+
+
+def test_errors_are_status_codes():
+    import ctypes
+    with _lib.Context(0) as c:
+        q = np.zeros(4, complex)
+        p = np.zeros(4, complex)
+        st = c.lib.beat_b200_solve(c.handle, 10.0, 0.1, 1, _lib._dp(q), None, _lib._dp(p), None)
+        assert st == _lib.STATE
+        assert b"set_mesh" in c.lib.beat_b200_last_error(c.handle)
+        st = c.lib.beat_b200_farfield(c.handle, 10.0, 1, _lib._dp(np.ones(3)), 1, _lib._dp(p), _lib._dp(q),
+                                      _lib._dp(p))
+        assert st == _lib.STATE
+        h = ctypes.c_void_p()
+        assert c.lib.beat_b200_create(99, ctypes.byref(h)) == _lib.INVALID_ARG
+        with pytest.raises(_lib.BeatB200Error) as e:
+            c.set_mesh(np.zeros((3, 3)), np.array([[0, 1, 2]]))
+        assert e.value.status == _lib.INVALID_ARG
+        mesh = tetrahedron()
+        c.set_mesh(mesh.vertices, mesh.faces)
+        with pytest.raises(_lib.BeatB200Error) as e:
+            c.solve(0.0, 0.0, np.ones(4, complex))
+        assert e.value.status == _lib.INVALID_ARG
