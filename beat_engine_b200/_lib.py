@@ -24,7 +24,7 @@ EXPORTS = (
     "beat_b200_abi_version", "beat_b200_default_opts", "beat_b200_create", "beat_b200_destroy",
     "beat_b200_last_error", "beat_b200_set_mesh", "beat_b200_solve", "beat_b200_solve_device",
     "beat_b200_field", "beat_b200_farfield", "beat_b200_farfield_device", "beat_b200_assemble",
-    "beat_b200_release_workspace", "beat_b200_device_bytes",
+    "beat_b200_release_workspace", "beat_b200_device_bytes", "beat_b200_stream",
 )
 
 
@@ -35,7 +35,8 @@ class Opts(ctypes.Structure):
 
 
 class Diag(ctypes.Structure):
-    _fields_ = [("assembly_ms", ctypes.c_double), ("singular_ms", ctypes.c_double), ("lu_ms", ctypes.c_double),
+    _fields_ = [("assembly_ms", ctypes.c_double), ("singular_ms", ctypes.c_double),
+                ("regular_ms", ctypes.c_double), ("lu_ms", ctypes.c_double),
                 ("solve_ms", ctypes.c_double), ("ir_ms", ctypes.c_double), ("field_ms", ctypes.c_double),
                 ("ir_iterations", ctypes.c_int32), ("ir_converged", ctypes.c_int32),
                 ("ir_residual", ctypes.c_double), ("regular_pairs", ctypes.c_int64),
@@ -94,6 +95,8 @@ def load(path: str = LIB_PATH):
     L.beat_b200_release_workspace.restype = i32
     L.beat_b200_device_bytes.argtypes = [vp]
     L.beat_b200_device_bytes.restype = ctypes.c_int64
+    L.beat_b200_stream.argtypes = [vp]
+    L.beat_b200_stream.restype = vp
     _lib = L
     return L
 
@@ -222,3 +225,7 @@ class Context:
 
     def device_bytes(self) -> int:
         return int(self.lib.beat_b200_device_bytes(self.handle))
+
+    def stream_handle(self) -> int:
+        """cudaStream_t of this context as an integer (for torch.cuda.ExternalStream)."""
+        return int(self.lib.beat_b200_stream(self.handle) or 0)

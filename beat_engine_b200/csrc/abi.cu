@@ -106,16 +106,23 @@ void solve_core(beat_b200_ctx *c, double k, double eta, int R, const double *d_q
     } else {
         lu_precond_fp32(c, R, w.b.as<double>(), d_x);
         BB_CUDA(cudaEventRecord(c->ev[6], c->stream));
-        ir = gmres_refine(c, R, d_x, w.b.as<double>(), o.ir_restart, o.ir_max_iters, o.ir_rtol);
+        if (o.flags & BEAT_B200_FLAG_NO_REFINE)
+            ir = IrResult{0, 0, -1.0};
+        else
+            ir = gmres_refine(c, R, d_x, w.b.as<double>(), o.ir_restart, o.ir_max_iters, o.ir_rtol);
         BB_CUDA(cudaEventRecord(c->ev[7], c->stream));
     }
     BB_CUDA(cudaEventSynchronize(c->ev[7]));
+    const int st2 = read_status(c);
+    BB_REQUIRE(!(st2 & DEV_BARRIER_TIMEOUT), BEAT_B200_TIMEOUT,
+               "triangular solve: a block wait ran out of its budget");
     BB_CUDA(cudaEventElapsedTime(&ms_lu, c->ev[4], c->ev[5]));
     BB_CUDA(cudaEventElapsedTime(&ms_solve, c->ev[5], c->ev[6]));
     BB_CUDA(cudaEventElapsedTime(&ms_ir, c->ev[6], c->ev[7]));
     if (diag) {
         diag->assembly_ms = ms_asm;
         diag->singular_ms = ms_sing;
+        diag->regular_ms = c->last_regular_ms;
         diag->lu_ms = ms_lu;
         diag->solve_ms = ms_solve;
         diag->ir_ms = ms_ir;
@@ -130,7 +137,8 @@ void solve_core(beat_b200_ctx *c, double k, double eta, int R, const double *d_q
         diag->lu_split_terms = o.lu_split_terms;
         diag->reserved = 0;
     }
-    BB_REQUIRE(ir.converged || o.precision == BEAT_B200_FP64, BEAT_B200_NOT_CONVERGED,
+    BB_REQUIRE(ir.converged || o.precision == BEAT_B200_FP64 || (o.flags & BEAT_B200_FLAG_NO_REFINE),
+               BEAT_B200_NOT_CONVERGED,
                "GMRES refinement missed its tolerance (worst relative residual " + std::to_string(ir.residual) + ")");
 }
 
@@ -338,5 +346,7 @@ int32_t beat_b200_release_workspace(beat_b200_ctx *c) {
 }
 
 int64_t beat_b200_device_bytes(const beat_b200_ctx *c) { return c ? device_bytes(c) : 0; }
+
+void *beat_b200_stream(const beat_b200_ctx *c) { return c ? (void *)c->stream : nullptr; }
 
 }  // extern "C"

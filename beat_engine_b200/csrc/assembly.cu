@@ -497,6 +497,7 @@ template <typename T> static void assemble_t(beat_b200_ctx *c, double k, double 
     BB_CUDA(cudaEventRecord(c->ev[0], c->stream));
     BB_CUDA(cudaMemsetAsync(w.A.p, 0, (size_t)N * w.ld * sizeof(Cx<T>), c->stream));
     BB_CUDA(cudaMemsetAsync(w.B.p, 0, (size_t)N * F * sizeof(Cx<T>), c->stream));
+    BB_CUDA(cudaEventRecord(c->ev[8], c->stream));
     switch (c->Q) {
         case 1: launch_regular<T, 1>(c, k, eta); break;
         case 3: launch_regular<T, 3>(c, k, eta); break;
@@ -540,6 +541,7 @@ template <typename T> static void assemble_t(beat_b200_ctx *c, double k, double 
         BB_CUDA(cudaEventSynchronize(c->ev[3]));
         if (ms_total) BB_CUDA(cudaEventElapsedTime(ms_total, c->ev[0], c->ev[3]));
         if (ms_singular) BB_CUDA(cudaEventElapsedTime(ms_singular, c->ev[1], c->ev[2]));
+        BB_CUDA(cudaEventElapsedTime(&c->last_regular_ms, c->ev[8], c->ev[1]));
     }
 }
 

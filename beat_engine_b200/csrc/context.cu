@@ -516,18 +516,19 @@ void ensure_workspace(beat_b200_ctx *c, int precision, int R) {
 void release_workspace(beat_b200_ctx *c) {
     Workspace &w = c->ws;
     for (DevBuf *b : {&w.A, &w.Aop, &w.B, &w.b, &w.x, &w.ipiv, &w.perm, &w.panel_scratch, &w.stage, &w.krylov,
-                      &w.small, &w.q})
+                      &w.small, &w.q, &w.small_solve, &w.dinv})
         b->free_();
     w.precision = -1;
     w.N = w.F = w.R = 0;
     w.lu_valid = 0;
+    w.solve_epoch = 0;
 }
 
 int64_t device_bytes(const beat_b200_ctx *c) {
     int64_t s = 0;
     const Workspace &w = c->ws;
     for (const DevBuf *b : {&w.A, &w.Aop, &w.B, &w.b, &w.x, &w.ipiv, &w.perm, &w.panel_scratch, &w.stage, &w.krylov,
-                            &w.small, &w.q})
+                            &w.small, &w.q, &w.small_solve, &w.dinv})
         s += (int64_t)b->bytes;
     for (const DevBuf *b : {&c->pos_face, &c->pos_qpts64, &c->pos_qpts32, &c->pos_normal64, &c->pos_normal32,
                             &c->pos_curl64, &c->pos_curl32, &c->pos_area64, &c->pos_area32, &c->pos_gvert,

@@ -93,6 +93,9 @@ struct Workspace {
     DevBuf krylov;        // GMRES bases
     DevBuf small;         // GMRES small vectors
     DevBuf q;             // F x R FP64 Neumann data (column-major)
+    DevBuf small_solve;   // block-substitution claim counter and per-block flags
+    DevBuf dinv;          // FP64 inverses of the 64 x 64 diagonal blocks of L and U
+    int solve_epoch = 0;  // flag value of the latest substitution launch
     int lu_valid = 0;     // factors match the current operator
 };
 
@@ -150,7 +153,8 @@ struct beat_b200_ctx {
     bb::DevBuf barrier;           // grid-barrier counters
     bb::Workspace ws;
 
-    cudaEvent_t ev[8] = {};
+    cudaEvent_t ev[10] = {};
+    float last_regular_ms = 0.f;
 };
 
 namespace bb {

@@ -427,13 +427,7 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
     }
 }
 
-void lu_factor(beat_b200_ctx *c, int precision, int nb, int split_terms) {
-    if (precision == BEAT_B200_FP64)
-        lu_factor_t<double>(c, nb, split_terms);
-    else
-        lu_factor_t<float>(c, nb, split_terms);
-    c->ws.lu_valid = 1;
-}
+
 
 // ---------------------------------------------------------------------------
 // triangular solves with R right-hand sides (X column-major N x R, FP64)
@@ -445,91 +439,162 @@ __global__ void permute_rows_kernel(const double2 *in, double2 *out, const int *
     for (int r = 0; r < R; ++r) out[(size_t)r * n + i] = in[(size_t)r * n + src];
 }
 
-constexpr int SB = 64;  // solve block
-// solve the diagonal block [kb, kb+bs) in place (unit lower or upper)
-template <typename T, bool LOWER>
-__global__ void __launch_bounds__(256) diag_solve_kernel(const Cx<T> *A, int64_t ld, int n, int kb, int bs,
-                                                         double2 *X, int R) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    Cx<double>(*D)[SB + 1] = reinterpret_cast<Cx<double>(*)[SB + 1]>(smem_raw);
-    Cx<double>(*Y)[17] = reinterpret_cast<Cx<double>(*)[17]>(smem_raw + sizeof(Cx<double>) * SB * (SB + 1));
-    const int r0 = blockIdx.x * 16;
-    const int rc = min(16, R - r0);
-    for (int i = threadIdx.x; i < bs * bs; i += blockDim.x) {
-        const int a = i / bs, b = i % bs;
-        const Cx<T> v = A[(int64_t)(kb + a) * ld + kb + b];
-        D[a][b] = Cx<double>{(double)v.re, (double)v.im};
-    }
-    for (int i = threadIdx.x; i < bs * 16; i += blockDim.x) {
-        const int a = i / 16, r = i % 16;
-        const double2 v = r < rc ? X[(size_t)(r0 + r) * n + kb + a] : make_double2(0, 0);
-        Y[a][r] = Cx<double>{v.x, v.y};
-    }
-    __syncthreads();
-    const int r = threadIdx.x;  // one thread per RHS column
-    if (r < 16) {
-        if (LOWER) {
-            for (int j = 0; j < bs; ++j) {
-                const Cx<double> y = Y[j][r];
-                for (int i = j + 1; i < bs; ++i) {
-                    const Cx<double> l = D[i][j];
-                    Y[i][r].re -= l.re * y.re - l.im * y.im;
-                    Y[i][r].im -= l.re * y.im + l.im * y.re;
-                }
-            }
-        } else {
-            for (int j = bs - 1; j >= 0; --j) {
-                const Cx<double> u = D[j][j];
-                const double den = u.re * u.re + u.im * u.im;
-                const Cx<double> v = Y[j][r];
-                const Cx<double> y = {(v.re * u.re + v.im * u.im) / den, (v.im * u.re - v.re * u.im) / den};
-                Y[j][r] = y;
-                for (int i = 0; i < j; ++i) {
-                    const Cx<double> l = D[i][j];
-                    Y[i][r].re -= l.re * y.re - l.im * y.im;
-                    Y[i][r].im -= l.re * y.im + l.im * y.re;
-                }
-            }
-        }
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < bs * 16; i += blockDim.x) {
-        const int a = i / 16, rr = i % 16;
-        if (rr < rc) X[(size_t)(r0 + rr) * n + kb + a] = make_double2(Y[a][rr].re, Y[a][rr].im);
-    }
+// Block substitution in one kernel.  The solution is cut into 64-row blocks;
+// each CTA claims the next block from a counter (so it only ever waits on
+// blocks already claimed by running CTAs), folds in L_bj X_j (or U_bj X_j)
+// for every finished block j as its flag appears, solves its diagonal block
+// and publishes X_b with a flag.  Waits are bounded: on expiry the kernel sets
+// a status bit and continues, so it always terminates.
+constexpr int SB = 64, SRC = 16, SOLVE_THREADS = 256, SBP = SB + 1;
+
+template <typename T> __device__ __forceinline__ Cx<double> to_d(Cx<T> v) {
+    return Cx<double>{(double)v.re, (double)v.im};
 }
 
-// X[rows] -= A[rows, kb:kb+bs] X[kb:kb+bs]; 16 rows per CTA, 16 RHS per CTA
+// Inverse of every 64 x 64 diagonal block of L (unit lower, blockIdx.y = 0)
+// and U (upper, blockIdx.y = 1), FP64, one CTA per block: column c of the
+// inverse by substitution on e_c (64 threads, one column each).
 template <typename T>
-__global__ void __launch_bounds__(256) block_update_kernel(const Cx<T> *A, int64_t ld, int n, int kb, int bs,
-                                                           int row_begin, int row_end, double2 *X, int R) {
-    __shared__ Cx<double> Lt[16][SB + 1];
-    __shared__ Cx<double> Y[SB][17];
-    const int i0 = row_begin + blockIdx.x * 16, r0 = blockIdx.y * 16;
-    const int rc = min(16, R - r0);
-    for (int i = threadIdx.x; i < 16 * bs; i += blockDim.x) {
-        const int a = i / bs, b = i % bs;
-        Cx<T> v = (i0 + a < row_end) ? A[(int64_t)(i0 + a) * ld + kb + b] : Cx<T>{T(0), T(0)};
-        Lt[a][b] = Cx<double>{(double)v.re, (double)v.im};
+__global__ void __launch_bounds__(SB) diag_inverse_kernel(const Cx<T> *A, int64_t ld, int n, Cx<double> *Dinv) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cx<double>(*D)[SBP] = reinterpret_cast<Cx<double>(*)[SBP]>(smem_raw);
+    Cx<double>(*X)[SBP] = reinterpret_cast<Cx<double>(*)[SBP]>(smem_raw + sizeof(Cx<double>) * SB * SBP);
+    const int b = blockIdx.x, upper = blockIdx.y;
+    const int rb = b * SB, rows = min(SB, n - rb), c = threadIdx.x;
+    for (int i = 0; i < SB; ++i)
+        D[i][c] = (i < rows && c < rows) ? to_d(A[(int64_t)(rb + i) * ld + rb + c]) : Cx<double>{i == c ? 1.0 : 0.0, 0.0};
+    __syncthreads();
+    if (!upper) {
+        for (int i = 0; i < SB; ++i) {
+            Cx<double> s{i == c ? 1.0 : 0.0, 0.0};
+            for (int q = 0; q < i; ++q) {
+                const Cx<double> l = D[i][q], x = X[q][c];
+                s.re -= l.re * x.re - l.im * x.im;
+                s.im -= l.re * x.im + l.im * x.re;
+            }
+            X[i][c] = s;
+        }
+    } else {
+        for (int i = SB - 1; i >= 0; --i) {
+            Cx<double> s{i == c ? 1.0 : 0.0, 0.0};
+            for (int q = i + 1; q < SB; ++q) {
+                const Cx<double> u = D[i][q], x = X[q][c];
+                s.re -= u.re * x.re - u.im * x.im;
+                s.im -= u.re * x.im + u.im * x.re;
+            }
+            const Cx<double> u = D[i][i];
+            const double den = u.re * u.re + u.im * u.im;
+            X[i][c] = den > 0 ? Cx<double>{(s.re * u.re + s.im * u.im) / den, (s.im * u.re - s.re * u.im) / den}
+                              : Cx<double>{0.0, 0.0};
+        }
     }
-    for (int i = threadIdx.x; i < bs * 16; i += blockDim.x) {
-        const int a = i / 16, r = i % 16;
-        const double2 v = r < rc ? X[(size_t)(r0 + r) * n + kb + a] : make_double2(0, 0);
-        Y[a][r] = Cx<double>{v.x, v.y};
+    Cx<double> *out = Dinv + ((size_t)upper * gridDim.x + b) * SB * SB;
+    for (int i = 0; i < SB; ++i) out[i * SB + c] = X[i][c];
+}
+
+// Block substitution in one kernel.  The solution is cut into 64-row blocks;
+// each CTA claims the next block from a counter (so it only ever waits on
+// blocks already claimed by running CTAs), folds in L_bj X_j (or U_bj X_j)
+// for every finished block j as its flag appears, applies the inverted
+// diagonal block and publishes X_b with a flag.  Waits are bounded: on expiry
+// the kernel sets a status bit and continues, so it always terminates.
+template <typename T, bool LOWER>
+__global__ void __launch_bounds__(SOLVE_THREADS) block_subst_kernel(const Cx<T> *A, int64_t ld, int n,
+                                                                    const Cx<double> *Dinv, double2 *X, int R,
+                                                                    int r0, int *counter, int *flags, int epoch,
+                                                                    int *status, unsigned spin_limit) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cx<double> *Lt = reinterpret_cast<Cx<double> *>(smem_raw);  // SB x SBP
+    Cx<double> *Xj = Lt + SB * SBP;                               // SB x SRC
+    __shared__ int s_blk;
+    const int nblk = (n + SB - 1) / SB;
+    if (threadIdx.x == 0) s_blk = atomicAdd(counter, 1);
+    __syncthreads();
+    const int claim = s_blk;
+    if (claim >= nblk) return;
+    const int b = LOWER ? claim : nblk - 1 - claim;
+    const int rb = b * SB, rows = min(SB, n - rb);
+    const int rc = min(SRC, R - r0);
+    const int r = threadIdx.x >> 2, cg = (threadIdx.x & 3) * 4;  // row, first of 4 columns
+    double ar[4] = {0, 0, 0, 0}, ai[4] = {0, 0, 0, 0};
+    for (int step = 0; step < claim; ++step) {
+        const int j = LOWER ? step : nblk - 1 - step;  // dependencies in the order they finish
+        const int cj = j * SB, cols = min(SB, n - cj);
+        // the L tile does not depend on the wait: load it first
+        for (int i = threadIdx.x; i < SB * SB; i += SOLVE_THREADS) {
+            const int a = i / SB, q = i % SB;
+            Lt[a * SBP + q] = (a < rows && q < cols) ? to_d(A[(int64_t)(rb + a) * ld + cj + q]) : Cx<double>{0.0, 0.0};
+        }
+        if (threadIdx.x == 0) {
+            unsigned it = 0;
+            while (true) {
+                int v;
+                asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(flags + j) : "memory");
+                if (v == epoch) break;
+                if ((*(volatile int *)status & DEV_BARRIER_TIMEOUT) || ++it > spin_limit) {
+                    atomicOr(status, (int)DEV_BARRIER_TIMEOUT);
+                    break;
+                }
+                __nanosleep(20);
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < SB * SRC; i += SOLVE_THREADS) {
+            const int q = i / SB, a = i % SB;  // consecutive threads: consecutive rows of one column
+            double2 v = make_double2(0, 0);
+            if (a < cols && q < rc) v = __ldcg(&X[(size_t)(r0 + q) * n + cj + a]);
+            Xj[a * SRC + q] = Cx<double>{v.x, v.y};
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int q = 0; q < SB; ++q) {
+            const Cx<double> l = Lt[r * SBP + q];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const Cx<double> x = Xj[q * SRC + cg + e];
+                ar[e] += l.re * x.re - l.im * x.im;
+                ai[e] += l.re * x.im + l.im * x.re;
+            }
+        }
+        __syncthreads();
+    }
+    // Y = B_b - acc;  X_b = inv(D_bb) Y
+    const Cx<double> *Di = Dinv + ((size_t)(LOWER ? 0 : 1) * nblk + b) * SB * SB;
+    for (int i = threadIdx.x; i < SB * SB; i += SOLVE_THREADS) Lt[(i / SB) * SBP + i % SB] = Di[i];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        double2 v = make_double2(0, 0);
+        if (r < rows && cg + e < rc) v = X[(size_t)(r0 + cg + e) * n + rb + r];
+        Xj[r * SRC + cg + e] = Cx<double>{v.x - ar[e], v.y - ai[e]};
     }
     __syncthreads();
-    const int a = threadIdx.x >> 4, r = threadIdx.x & 15;
-    if (i0 + a < row_end && r < rc) {
-        double sr = 0, si = 0;
-        for (int b = 0; b < bs; ++b) {
-            const Cx<double> l = Lt[a][b], y = Y[b][r];
-            sr += l.re * y.re - l.im * y.im;
-            si += l.re * y.im + l.im * y.re;
+    double xr[4] = {0, 0, 0, 0}, xi[4] = {0, 0, 0, 0};
+#pragma unroll 8
+    for (int q = 0; q < SB; ++q) {
+        const Cx<double> d = Lt[r * SBP + q];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const Cx<double> y = Xj[q * SRC + cg + e];
+            xr[e] += d.re * y.re - d.im * y.im;
+            xi[e] += d.re * y.im + d.im * y.re;
         }
-        double2 &d = X[(size_t)(r0 + r) * n + i0 + a];
-        d.x -= sr;
-        d.y -= si;
     }
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+        if (r < rows && cg + e < rc) X[(size_t)(r0 + cg + e) * n + rb + r] = make_double2(xr[e], xi[e]);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(flags + b), "r"(epoch) : "memory");
+}
+
+template <typename T> static void diag_inverses(beat_b200_ctx *c) {
+    Workspace &w = c->ws;
+    const int n = c->V, nblk = (n + SB - 1) / SB;
+    w.dinv.alloc(sizeof(Cx<double>) * 2 * (size_t)nblk * SB * SB);
+    const size_t smem = 2 * sizeof(Cx<double>) * SB * SBP;
+    BB_CUDA(cudaFuncSetAttribute(diag_inverse_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    diag_inverse_kernel<T><<<dim3(nblk, 2), SB, smem, c->stream>>>(w.A.as<Cx<T>>(), w.ld, n, w.dinv.as<Cx<double>>());
+    BB_CUDA(cudaGetLastError());
 }
 
 template <typename T> static void lu_solve_t(beat_b200_ctx *c, int R, const double *in, double *out) {
@@ -537,29 +602,42 @@ template <typename T> static void lu_solve_t(beat_b200_ctx *c, int R, const doub
     const int n = c->V;
     const Cx<T> *A = w.A.as<Cx<T>>();
     double2 *X = reinterpret_cast<double2 *>(out);
-    const size_t dsm = sizeof(Cx<double>) * (SB * (SB + 1) + SB * 17);
-    BB_CUDA(cudaFuncSetAttribute(diag_solve_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
-    BB_CUDA(cudaFuncSetAttribute(diag_solve_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
+    const int nblk = (n + SB - 1) / SB;
+    // counters: [0] claim counter, then nblk flags
+    w.small_solve.alloc(sizeof(int) * (size_t)(nblk + 64));
+    int *counter = w.small_solve.as<int>();
+    int *flags = counter + 32;
+    if (w.solve_epoch == 0) BB_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * nblk, c->stream));
+    const size_t smem = sizeof(Cx<double>) * (SB * SBP + SB * SRC);
+    BB_CUDA(cudaFuncSetAttribute(block_subst_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    BB_CUDA(cudaFuncSetAttribute(block_subst_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     permute_rows_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(reinterpret_cast<const double2 *>(in), X,
                                                                 w.perm.as<int>(), n, R);
-    const int rg = (R + 15) / 16;
-    for (int kb = 0; kb < n; kb += SB) {
-        const int bs = std::min(SB, n - kb);
-        diag_solve_kernel<T, true><<<rg, 256, dsm, c->stream>>>(A, w.ld, n, kb, bs, X, R);
-        if (kb + bs < n) {
-            dim3 grid((n - kb - bs + 15) / 16, rg);
-            block_update_kernel<T><<<grid, 256, 0, c->stream>>>(A, w.ld, n, kb, bs, kb + bs, n, X, R);
-        }
-    }
-    for (int kb = ((n - 1) / SB) * SB; kb >= 0; kb -= SB) {
-        const int bs = std::min(SB, n - kb);
-        diag_solve_kernel<T, false><<<rg, 256, dsm, c->stream>>>(A, w.ld, n, kb, bs, X, R);
-        if (kb > 0) {
-            dim3 grid((kb + 15) / 16, rg);
-            block_update_kernel<T><<<grid, 256, 0, c->stream>>>(A, w.ld, n, kb, bs, 0, kb, X, R);
+    const Cx<double> *Dinv = w.dinv.as<Cx<double>>();
+    for (int r0 = 0; r0 < R; r0 += SRC) {
+        for (int pass = 0; pass < 2; ++pass) {
+            const int epoch = ++w.solve_epoch;
+            BB_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), c->stream));
+            if (pass == 0)
+                block_subst_kernel<T, true><<<nblk, SOLVE_THREADS, smem, c->stream>>>(
+                    A, w.ld, n, Dinv, X, R, r0, counter, flags, epoch, c->status.as<int>(), 1u << 22);
+            else
+                block_subst_kernel<T, false><<<nblk, SOLVE_THREADS, smem, c->stream>>>(
+                    A, w.ld, n, Dinv, X, R, r0, counter, flags, epoch, c->status.as<int>(), 1u << 22);
         }
     }
     BB_CUDA(cudaGetLastError());
+}
+
+void lu_factor(beat_b200_ctx *c, int precision, int nb, int split_terms) {
+    if (precision == BEAT_B200_FP64) {
+        lu_factor_t<double>(c, nb, split_terms);
+        diag_inverses<double>(c);
+    } else {
+        lu_factor_t<float>(c, nb, split_terms);
+        diag_inverses<float>(c);
+    }
+    c->ws.lu_valid = 1;
 }
 
 void lu_solve_fp64(beat_b200_ctx *c, int R, double *x_dev) {

@@ -62,12 +62,17 @@ typedef struct {
     int32_t lu_split_terms; /* TF32 products per trailing update: 1 or 3 (3) */
     double ir_rtol;         /* relative residual target of the refinement (1e-10) */
     int32_t lu_block;       /* LU panel width; 0 = tuned default */
-    int32_t flags;          /* reserved, pass 0 */
+    int32_t flags;          /* BEAT_B200_FLAG_* bits, 0 by default */
 } beat_b200_opts;
+
+/* opts.flags: return the mixed form's direct FP32-LU solution without the
+ * GMRES refinement (diagnostics; the result is then FP32-LU accurate only) */
+#define BEAT_B200_FLAG_NO_REFINE 1
 
 typedef struct {
     double assembly_ms;     /* regular + singular + identity + RHS */
     double singular_ms;     /* Duffy pass alone (part of assembly_ms) */
+    double regular_ms;      /* element-pair kernel alone (part of assembly_ms) */
     double lu_ms;
     double solve_ms;        /* triangular solves of the direct solve */
     double ir_ms;           /* GMRES refinement (mixed form) */
@@ -141,6 +146,11 @@ int32_t beat_b200_release_workspace(beat_b200_ctx *ctx);
 
 /* Bytes of device memory the context holds right now. */
 int64_t beat_b200_device_bytes(const beat_b200_ctx *ctx);
+
+/* The CUDA stream (cudaStream_t) every kernel of this context is launched
+ * on, so a caller can order its own work or record timing events on it.
+ * Entry points return only after their work on it has completed. */
+void *beat_b200_stream(const beat_b200_ctx *ctx);
 
 #ifdef __cplusplus
 }

@@ -222,3 +222,32 @@ def test_errors_are_status_codes():
         with pytest.raises(_lib.BeatB200Error) as e:
             c.solve(0.0, 0.0, np.ones(4, complex))
         assert e.value.status == _lib.INVALID_ARG
+
+
+@pytest.mark.parametrize("split,tol", [(3, 2e-5), (1, 5e-3)])
+def test_fp32_tensor_core_lu_direct_solution(ctx3, sphere3, split, tol):
+    """The FP32 LU (tcgen05 TF32 trailing updates) before refinement: with 3
+    split products it is FP32-accurate; with 1 it is TF32-accurate."""
+    k = 36.6
+    q = random_q(sphere3.num_faces, 3, 50)
+    opts = _lib.Context.opts(_lib.MIXED_FP32_IR, lu_split_terms=split, flags=1)
+    p, d = ctx3.solve(k, 1 / k, q, opts)
+    Ao, bo = oracle.assemble(sphere3, k, 1 / k, q)
+    err = col_rel(p, oracle.lu_solve(Ao, bo))
+    assert np.all(err <= tol), err
+
+
+def test_larger_mesh_fp64_and_mixed_against_lapack():
+    """2,562 unknowns (several LU panels and partial tensor-core tiles)."""
+    scipy_linalg = pytest.importorskip("scipy.linalg")
+    mesh = M.reference_sphere(0.1, 4)
+    k = 2 * math.pi * 2000 / 343.0
+    q = random_q(mesh.num_faces, 16, 60)
+    Ao, bo = oracle.assemble(mesh, k, 1 / k, q)
+    po = scipy_linalg.lu_solve(scipy_linalg.lu_factor(Ao), bo)
+    with _lib.Context(0) as c:
+        c.set_mesh(mesh.vertices, mesh.faces)
+        p64, _ = c.solve(k, 1 / k, q, _lib.Context.opts(_lib.FP64))
+        pmx, d = c.solve(k, 1 / k, q, _lib.Context.opts(_lib.MIXED_FP32_IR))
+    assert np.all(col_rel(p64, po) <= 1e-10)
+    assert np.all(col_rel(pmx, po) <= 1e-6) and d["ir_converged"] == 1
