@@ -30,7 +30,7 @@ def needs_build() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, s) for s in SOURCES] + [os.path.join(CSRC, "internal.cuh"),
+    deps = [os.path.join(CSRC, s) for s in SOURCES] + [os.path.join(CSRC, "internal.cuh"), os.path.join(CSRC, "phase.cuh"),
                                                         os.path.join(HERE, "..", "include", "beat_b200.h")]
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 

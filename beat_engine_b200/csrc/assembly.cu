@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include "internal.cuh"
+#include "phase.cuh"
 
 namespace bb {
 
@@ -69,8 +70,8 @@ void upload_rule_tables(const std::vector<double> &pts, const std::vector<double
     BB_CUDA(cudaMemcpyToSymbol(c_rb32, b32, sizeof(b32)));
 }
 
-__device__ __forceinline__ void sincos_t(double x, double *s, double *c) { sincos(x, s, c); }
-__device__ __forceinline__ void sincos_t(float x, float *s, float *c) { sincosf(x, s, c); }
+__device__ __forceinline__ void sincos_t(double x, double *s, double *c) { sincos_cw(x, s, c); }
+__device__ __forceinline__ void sincos_t(float x, float *s, float *c) { sincos_cw(x, s, c); }
 __device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
 __device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
 
@@ -102,7 +103,7 @@ template <typename T> struct RegArgs {
 
 // Element-pair kernel.  grid = (trial tiles, test tiles), 256 threads.
 template <typename T, int Q>
-__global__ void __launch_bounds__(REG_THREADS) regular_pairs_kernel(RegArgs<T> g) {
+__global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_pairs_kernel(RegArgs<T> g) {
     constexpr int RI = Q == 1 ? 0 : Q == 3 ? 1 : 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cx<T> *sA = reinterpret_cast<Cx<T> *>(smem_raw);  // VT x VS
@@ -321,7 +322,7 @@ __global__ void __launch_bounds__(256) singular_pairs_kernel(SingArgs<T> g) {
         if (r2 == 0.0) continue;
         const double rad = sqrt(r2), ir = 1.0 / rad;
         double sn_, cs_;
-        sincos(k * rad, &sn_, &cs_);
+        sincos_cw(k * rad, &sn_, &cs_);
         const double scl = ir * (0.07957747154594767 * w);
         const double gr = cs_ * scl, gi = sn_ * scl;
         const double gsr = -gr * ir - gi * k, gsi = gr * k - gi * ir;
@@ -418,10 +419,13 @@ __global__ void __launch_bounds__(256) rhs_apply_kernel(const Cx<T> *B, int N, i
     for (int r = 0; r < BQ_RC; ++r) ar[r] = ai[r] = 0.0;
     for (int f0 = 0; f0 < F; f0 += BQ_CHUNK) {
         __syncthreads();
-        for (int i = threadIdx.x; i < BQ_RC * BQ_CHUNK; i += blockDim.x) {
-            const int r = i / BQ_CHUNK, f = f0 + i % BQ_CHUNK;
-            sq[r][i % BQ_CHUNK] = (r < rc && f < F) ? q[(size_t)(r0 + r) * F + f] : Cx<double>{0.0, 0.0};
-        }
+        batched_copy<256, 8, Cx<double>>(
+            BQ_RC * BQ_CHUNK,
+            [&](int i) {
+                const int r = i / BQ_CHUNK, f = f0 + i % BQ_CHUNK;
+                return (r < rc && f < F) ? q[(size_t)(r0 + r) * F + f] : Cx<double>{0.0, 0.0};
+            },
+            [&](int i, Cx<double> v) { sq[i / BQ_CHUNK][i % BQ_CHUNK] = v; });
         __syncthreads();
         if (row < N) {
             for (int j = lane; j < BQ_CHUNK && f0 + j < F; j += 32) {

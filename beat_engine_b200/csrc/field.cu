@@ -20,6 +20,7 @@
 #include <cmath>
 
 #include "internal.cuh"
+#include "phase.cuh"
 
 namespace bb {
 
@@ -100,7 +101,7 @@ __global__ void __launch_bounds__(FLD_THREADS) field_eval_kernel(const double *p
                 if (rad == 0.0) continue;
                 const double ir = 1.0 / rad;
                 double sn_, cs_;
-                sincos(k * rad, &sn_, &cs_);
+                sincos_cw(k * rad, &sn_, &cs_);
                 gr = cs_ * inv4pi * ir;
                 gi = sn_ * inv4pi * ir;
                 const double proj = (rx * sn[j][0] + ry * sn[j][1] + rz * sn[j][2]) * ir;
@@ -110,7 +111,7 @@ __global__ void __launch_bounds__(FLD_THREADS) field_eval_kernel(const double *p
             } else {
                 const double ph = -k * (x0 * sy[j][0] + x1 * sy[j][1] + x2 * sy[j][2]);
                 double sn_, cs_;
-                sincos(ph, &sn_, &cs_);
+                sincos_cw(ph, &sn_, &cs_);
                 gr = cs_ * inv4pi;
                 gi = sn_ * inv4pi;
                 const double dn = x0 * sn[j][0] + x1 * sn[j][1] + x2 * sn[j][2];

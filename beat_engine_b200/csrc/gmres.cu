@@ -39,10 +39,13 @@ __global__ void __launch_bounds__(256) matvec_kernel(const Cx<T> *A, int64_t ld,
         for (int r = 0; r < MV_RC; ++r) ar[a][r] = ai[a][r] = 0.0;
     for (int j0 = 0; j0 < n; j0 += MV_CHUNK) {
         __syncthreads();
-        for (int i = threadIdx.x; i < MV_RC * MV_CHUNK; i += blockDim.x) {
-            const int r = i / MV_CHUNK, j = j0 + i % MV_CHUNK;
-            sx[r][i % MV_CHUNK] = (r < rc && j < n) ? X[(size_t)(r0 + r) * n + j] : make_double2(0, 0);
-        }
+        batched_copy<256, 8, double2>(
+            MV_RC * MV_CHUNK,
+            [&](int i) {
+                const int r = i / MV_CHUNK, j = j0 + i % MV_CHUNK;
+                return (r < rc && j < n) ? X[(size_t)(r0 + r) * n + j] : make_double2(0, 0);
+            },
+            [&](int i, double2 v) { sx[i / MV_CHUNK][i % MV_CHUNK] = v; });
         __syncthreads();
         for (int jj = lane; jj < MV_CHUNK && j0 + jj < n; jj += 32) {
 #pragma unroll

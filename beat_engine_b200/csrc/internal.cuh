@@ -64,6 +64,29 @@ template <typename T> __host__ __device__ __forceinline__ Cx<T> cmul(Cx<T> a, Cx
     return Cx<T>{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
 }
 
+#ifdef __CUDACC__
+// Cooperative copy of `total` items by NT threads, BATCH loads in flight per
+// thread before any store: load(i) returns item i, store(i, v) writes it.
+// (A plain `for (i = tid; ...) dst = src` loop waits for each load before the
+// next one is issued when the store may alias the source.)
+template <int NT, int BATCH, typename V, typename Load, typename Store>
+__device__ __forceinline__ void batched_copy(int total, Load load, Store store) {
+    for (int base = 0; base < total; base += NT * BATCH) {
+        V v[BATCH];
+#pragma unroll
+        for (int u = 0; u < BATCH; ++u) {
+            const int i = base + u * NT + (int)threadIdx.x;
+            if (i < total) v[u] = load(i);
+        }
+#pragma unroll
+        for (int u = 0; u < BATCH; ++u) {
+            const int i = base + u * NT + (int)threadIdx.x;
+            if (i < total) store(i, v[u]);
+        }
+    }
+}
+#endif
+
 // ---------------------------------------------------------------------------
 // mesh-derived tables for the element-pair kernel
 // ---------------------------------------------------------------------------

@@ -13,9 +13,10 @@
 // Per panel of nb columns:
 //   1. panel_kernel: a cooperative kernel; the panel rows are split over the
 //      CTAs and held in shared memory.  Per column every CTA publishes its
-//      best candidate row, one grid barrier, every CTA picks the same winner,
-//      swaps and eliminates locally.  Candidate slots are double-buffered by
-//      column parity so one barrier per column suffices.
+//      best candidate row and record, passes one grid-wide barrier (an
+//      arrival counter), reads all records at once, picks the same winner,
+//      swaps and eliminates locally.  Slots are double-buffered by column
+//      parity so one barrier per column suffices.
 //   2. laswp_kernel: the panel's interchanges on all other columns (and on
 //      the running row permutation).
 //   3. trsm_kernel: U12 = L11^-1 A12.
@@ -31,30 +32,10 @@
 
 namespace bb {
 
-// device-side wait with a budget; gives up by setting a status bit
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
     unsigned v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
-}
-
-__device__ __forceinline__ void grid_barrier(unsigned *ctr, unsigned target, int *status, unsigned limit) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        atomicAdd(ctr, 1u);
-        unsigned it = 0;
-        while (ld_acquire_u32(ctr) < target) {
-            if (*(volatile int *)status & DEV_BARRIER_TIMEOUT) break;
-            if (++it > limit) {
-                atomicOr(status, (int)DEV_BARRIER_TIMEOUT);
-                break;
-            }
-            __nanosleep(64);
-        }
-        __threadfence();
-    }
-    __syncthreads();
 }
 
 template <typename T> __device__ __forceinline__ T cabs1(Cx<T> v) { return fabs(v.re) + fabs(v.im); }
@@ -72,6 +53,13 @@ __device__ __forceinline__ double ldcg(const double *p) { return __ldcg(p); }
 __device__ __forceinline__ float ldcg(const float *p) { return __ldcg(p); }
 __device__ __forceinline__ int ldcg(const int *p) { return __ldcg(p); }
 
+// Pivot candidate of one CTA for one column (value |re| + |im| and global row).
+struct PivotRec {
+    double val;
+    int idx;
+    int pad;
+};
+
 template <typename T> struct PanelArgs {
     Cx<T> *A;
     int64_t ld;
@@ -80,9 +68,8 @@ template <typename T> struct PanelArgs {
     int *ipiv;
     Cx<T> *pub_rows;    // [2][G][nb]
     Cx<T> *pub_diag;    // [2][nb]
-    T *pub_val;         // [2][G]
-    int *pub_idx;       // [2][G]
-    unsigned *barrier;
+    PivotRec *recs;     // [2][G]
+    unsigned *counter;  // grid-barrier arrivals of this panel launch (zeroed before it)
     int *status;
     unsigned spin_limit;
 };
@@ -98,15 +85,15 @@ template <typename T> __global__ void __launch_bounds__(PANEL_THREADS) panel_ker
     Cx<T> *lcol = drow + nb;                          // rpc
     __shared__ T red_v[PANEL_THREADS / 32];
     __shared__ int red_i[PANEL_THREADS / 32];
+    __shared__ int red_c[PANEL_THREADS / 32];
     __shared__ int s_piv;
     __shared__ T s_pv;
 
     const int gr0 = a.k + cta * a.rpc;
     const int nrows = max(0, min(a.rpc, a.n - gr0));
-    for (int i = tid; i < nrows * nb; i += PANEL_THREADS) {
-        const int r = i / nb, c = i % nb;
-        P[i] = a.A[(int64_t)(gr0 + r) * a.ld + a.k + c];
-    }
+    batched_copy<PANEL_THREADS, 8, Cx<T>>(
+        nrows * nb, [&](int i) { return a.A[(int64_t)(gr0 + i / nb) * a.ld + a.k + i % nb]; },
+        [&](int i, Cx<T> v) { P[i] = v; });
     __syncthreads();
 
     for (int j = 0; j < nb && a.k + j < a.n; ++j) {
@@ -142,9 +129,8 @@ template <typename T> __global__ void __launch_bounds__(PANEL_THREADS) panel_ker
                     bv = red_v[w];
                     bi = red_i[w];
                 }
-            a.pub_val[par * G + cta] = bv;
-            a.pub_idx[par * G + cta] = bi;
             s_piv = bi;
+            s_pv = bv;
         }
         __syncthreads();
         const int mine = s_piv;
@@ -153,20 +139,37 @@ template <typename T> __global__ void __launch_bounds__(PANEL_THREADS) panel_ker
                 a.pub_rows[((size_t)par * G + cta) * nb + c] = P[(mine - gr0) * nb + c];
         if (jr >= gr0 && jr < gr0 + nrows)
             for (int c = tid; c < nb; c += PANEL_THREADS) a.pub_diag[(size_t)par * nb + c] = P[(jr - gr0) * nb + c];
-        grid_barrier(a.barrier, (unsigned)(j + 1) * G, a.status, a.spin_limit);
-
-        // every CTA picks the same winner
-        if (tid < 32) {
+        __syncthreads();
+        // candidate record, then one grid-wide barrier: each CTA adds one
+        // arrival (release) and waits until all G arrivals of this column are in
+        if (tid == 0) {
+            PivotRec *rec = &a.recs[par * G + cta];
+            rec->val = (double)s_pv;
+            rec->idx = mine;
+            __threadfence();
+            asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(a.counter), "r"(1u) : "memory");
+            const unsigned target = (unsigned)(j + 1) * (unsigned)G;
+            unsigned it = 0;
+            while (true) {
+                unsigned v;
+                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(a.counter) : "memory");
+                if (v >= target) break;
+                if ((*(volatile int *)a.status & DEV_BARRIER_TIMEOUT) || ++it > a.spin_limit) {
+                    atomicOr(a.status, (int)DEV_BARRIER_TIMEOUT);
+                    break;
+                }
+            }
+        }
+        __syncthreads();
+        // every CTA reads all G records at once and picks the same winner
+        {
             T wv = T(-1);
             int wi = -1, wc = -1;
-            for (int g = tid; g < G; g += 32) {
-                const T v = ldcg(&a.pub_val[par * G + g]);
-                const int i = ldcg(&a.pub_idx[par * G + g]);
-                if (i >= 0 && (v > wv || (v == wv && (wi < 0 || i < wi)))) {
-                    wv = v;
-                    wi = i;
-                    wc = g;
-                }
+            if (tid < G) {
+                const PivotRec *rec = &a.recs[par * G + tid];
+                wi = __ldcg(&rec->idx);
+                wv = wi >= 0 ? (T)__ldcg(&rec->val) : T(-1);
+                wc = tid;
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
@@ -179,7 +182,19 @@ template <typename T> __global__ void __launch_bounds__(PANEL_THREADS) panel_ker
                     wc = oc;
                 }
             }
+            if ((tid & 31) == 0) {
+                red_v[tid >> 5] = wv;
+                red_i[tid >> 5] = wi;
+                red_c[tid >> 5] = wc;
+            }
+            __syncthreads();
             if (tid == 0) {
+                for (int w = 1; w < PANEL_THREADS / 32; ++w)
+                    if (red_i[w] >= 0 && (red_v[w] > wv || (red_v[w] == wv && (wi < 0 || red_i[w] < wi)))) {
+                        wv = red_v[w];
+                        wi = red_i[w];
+                        wc = red_c[w];
+                    }
                 s_piv = wi < 0 ? jr : wi;
                 s_pv = wv;
                 red_i[0] = wc;
@@ -272,14 +287,16 @@ template <typename T> __global__ void __launch_bounds__(256) trsm_kernel(Cx<T> *
     const int c0 = k + nb + blockIdx.x * TRSM_COLS;
     const int nc = min(TRSM_COLS, n - c0);
     const int kb = min(nb, n - k);
-    for (int i = threadIdx.x; i < kb * kb; i += blockDim.x) {
-        const int r = i / kb, c = i % kb;
-        L[r * nb + c] = A[(int64_t)(k + r) * ld + k + c];
-    }
-    for (int i = threadIdx.x; i < kb * TRSM_COLS; i += blockDim.x) {
-        const int r = i / TRSM_COLS, c = i % TRSM_COLS;
-        X[r * TRSM_COLS + c] = c < nc ? A[(int64_t)(k + r) * ld + c0 + c] : Cx<T>{T(0), T(0)};
-    }
+    batched_copy<256, 16, Cx<T>>(
+        kb * kb, [&](int i) { return A[(int64_t)(k + i / kb) * ld + k + i % kb]; },
+        [&](int i, Cx<T> v) { L[(i / kb) * nb + i % kb] = v; });
+    batched_copy<256, 8, Cx<T>>(
+        kb * TRSM_COLS,
+        [&](int i) {
+            const int c = i % TRSM_COLS;
+            return c < nc ? A[(int64_t)(k + i / TRSM_COLS) * ld + c0 + c] : Cx<T>{T(0), T(0)};
+        },
+        [&](int i, Cx<T> v) { X[i] = v; });
     __syncthreads();
     for (int j = 0; j < kb - 1; ++j) {
         for (int idx = threadIdx.x; idx < (kb - 1 - j) * TRSM_COLS; idx += blockDim.x) {
@@ -304,7 +321,7 @@ template <typename T> __global__ void __launch_bounds__(256) trsm_kernel(Cx<T> *
 // ---------------------------------------------------------------------------
 constexpr int GT = 64, GKC = 16;
 template <typename T>
-__global__ void __launch_bounds__(256) gemm_update_kernel(Cx<T> *A, int64_t ld, int n, int k, int kk, int row0,
+__global__ void __launch_bounds__(256, 2) gemm_update_kernel(Cx<T> *A, int64_t ld, int n, int k, int kk, int row0,
                                                           int col0) {
     __shared__ Cx<T> sL[GKC][GT + 1];
     __shared__ Cx<T> sU[GKC][GT];
@@ -316,13 +333,23 @@ __global__ void __launch_bounds__(256) gemm_update_kernel(Cx<T> *A, int64_t ld, 
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = T(0);
     for (int kc = 0; kc < kk; kc += GKC) {
-        for (int idx = threadIdx.x; idx < GT * GKC; idx += 256) {
-            const int i = idx / GKC, q = idx % GKC;
-            const int r = r0 + i, kq = kc + q;
-            sL[q][i] = (r < n && kq < kk) ? A[(int64_t)r * ld + k + kq] : Cx<T>{T(0), T(0)};
-            const int q2 = idx / GT, j = idx % GT;
-            const int c = c0 + j, kq2 = kc + q2;
-            sU[q2][j] = (c < n && kq2 < kk) ? A[(int64_t)(k + kq2) * ld + c] : Cx<T>{T(0), T(0)};
+        {
+            constexpr int PER = GT * GKC / 256;
+            Cx<T> vl[PER], vu[PER];
+#pragma unroll
+            for (int u = 0; u < PER; ++u) {
+                const int idx = threadIdx.x + u * 256;
+                const int i = idx / GKC, q = idx % GKC, r = r0 + i, kq = kc + q;
+                vl[u] = (r < n && kq < kk) ? A[(int64_t)r * ld + k + kq] : Cx<T>{T(0), T(0)};
+                const int q2 = idx / GT, j = idx % GT, c = c0 + j, kq2 = kc + q2;
+                vu[u] = (c < n && kq2 < kk) ? A[(int64_t)(k + kq2) * ld + c] : Cx<T>{T(0), T(0)};
+            }
+#pragma unroll
+            for (int u = 0; u < PER; ++u) {
+                const int idx = threadIdx.x + u * 256;
+                sL[idx % GKC][idx / GKC] = vl[u];
+                sU[idx / GT][idx % GT] = vu[u];
+            }
         }
         __syncthreads();
 #pragma unroll 4
@@ -374,13 +401,13 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
     size_t smem = sizeof(Cx<T>) * ((size_t)rpc * nb + 2 * nb + rpc);
     BB_REQUIRE(smem <= smem_cap, BEAT_B200_INVALID_ARG,
                "LU: system of order " + std::to_string(n) + " exceeds the shared-memory panel limit");
-    // scratch: [2][G][nb] rows + [2][nb] diag + [2][G] vals + [2][G] idx
-    const size_t scratch = sizeof(Cx<T>) * (2 * (size_t)G * nb + 2 * nb) + sizeof(T) * 2 * G + sizeof(int) * 2 * G;
+    // scratch: [2][G] pivot records, [2][G][nb] candidate rows, [2][nb] diagonal rows
+    const size_t rec_bytes = sizeof(PivotRec) * 2 * (size_t)G;
+    const size_t scratch = rec_bytes + sizeof(Cx<T>) * (2 * (size_t)G * nb + 2 * nb);
     w.panel_scratch.alloc(scratch + 256);
-    Cx<T> *pub_rows = w.panel_scratch.as<Cx<T>>();
+    PivotRec *recs = w.panel_scratch.as<PivotRec>();
+    Cx<T> *pub_rows = reinterpret_cast<Cx<T> *>(recs + 2 * G);
     Cx<T> *pub_diag = pub_rows + 2 * (size_t)G * nb;
-    T *pub_val = reinterpret_cast<T *>(pub_diag + 2 * nb);
-    int *pub_idx = reinterpret_cast<int *>(pub_val + 2 * G);
     c->barrier.alloc(sizeof(unsigned) * 4096);
     BB_CUDA(cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
     const size_t trsm_smem = sizeof(Cx<T>) * ((size_t)nb * nb + (size_t)nb * TRSM_COLS);
@@ -401,9 +428,8 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
         a.ipiv = w.ipiv.as<int>();
         a.pub_rows = pub_rows;
         a.pub_diag = pub_diag;
-        a.pub_val = pub_val;
-        a.pub_idx = pub_idx;
-        a.barrier = c->barrier.as<unsigned>();
+        a.recs = recs;
+        a.counter = c->barrier.as<unsigned>();
         a.status = c->status.as<int>();
         a.spin_limit = 1u << 22;
         const size_t ps = sizeof(Cx<T>) * ((size_t)rows * nb + 2 * nb + rows);
@@ -439,13 +465,7 @@ __global__ void permute_rows_kernel(const double2 *in, double2 *out, const int *
     for (int r = 0; r < R; ++r) out[(size_t)r * n + i] = in[(size_t)r * n + src];
 }
 
-// Block substitution in one kernel.  The solution is cut into 64-row blocks;
-// each CTA claims the next block from a counter (so it only ever waits on
-// blocks already claimed by running CTAs), folds in L_bj X_j (or U_bj X_j)
-// for every finished block j as its flag appears, solves its diagonal block
-// and publishes X_b with a flag.  Waits are bounded: on expiry the kernel sets
-// a status bit and continues, so it always terminates.
-constexpr int SB = 64, SRC = 16, SOLVE_THREADS = 256, SBP = SB + 1;
+constexpr int SB = 64, SRC = 16, SBP = SB + 1;
 
 template <typename T> __device__ __forceinline__ Cx<double> to_d(Cx<T> v) {
     return Cx<double>{(double)v.re, (double)v.im};
@@ -492,20 +512,94 @@ __global__ void __launch_bounds__(SB) diag_inverse_kernel(const Cx<T> *A, int64_
     for (int i = 0; i < SB; ++i) out[i * SB + c] = X[i][c];
 }
 
+// H_b = D_b^-1 M_b for the block next to the diagonal on the solve's
+// critical path: M_b = L[b, b-1] (lower, blockIdx.y = 0) or U[b, b+1] (upper,
+// blockIdx.y = 1).  With it, X_b = Z_b - H_b X_{b-1 or b+1}, where Z_b is
+// everything else and can be formed while the neighbouring block is solved.
+template <typename T>
+__global__ void __launch_bounds__(256) offdiag_product_kernel(const Cx<T> *A, int64_t ld, int n, Cx<double> *Dinv) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cx<double> *Dt = reinterpret_cast<Cx<double> *>(smem_raw);  // SB x SBP
+    Cx<double> *Mt = Dt + SB * SBP;                               // SB x SBP
+    const int nblk = gridDim.x, b = blockIdx.x, upper = blockIdx.y;
+    const int nb2 = upper ? b + 1 : b - 1;
+    Cx<double> *H = Dinv + ((size_t)(2 + upper) * nblk + b) * SB * SB;
+    if (nb2 < 0 || nb2 >= nblk) {
+        for (int i = threadIdx.x; i < SB * SB; i += blockDim.x) H[i] = Cx<double>{0.0, 0.0};
+        return;
+    }
+    const Cx<double> *D = Dinv + ((size_t)upper * nblk + b) * SB * SB;
+    const int rb = b * SB, rows = min(SB, n - rb), cb = nb2 * SB, cols = min(SB, n - cb);
+    batched_copy<256, 8, Cx<double>>(SB * SB, [&](int i) { return D[i]; },
+                                     [&](int i, Cx<double> v) { Dt[(i / SB) * SBP + i % SB] = v; });
+    batched_copy<256, 8, Cx<double>>(
+        SB * SB,
+        [&](int i) {
+            const int a = i / SB, q = i % SB;
+            return (a < rows && q < cols) ? to_d(A[(int64_t)(rb + a) * ld + cb + q]) : Cx<double>{0.0, 0.0};
+        },
+        [&](int i, Cx<double> v) { Mt[(i / SB) * SBP + i % SB] = v; });
+    __syncthreads();
+    for (int o = threadIdx.x; o < SB * SB; o += blockDim.x) {
+        const int r = o / SB, c = o % SB;
+        double sr = 0, si = 0;
+        for (int q = 0; q < SB; ++q) {
+            const Cx<double> d = Dt[r * SBP + q], m = Mt[q * SBP + c];
+            sr += d.re * m.re - d.im * m.im;
+            si += d.re * m.im + d.im * m.re;
+        }
+        H[o] = Cx<double>{sr, si};
+    }
+}
+
+// out[2] (+)= M[r, :] V[:, c..c+1] over a 64 x 64 shared tile (row stride SBP)
+// and a 64 x SRC shared block
+__device__ __forceinline__ void tile_rows_times_block(const Cx<double> *M, const Cx<double> *V, int r, int c,
+                                                      double *o_re, double *o_im) {
+#pragma unroll 16
+    for (int q = 0; q < SB; ++q) {
+        const Cx<double> m = M[r * SBP + q];
+        const Cx<double> v0 = V[q * SRC + c], v1 = V[q * SRC + c + 1];
+        o_re[0] += m.re * v0.re - m.im * v0.im;
+        o_im[0] += m.re * v0.im + m.im * v0.re;
+        o_re[1] += m.re * v1.re - m.im * v1.im;
+        o_im[1] += m.re * v1.im + m.im * v1.re;
+    }
+}
+
 // Block substitution in one kernel.  The solution is cut into 64-row blocks;
 // each CTA claims the next block from a counter (so it only ever waits on
-// blocks already claimed by running CTAs), folds in L_bj X_j (or U_bj X_j)
-// for every finished block j as its flag appears, applies the inverted
-// diagonal block and publishes X_b with a flag.  Waits are bounded: on expiry
-// the kernel sets a status bit and continues, so it always terminates.
+// blocks already claimed by running CTAs).  For block b it folds in
+// L_bj X_j (or U_bj X_j) for every finished block j other than the
+// neighbour, forms Z_b = D_b^-1 (B_b - that sum) while the neighbour is still
+// being solved, and then X_b = Z_b - H_b X_neighbour: one 64 x 64 x R product
+// on the critical path per block.  Waits are bounded: on expiry the kernel
+// sets a status bit and continues, so it always terminates.
+constexpr int SUBST_THREADS = 512;
+
+__device__ __forceinline__ bool wait_flag(const int *flag, int epoch, int *status, unsigned spin_limit) {
+    unsigned it = 0;
+    while (true) {
+        int v;
+        asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
+        if (v == epoch) return true;
+        if ((*(volatile int *)status & DEV_BARRIER_TIMEOUT) || ++it > spin_limit) {
+            atomicOr(status, (int)DEV_BARRIER_TIMEOUT);
+            return false;
+        }
+    }
+}
+
 template <typename T, bool LOWER>
-__global__ void __launch_bounds__(SOLVE_THREADS) block_subst_kernel(const Cx<T> *A, int64_t ld, int n,
+__global__ void __launch_bounds__(SUBST_THREADS) block_subst_kernel(const Cx<T> *A, int64_t ld, int n,
                                                                     const Cx<double> *Dinv, double2 *X, int R,
                                                                     int r0, int *counter, int *flags, int epoch,
                                                                     int *status, unsigned spin_limit) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Cx<double> *Lt = reinterpret_cast<Cx<double> *>(smem_raw);  // SB x SBP
-    Cx<double> *Xj = Lt + SB * SBP;                               // SB x SRC
+    Cx<double> *Lt = reinterpret_cast<Cx<double> *>(smem_raw);  // SB x SBP: off-diagonal tile
+    Cx<double> *Dt = Lt + SB * SBP;                               // SB x SBP: D_b^-1
+    Cx<double> *Ht = Dt + SB * SBP;                               // SB x SBP: H_b
+    Cx<double> *Xj = Ht + SB * SBP;                               // SB x SRC
     __shared__ int s_blk;
     const int nblk = (n + SB - 1) / SB;
     if (threadIdx.x == 0) s_blk = atomicAdd(counter, 1);
@@ -515,73 +609,76 @@ __global__ void __launch_bounds__(SOLVE_THREADS) block_subst_kernel(const Cx<T> 
     const int b = LOWER ? claim : nblk - 1 - claim;
     const int rb = b * SB, rows = min(SB, n - rb);
     const int rc = min(SRC, R - r0);
-    const int r = threadIdx.x >> 2, cg = (threadIdx.x & 3) * 4;  // row, first of 4 columns
-    double ar[4] = {0, 0, 0, 0}, ai[4] = {0, 0, 0, 0};
-    for (int step = 0; step < claim; ++step) {
-        const int j = LOWER ? step : nblk - 1 - step;  // dependencies in the order they finish
-        const int cj = j * SB, cols = min(SB, n - cj);
-        // the L tile does not depend on the wait: load it first
-        for (int i = threadIdx.x; i < SB * SB; i += SOLVE_THREADS) {
-            const int a = i / SB, q = i % SB;
-            Lt[a * SBP + q] = (a < rows && q < cols) ? to_d(A[(int64_t)(rb + a) * ld + cj + q]) : Cx<double>{0.0, 0.0};
-        }
-        if (threadIdx.x == 0) {
-            unsigned it = 0;
-            while (true) {
-                int v;
-                asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(flags + j) : "memory");
-                if (v == epoch) break;
-                if ((*(volatile int *)status & DEV_BARRIER_TIMEOUT) || ++it > spin_limit) {
-                    atomicOr(status, (int)DEV_BARRIER_TIMEOUT);
-                    break;
-                }
-                __nanosleep(20);
-            }
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < SB * SRC; i += SOLVE_THREADS) {
-            const int q = i / SB, a = i % SB;  // consecutive threads: consecutive rows of one column
-            double2 v = make_double2(0, 0);
-            if (a < cols && q < rc) v = __ldcg(&X[(size_t)(r0 + q) * n + cj + a]);
-            Xj[a * SRC + q] = Cx<double>{v.x, v.y};
-        }
-        __syncthreads();
-#pragma unroll 8
-        for (int q = 0; q < SB; ++q) {
-            const Cx<double> l = Lt[r * SBP + q];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const Cx<double> x = Xj[q * SRC + cg + e];
-                ar[e] += l.re * x.re - l.im * x.im;
-                ai[e] += l.re * x.im + l.im * x.re;
-            }
-        }
-        __syncthreads();
-    }
-    // Y = B_b - acc;  X_b = inv(D_bb) Y
+    const int r = threadIdx.x >> 3, c = (threadIdx.x & 7) * 2;  // row, first of 2 columns
+    // independent of every other block: D_b^-1, H_b and B_b
     const Cx<double> *Di = Dinv + ((size_t)(LOWER ? 0 : 1) * nblk + b) * SB * SB;
-    for (int i = threadIdx.x; i < SB * SB; i += SOLVE_THREADS) Lt[(i / SB) * SBP + i % SB] = Di[i];
+    const Cx<double> *Hi = Dinv + ((size_t)(LOWER ? 2 : 3) * nblk + b) * SB * SB;
+    batched_copy<SUBST_THREADS, 8, Cx<double>>(SB * SB, [&](int i) { return Di[i]; },
+                                                [&](int i, Cx<double> v) { Dt[(i / SB) * SBP + i % SB] = v; });
+    batched_copy<SUBST_THREADS, 8, Cx<double>>(SB * SB, [&](int i) { return Hi[i]; },
+                                                [&](int i, Cx<double> v) { Ht[(i / SB) * SBP + i % SB] = v; });
+    double acc_re[2] = {0, 0}, acc_im[2] = {0, 0};
+    double b_re[2], b_im[2];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
+    for (int e = 0; e < 2; ++e) {
         double2 v = make_double2(0, 0);
-        if (r < rows && cg + e < rc) v = X[(size_t)(r0 + cg + e) * n + rb + r];
-        Xj[r * SRC + cg + e] = Cx<double>{v.x - ar[e], v.y - ai[e]};
+        if (r < rows && c + e < rc) v = X[(size_t)(r0 + c + e) * n + rb + r];
+        b_re[e] = v.x;
+        b_im[e] = v.y;
     }
-    __syncthreads();
-    double xr[4] = {0, 0, 0, 0}, xi[4] = {0, 0, 0, 0};
-#pragma unroll 8
-    for (int q = 0; q < SB; ++q) {
-        const Cx<double> d = Lt[r * SBP + q];
+    auto load_x = [&](int j) {
+        const int cj = j * SB, cols = min(SB, n - cj);
+        batched_copy<SUBST_THREADS, 2, double2>(
+            SB * SRC,
+            [&](int i) {
+                const int q = i / SB, a = i % SB;  // consecutive threads: consecutive rows of one column
+                return (a < cols && q < rc) ? __ldcg(&X[(size_t)(r0 + q) * n + cj + a]) : make_double2(0, 0);
+            },
+            [&](int i, double2 v) { Xj[(i % SB) * SRC + i / SB] = Cx<double>{v.x, v.y}; });
+    };
+    // all finished blocks except the neighbour
+    for (int step = 0; step + 1 < claim; ++step) {
+        const int j = LOWER ? step : nblk - 1 - step;
+        const int cj = j * SB, cols = min(SB, n - cj);
+        batched_copy<SUBST_THREADS, 8, Cx<double>>(
+            SB * SB,
+            [&](int i) {
+                const int a = i / SB, q = i % SB;
+                return (a < rows && q < cols) ? to_d(A[(int64_t)(rb + a) * ld + cj + q]) : Cx<double>{0.0, 0.0};
+            },
+            [&](int i, Cx<double> v) { Lt[(i / SB) * SBP + i % SB] = v; });
+        if (threadIdx.x == 0) wait_flag(flags + j, epoch, status, spin_limit);
+        __syncthreads();
+        load_x(j);
+        __syncthreads();
+        tile_rows_times_block(Lt, Xj, r, c, acc_re, acc_im);
+        __syncthreads();
+    }
+    // Z_b = D_b^-1 (B_b - acc)
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const Cx<double> y = Xj[q * SRC + cg + e];
-            xr[e] += d.re * y.re - d.im * y.im;
-            xi[e] += d.re * y.im + d.im * y.re;
+    for (int e = 0; e < 2; ++e) Xj[r * SRC + c + e] = Cx<double>{b_re[e] - acc_re[e], b_im[e] - acc_im[e]};
+    __syncthreads();
+    double z_re[2] = {0, 0}, z_im[2] = {0, 0};
+    tile_rows_times_block(Dt, Xj, r, c, z_re, z_im);
+    __syncthreads();
+    if (claim > 0) {
+        // X_b = Z_b - H_b X_neighbour
+        const int jn = LOWER ? b - 1 : b + 1;
+        if (threadIdx.x == 0) wait_flag(flags + jn, epoch, status, spin_limit);
+        __syncthreads();
+        load_x(jn);
+        __syncthreads();
+        double h_re[2] = {0, 0}, h_im[2] = {0, 0};
+        tile_rows_times_block(Ht, Xj, r, c, h_re, h_im);
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            z_re[e] -= h_re[e];
+            z_im[e] -= h_im[e];
         }
     }
 #pragma unroll
-    for (int e = 0; e < 4; ++e)
-        if (r < rows && cg + e < rc) X[(size_t)(r0 + cg + e) * n + rb + r] = make_double2(xr[e], xi[e]);
+    for (int e = 0; e < 2; ++e)
+        if (r < rows && c + e < rc) X[(size_t)(r0 + c + e) * n + rb + r] = make_double2(z_re[e], z_im[e]);
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(flags + b), "r"(epoch) : "memory");
@@ -590,10 +687,13 @@ __global__ void __launch_bounds__(SOLVE_THREADS) block_subst_kernel(const Cx<T> 
 template <typename T> static void diag_inverses(beat_b200_ctx *c) {
     Workspace &w = c->ws;
     const int n = c->V, nblk = (n + SB - 1) / SB;
-    w.dinv.alloc(sizeof(Cx<double>) * 2 * (size_t)nblk * SB * SB);
+    w.dinv.alloc(sizeof(Cx<double>) * 4 * (size_t)nblk * SB * SB);
     const size_t smem = 2 * sizeof(Cx<double>) * SB * SBP;
     BB_CUDA(cudaFuncSetAttribute(diag_inverse_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     diag_inverse_kernel<T><<<dim3(nblk, 2), SB, smem, c->stream>>>(w.A.as<Cx<T>>(), w.ld, n, w.dinv.as<Cx<double>>());
+    BB_CUDA(cudaFuncSetAttribute(offdiag_product_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    offdiag_product_kernel<T><<<dim3(nblk, 2), 256, smem, c->stream>>>(w.A.as<Cx<T>>(), w.ld, n,
+                                                                     w.dinv.as<Cx<double>>());
     BB_CUDA(cudaGetLastError());
 }
 
@@ -608,7 +708,7 @@ template <typename T> static void lu_solve_t(beat_b200_ctx *c, int R, const doub
     int *counter = w.small_solve.as<int>();
     int *flags = counter + 32;
     if (w.solve_epoch == 0) BB_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * nblk, c->stream));
-    const size_t smem = sizeof(Cx<double>) * (SB * SBP + SB * SRC);
+    const size_t smem = sizeof(Cx<double>) * (3 * SB * SBP + SB * SRC);
     BB_CUDA(cudaFuncSetAttribute(block_subst_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     BB_CUDA(cudaFuncSetAttribute(block_subst_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     permute_rows_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(reinterpret_cast<const double2 *>(in), X,
@@ -619,10 +719,10 @@ template <typename T> static void lu_solve_t(beat_b200_ctx *c, int R, const doub
             const int epoch = ++w.solve_epoch;
             BB_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), c->stream));
             if (pass == 0)
-                block_subst_kernel<T, true><<<nblk, SOLVE_THREADS, smem, c->stream>>>(
+                block_subst_kernel<T, true><<<nblk, SUBST_THREADS, smem, c->stream>>>(
                     A, w.ld, n, Dinv, X, R, r0, counter, flags, epoch, c->status.as<int>(), 1u << 22);
             else
-                block_subst_kernel<T, false><<<nblk, SOLVE_THREADS, smem, c->stream>>>(
+                block_subst_kernel<T, false><<<nblk, SUBST_THREADS, smem, c->stream>>>(
                     A, w.ld, n, Dinv, X, R, r0, counter, flags, epoch, c->status.as<int>(), 1u << 22);
         }
     }
