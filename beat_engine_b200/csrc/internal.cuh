@@ -178,6 +178,8 @@ struct beat_b200_ctx {
 
     cudaEvent_t ev[10] = {};
     float last_regular_ms = 0.f;
+    bool cluster_checked = false;  // can a 16-CTA cluster of the panel kernel be scheduled?
+    bool cluster_ok = false;
 };
 
 namespace bb {

@@ -278,14 +278,16 @@ __global__ void iota_kernel(int *perm, int n) {
     if (i < n) perm[i] = i;
 }
 
-// U12 = L11^-1 A12 for columns [k+nb, n); 32 columns per CTA
+// A[k:k+kb, c_begin:c_end] = L^-1 A[...] with L = A[k:k+kb, k:k+kb] unit
+// lower (nb = allocated width of the triangle); 32 columns per CTA
 constexpr int TRSM_COLS = 32;
-template <typename T> __global__ void __launch_bounds__(256) trsm_kernel(Cx<T> *A, int64_t ld, int n, int k, int nb) {
+template <typename T>
+__global__ void __launch_bounds__(256) trsm_kernel(Cx<T> *A, int64_t ld, int n, int k, int nb, int c_begin, int c_end) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cx<T> *L = reinterpret_cast<Cx<T> *>(smem_raw);  // nb x nb
     Cx<T> *X = L + nb * nb;                           // nb x TRSM_COLS
-    const int c0 = k + nb + blockIdx.x * TRSM_COLS;
-    const int nc = min(TRSM_COLS, n - c0);
+    const int c0 = c_begin + blockIdx.x * TRSM_COLS;
+    const int nc = min(TRSM_COLS, c_end - c0);
     const int kb = min(nb, n - k);
     batched_copy<256, 16, Cx<T>>(
         kb * kb, [&](int i) { return A[(int64_t)(k + i / kb) * ld + k + i % kb]; },
@@ -322,7 +324,7 @@ template <typename T> __global__ void __launch_bounds__(256) trsm_kernel(Cx<T> *
 constexpr int GT = 64, GKC = 16;
 template <typename T>
 __global__ void __launch_bounds__(256, 2) gemm_update_kernel(Cx<T> *A, int64_t ld, int n, int k, int kk, int row0,
-                                                          int col0) {
+                                                          int col0, int col_end) {
     __shared__ Cx<T> sL[GKC][GT + 1];
     __shared__ Cx<T> sU[GKC][GT];
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -342,7 +344,7 @@ __global__ void __launch_bounds__(256, 2) gemm_update_kernel(Cx<T> *A, int64_t l
                 const int i = idx / GKC, q = idx % GKC, r = r0 + i, kq = kc + q;
                 vl[u] = (r < n && kq < kk) ? A[(int64_t)r * ld + k + kq] : Cx<T>{T(0), T(0)};
                 const int q2 = idx / GT, j = idx % GT, c = c0 + j, kq2 = kc + q2;
-                vu[u] = (c < n && kq2 < kk) ? A[(int64_t)(k + kq2) * ld + c] : Cx<T>{T(0), T(0)};
+                vu[u] = (c < col_end && kq2 < kk) ? A[(int64_t)(k + kq2) * ld + c] : Cx<T>{T(0), T(0)};
             }
 #pragma unroll
             for (int u = 0; u < PER; ++u) {
@@ -374,12 +376,241 @@ __global__ void __launch_bounds__(256, 2) gemm_update_kernel(Cx<T> *A, int64_t l
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int r = r0 + ty + 16 * i, c = c0 + tx + 16 * j;
-            if (r < n && c < n) {
+            if (r < n && c < col_end) {
                 Cx<T> &d = A[(int64_t)r * ld + c];
                 d.re -= acc[i][j][0];
                 d.im -= acc[i][j][1];
             }
         }
+}
+
+// ---------------------------------------------------------------------------
+// Sub-panel factorisation on one thread-block cluster.  CP_CTAS CTAs hold all
+// rows of a W-column sub-panel in shared memory.  Per column: local pivot
+// candidate, candidate value/row written into every CTA's shared memory
+// (distributed shared memory stores), the candidate's row and the current
+// diagonal row copied to a local publish buffer, one hardware cluster
+// barrier, every CTA picks the same winner from its own copy of the
+// candidates and reads the winner's row from the winner CTA's publish buffer.
+// Publish buffers and candidate slots alternate with the column parity, so
+// one barrier per column suffices.
+// ---------------------------------------------------------------------------
+constexpr int CP_CTAS = 16, CP_THREADS = 256;
+
+__device__ __forceinline__ uint32_t cl_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cl_map(const void *p, uint32_t rank) {
+    uint32_t a = (uint32_t)__cvta_generic_to_shared(p), r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void cl_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cl_st(uint32_t addr, double v) {
+    asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(addr), "d"(v) : "memory");
+}
+__device__ __forceinline__ void cl_st(uint32_t addr, int v) {
+    asm volatile("st.shared::cluster.b32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+__device__ __forceinline__ Cx<double> cl_ld(uint32_t addr, const Cx<double> *) {
+    double x, y;
+    asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(x), "=d"(y) : "r"(addr) : "memory");
+    return Cx<double>{x, y};
+}
+__device__ __forceinline__ Cx<float> cl_ld(uint32_t addr, const Cx<float> *) {
+    float x, y;
+    asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(x), "=f"(y) : "r"(addr) : "memory");
+    return Cx<float>{x, y};
+}
+
+template <typename T> struct ClusterPanelArgs {
+    Cx<T> *A;
+    int64_t ld;
+    int n, k, w;  // sub-panel: rows [k, n), columns [k, k + w)
+    int rpc;      // rows per CTA
+    int *ipiv;
+    int *status;
+};
+
+// combine two pivot candidates: larger |re|+|im|, then the smaller row
+template <typename T> __device__ __forceinline__ void better(T &v, int &i, T ov, int oi) {
+    if (oi >= 0 && (ov > v || (ov == v && (i < 0 || oi < i)))) {
+        v = ov;
+        i = oi;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(CP_THREADS) cluster_panel_kernel(ClusterPanelArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int w = a.w, wp = a.w + 1, tid = threadIdx.x;  // row stride padded by one entry
+    Cx<T> *P = reinterpret_cast<Cx<T> *>(smem_raw);       // rpc x wp
+    Cx<T> *pub = P + (size_t)a.rpc * wp;                   // [2][w] candidate rows
+    Cx<T> *pdg = pub + 2 * w;                              // [2][w] diagonal rows
+    Cx<T> *prow = pdg + 2 * w;                             // w
+    Cx<T> *drow = prow + w;                                // w
+    __shared__ double cand_v[2][CP_CTAS];
+    __shared__ int cand_i[2][CP_CTAS];
+    __shared__ T red_v[CP_THREADS / 32];
+    __shared__ int red_i[CP_THREADS / 32];
+    __shared__ int s_mine;
+    __shared__ T s_val;
+    const uint32_t rank = cl_rank();
+    const int gr0 = a.k + (int)rank * a.rpc;
+    const int nrows = max(0, min(a.rpc, a.n - gr0));
+    batched_copy<CP_THREADS, 8, Cx<T>>(
+        nrows * w, [&](int i) { return a.A[(int64_t)(gr0 + i / w) * a.ld + a.k + i % w]; },
+        [&](int i, Cx<T> v) { P[(i / w) * wp + i % w] = v; });
+    __syncthreads();
+    // block-wide candidate of column `col` over rows >= row_min: thread-local
+    // (bv, bi) in, s_mine / s_val out
+    auto reduce_candidate = [&](T bv, int bi) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const T ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            better(bv, bi, ov, oi);
+        }
+        if ((tid & 31) == 0) {
+            red_v[tid >> 5] = bv;
+            red_i[tid >> 5] = bi;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            for (int q = 1; q < CP_THREADS / 32; ++q) better(bv, bi, red_v[q], red_i[q]);
+            s_mine = bi;
+            s_val = bv;
+        }
+        __syncthreads();
+    };
+    {
+        T bv = T(-1);
+        int bi = -1;
+        for (int i = tid; i < nrows; i += CP_THREADS) better(bv, bi, cabs1(P[i * wp]), gr0 + i);
+        reduce_candidate(bv, bi);
+    }
+    cl_sync();  // every CTA of the cluster is running before any remote access
+    for (int j = 0; j < w && a.k + j < a.n; ++j) {
+        const int jr = a.k + j, par = j & 1;
+        const int mine = s_mine;
+        if (tid < CP_CTAS) {
+            // this CTA's candidate into slot [par][rank] of CTA `tid`
+            cl_st(cl_map(&cand_v[par][rank], tid), (double)s_val);
+            cl_st(cl_map(&cand_i[par][rank], tid), mine);
+        }
+        for (int c = tid; c < w; c += CP_THREADS) {
+            if (mine >= 0) pub[par * w + c] = P[(mine - gr0) * wp + c];
+            if (jr >= gr0 && jr < gr0 + nrows) pdg[par * w + c] = P[(jr - gr0) * wp + c];
+        }
+        cl_sync();
+        // every thread picks the winner from its CTA's copy of the candidates
+        double wv = -1.0;
+        int p = -1, wc = -1;
+#pragma unroll
+        for (int q = 0; q < CP_CTAS; ++q) {
+            const int i = cand_i[par][q];
+            const double v = cand_v[par][q];
+            if (i >= 0 && (v > wv || (v == wv && (p < 0 || i < p)))) {
+                wv = v;
+                p = i;
+                wc = q;
+            }
+        }
+        if (p < 0) p = jr;
+        if (tid == 0) {
+            if (!(wv > 0.0)) atomicOr(a.status, (int)DEV_ZERO_PIVOT);
+            if (rank == 0) a.ipiv[jr] = p;
+        }
+        const int jr_owner = (jr - a.k) / a.rpc;
+        const bool own_p = p != jr && p >= gr0 && p < gr0 + nrows;
+        for (int c = tid; c < w; c += CP_THREADS) {
+            prow[c] = wc >= 0 ? cl_ld(cl_map(&pub[par * w + c], wc), pub) : Cx<T>{T(0), T(0)};
+            if (own_p) drow[c] = cl_ld(cl_map(&pdg[par * w + c], jr_owner), pdg);
+        }
+        __syncthreads();
+        // rows: jr takes the pivot row (it is U); p (if here and distinct)
+        // takes the old row jr and is eliminated like the others
+        const Cx<T> pv = prow[j];
+        const T den = pv.re * pv.re + pv.im * pv.im;
+        const Cx<T> inv = den > T(0) ? Cx<T>{pv.re / den, -pv.im / den} : Cx<T>{T(0), T(0)};
+        T bv = T(-1);
+        int bi = -1;
+        for (int i = tid; i < nrows; i += CP_THREADS) {
+            const int gi = gr0 + i;
+            Cx<T> *row = P + (size_t)i * wp;
+            if (gi == jr) {
+                if (p != jr)
+                    for (int c = 0; c < w; ++c) row[c] = prow[c];  // L entries of row p move with it
+                continue;
+            }
+            if (gi < jr) continue;
+            const Cx<T> *src = gi == p ? drow : row;
+            const Cx<T> l = cmul(src[j], inv);
+            if (gi == p)
+                for (int c = 0; c < j; ++c) row[c] = drow[c];
+            row[j] = l;
+            for (int c = j + 1; c < w; ++c) {
+                const Cx<T> u = prow[c], x = src[c];
+                row[c] = Cx<T>{x.re - (l.re * u.re - l.im * u.im), x.im - (l.re * u.im + l.im * u.re)};
+            }
+            if (j + 1 < w) better(bv, bi, cabs1(row[j + 1]), gi);
+        }
+        reduce_candidate(bv, bi);
+    }
+    for (int i = tid; i < nrows * w; i += CP_THREADS) a.A[(int64_t)(gr0 + i / w) * a.ld + a.k + i % w] = P[(i / w) * wp + i % w];
+    cl_sync();  // no CTA leaves while others may still read its shared memory
+}
+
+// Launches the cluster kernel for a sub-panel; false when the rows do not fit
+// the cluster's shared memory or no cluster of CP_CTAS can be scheduled.
+template <typename T>
+static bool cluster_panel(beat_b200_ctx *c, Cx<T> *A, int64_t ld, int n, int k, int w, int *ipiv) {
+    const int m = n - k;
+    const int rpc = (m + CP_CTAS - 1) / CP_CTAS;
+    const size_t smem = sizeof(Cx<T>) * ((size_t)rpc * (w + 1) + 6 * (size_t)w);
+    if (smem > 200 * 1024) return false;
+    static bool attr_done[2] = {false, false};
+    const int ti = sizeof(T) == 8;
+    if (!attr_done[ti]) {
+        BB_CUDA(cudaFuncSetAttribute(cluster_panel_kernel<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        BB_CUDA(cudaFuncSetAttribute(cluster_panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr_done[ti] = true;
+    }
+    ClusterPanelArgs<T> a;
+    a.A = A;
+    a.ld = ld;
+    a.n = n;
+    a.k = k;
+    a.w = w;
+    a.rpc = rpc;
+    a.ipiv = ipiv;
+    a.status = c->status.as<int>();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(CP_CTAS);
+    cfg.blockDim = dim3(CP_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CP_CTAS;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (!c->cluster_checked) {
+        int nclusters = 0;
+        cudaError_t e = cudaOccupancyMaxActiveClusters(&nclusters, (void *)cluster_panel_kernel<T>, &cfg);
+        c->cluster_ok = (e == cudaSuccess && nclusters >= 1);
+        cudaGetLastError();
+        c->cluster_checked = true;
+    }
+    if (!c->cluster_ok) return false;
+    BB_CUDA(cudaLaunchKernelEx(&cfg, cluster_panel_kernel<T>, a));
+    return true;
 }
 
 // FP32 form trailing update on the tensor cores (tc_gemm.cu); returns false
@@ -414,39 +645,58 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
     BB_CUDA(cudaFuncSetAttribute(trsm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
     iota_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(w.perm.as<int>(), n);
     BB_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream));
+    // sub-panel width: 256-byte rows in the cluster kernel
+    const int W = std::min(nb, (int)(256 / sizeof(Cx<T>)));
+    const size_t trsm_w_smem = sizeof(Cx<T>) * ((size_t)W * W + (size_t)W * TRSM_COLS);
     for (int k = 0; k < n; k += nb) {
-        const int m = n - k;
-        int g = std::min(G, std::max(1, (m + 15) / 16));
-        int rows = (m + g - 1) / g;
-        PanelArgs<T> a;
-        a.A = A;
-        a.ld = ld;
-        a.n = n;
-        a.k = k;
-        a.nb = nb;
-        a.rpc = rows;
-        a.ipiv = w.ipiv.as<int>();
-        a.pub_rows = pub_rows;
-        a.pub_diag = pub_diag;
-        a.recs = recs;
-        a.counter = c->barrier.as<unsigned>();
-        a.status = c->status.as<int>();
-        a.spin_limit = 1u << 22;
-        const size_t ps = sizeof(Cx<T>) * ((size_t)rows * nb + 2 * nb + rows);
-        BB_CUDA(cudaMemsetAsync(c->barrier.p, 0, sizeof(unsigned), c->stream));
-        void *args[] = {&a};
-        BB_CUDA(cudaLaunchCooperativeKernel((void *)panel_kernel<T>, dim3(g), dim3(PANEL_THREADS), args, ps,
-                                            c->stream));
-        laswp_kernel<T><<<(n + 1 + 255) / 256, 256, 0, c->stream>>>(A, ld, n, k, nb, w.ipiv.as<int>(),
-                                                                    w.perm.as<int>());
-        BB_CUDA(cudaGetLastError());
+        const int pe = std::min(k + nb, n);  // end of this panel
+        for (int ks = k; ks < pe; ks += W) {
+            const int m = n - ks;
+            if (!cluster_panel<T>(c, A, ld, n, ks, W, w.ipiv.as<int>())) {
+                // grid-wide panel kernel on the sub-panel
+                int g = std::min(G, std::max(1, (m + 15) / 16));
+                int rows = (m + g - 1) / g;
+                PanelArgs<T> a;
+                a.A = A;
+                a.ld = ld;
+                a.n = n;
+                a.k = ks;
+                a.nb = W;
+                a.rpc = rows;
+                a.ipiv = w.ipiv.as<int>();
+                a.pub_rows = pub_rows;
+                a.pub_diag = pub_diag;
+                a.recs = recs;
+                a.counter = c->barrier.as<unsigned>();
+                a.status = c->status.as<int>();
+                a.spin_limit = 1u << 22;
+                const size_t ps = sizeof(Cx<T>) * ((size_t)rows * W + 2 * W + rows);
+                BB_CUDA(cudaMemsetAsync(c->barrier.p, 0, sizeof(unsigned), c->stream));
+                void *args[] = {&a};
+                BB_CUDA(cudaLaunchCooperativeKernel((void *)panel_kernel<T>, dim3(g), dim3(PANEL_THREADS), args, ps,
+                                                    c->stream));
+            }
+            laswp_kernel<T><<<(n + 1 + 255) / 256, 256, 0, c->stream>>>(A, ld, n, ks, W, w.ipiv.as<int>(),
+                                                                        w.perm.as<int>());
+            BB_CUDA(cudaGetLastError());
+            if (ks + W < pe) {
+                // rest of this panel: U row block, then the panel's own trailing update
+                const int cols = pe - ks - W;
+                trsm_kernel<T><<<(cols + TRSM_COLS - 1) / TRSM_COLS, 256, trsm_w_smem, c->stream>>>(
+                    A, ld, n, ks, W, ks + W, pe);
+                dim3 grid((cols + GT - 1) / GT, (n - ks - W + GT - 1) / GT);
+                gemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(A, ld, n, ks, W, ks + W, ks + W, pe);
+                BB_CUDA(cudaGetLastError());
+            }
+        }
         const int rest = n - k - nb;
         if (rest > 0) {
-            trsm_kernel<T><<<(rest + TRSM_COLS - 1) / TRSM_COLS, 256, trsm_smem, c->stream>>>(A, ld, n, k, nb);
+            trsm_kernel<T><<<(rest + TRSM_COLS - 1) / TRSM_COLS, 256, trsm_smem, c->stream>>>(A, ld, n, k, nb, k + nb,
+                                                                                           n);
             BB_CUDA(cudaGetLastError());
             if (!(sizeof(T) == 4 && tc_trailing_update(c, k, nb, split_terms))) {
                 dim3 grid((rest + GT - 1) / GT, (rest + GT - 1) / GT);
-                gemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(A, ld, n, k, nb, k + nb, k + nb);
+                gemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(A, ld, n, k, nb, k + nb, k + nb, n);
                 BB_CUDA(cudaGetLastError());
             }
         }
