@@ -24,7 +24,7 @@ EXPORTS = (
     "beat_b200_abi_version", "beat_b200_default_opts", "beat_b200_create", "beat_b200_destroy",
     "beat_b200_last_error", "beat_b200_set_mesh", "beat_b200_solve", "beat_b200_solve_device",
     "beat_b200_field", "beat_b200_farfield", "beat_b200_farfield_device", "beat_b200_assemble",
-    "beat_b200_release_workspace", "beat_b200_device_bytes", "beat_b200_stream",
+    "beat_b200_release_workspace", "beat_b200_device_bytes", "beat_b200_stream", "beat_b200_resolve_noalloc",
 )
 
 
@@ -97,6 +97,8 @@ def load(path: str = LIB_PATH):
     L.beat_b200_device_bytes.restype = ctypes.c_int64
     L.beat_b200_stream.argtypes = [vp]
     L.beat_b200_stream.restype = vp
+    L.beat_b200_resolve_noalloc.argtypes = [vp, i32, vp, vp]
+    L.beat_b200_resolve_noalloc.restype = i32
     _lib = L
     return L
 
@@ -225,6 +227,12 @@ class Context:
 
     def device_bytes(self) -> int:
         return int(self.lib.beat_b200_device_bytes(self.handle))
+
+    def resolve_noalloc(self, R: int, d_b_ptr: int, d_x_ptr: int) -> None:
+        """Solve R more right-hand sides (device N x R complex128, column-major)
+        with the current factors, allocating nothing (beat_b200_resolve_noalloc)."""
+        self._check(self.lib.beat_b200_resolve_noalloc(self.handle, R, ctypes.c_void_p(d_b_ptr),
+                                                       ctypes.c_void_p(d_x_ptr)))
 
     def stream_handle(self) -> int:
         """cudaStream_t of this context as an integer (for torch.cuda.ExternalStream)."""

@@ -1000,4 +1000,46 @@ void lu_precond_fp32(beat_b200_ctx *c, int R, const double *in, double *out) {
     lu_solve_t<float>(c, R, in, out);
 }
 
+// The same permutation and block substitutions as lu_solve_t, with the claim
+// counter and per-block flags in caller-provided device memory (`scratch`,
+// at least nblk + 32 ints): x = (L U)^-1 P b with the context's factors.
+template <typename T>
+static void lu_resolve_into_t(beat_b200_ctx *c, int R, const double *b, double *x, int *scratch) {
+    Workspace &w = c->ws;
+    const int n = c->V;
+    const Cx<T> *A = w.A.as<Cx<T>>();
+    double2 *X = reinterpret_cast<double2 *>(x);
+    const int nblk = (n + SB - 1) / SB;
+    int *counter = scratch;
+    int *flags = scratch + 32;
+    BB_CUDA(cudaMemsetAsync(scratch, 0, sizeof(int) * (size_t)(nblk + 32), c->stream));
+    const size_t smem = sizeof(Cx<double>) * (3 * SB * SBP + SB * SRC);
+    BB_CUDA(cudaFuncSetAttribute(block_subst_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    BB_CUDA(cudaFuncSetAttribute(block_subst_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    permute_rows_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(reinterpret_cast<const double2 *>(b), X,
+                                                                w.perm.as<int>(), n, R);
+    const Cx<double> *Dinv = w.dinv.as<Cx<double>>();
+    int epoch = 0;
+    for (int r0 = 0; r0 < R; r0 += SRC) {
+        for (int pass = 0; pass < 2; ++pass) {
+            ++epoch;
+            BB_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), c->stream));
+            if (pass == 0)
+                block_subst_kernel<T, true><<<nblk, SUBST_THREADS, smem, c->stream>>>(
+                    A, w.ld, n, Dinv, X, R, r0, counter, flags, epoch, c->status.as<int>(), 1u << 22);
+            else
+                block_subst_kernel<T, false><<<nblk, SUBST_THREADS, smem, c->stream>>>(
+                    A, w.ld, n, Dinv, X, R, r0, counter, flags, epoch, c->status.as<int>(), 1u << 22);
+        }
+    }
+    BB_CUDA(cudaGetLastError());
+}
+
+void lu_resolve_into(beat_b200_ctx *c, int R, const double *b, double *x, int *scratch) {
+    if (c->ws.precision == BEAT_B200_FP64)
+        lu_resolve_into_t<double>(c, R, b, x, scratch);
+    else
+        lu_resolve_into_t<float>(c, R, b, x, scratch);
+}
+
 }  // namespace bb

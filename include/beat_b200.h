@@ -147,6 +147,21 @@ int32_t beat_b200_release_workspace(beat_b200_ctx *ctx);
 /* Bytes of device memory the context holds right now. */
 int64_t beat_b200_device_bytes(const beat_b200_ctx *ctx);
 
+/* No counterpart in the reference.  Solve R more right-hand sides with the
+ * factors of the last beat_b200_solve on this context, allocating no memory:
+ * for callers whose device memory belongs to their own pool (so a
+ * library-side cudaMalloc would bypass its accounting) or that cannot afford
+ * cudaMalloc/cudaFree on their thread.  d_b (input) and d_x (output) are
+ * distinct device buffers of N x R complex doubles, column-major.  The FP64
+ * form gives the exact LU solution; the mixed form gives its FP32-LU
+ * solution without the GMRES refinement.  Limit: N <= 262144.  Its scratch
+ * is a 16 KB static device array that every GPU loading the library holds
+ * until exit, shared by all calls on that device: calls whose work overlaps
+ * on the GPU race and must be serialised by the caller.  The first call on a
+ * device looks up that array's address; make that first call before any
+ * stream capture.  Synchronises the context's stream before returning. */
+int32_t beat_b200_resolve_noalloc(beat_b200_ctx *ctx, int32_t R, const void *d_b, void *d_x);
+
 /* The CUDA stream (cudaStream_t) every kernel of this context is launched
  * on, so a caller can order its own work or record timing events on it.
  * Entry points return only after their work on it has completed. */
