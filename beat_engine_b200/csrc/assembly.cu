@@ -403,64 +403,6 @@ __global__ void identity_kernel(const int *faces, const double *areas, int F, in
 }
 
 // ---------------------------------------------------------------------------
-// b = B q: one warp per row, up to 16 columns per pass, q chunk in smem
-// ---------------------------------------------------------------------------
-constexpr int BQ_ROWS = 8, BQ_CHUNK = 128, BQ_RC = 16;
-
-template <typename T>
-__global__ void __launch_bounds__(256) rhs_apply_kernel(const Cx<T> *B, int N, int F, const Cx<double> *q, int R,
-                                                        int r0, Cx<double> *b) {
-    __shared__ Cx<double> sq[BQ_RC][BQ_CHUNK];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int row = blockIdx.x * BQ_ROWS + warp;
-    const int rc = min(BQ_RC, R - r0);
-    double ar[BQ_RC], ai[BQ_RC];
-#pragma unroll
-    for (int r = 0; r < BQ_RC; ++r) ar[r] = ai[r] = 0.0;
-    for (int f0 = 0; f0 < F; f0 += BQ_CHUNK) {
-        __syncthreads();
-        batched_copy<256, 8, Cx<double>>(
-            BQ_RC * BQ_CHUNK,
-            [&](int i) {
-                const int r = i / BQ_CHUNK, f = f0 + i % BQ_CHUNK;
-                return (r < rc && f < F) ? q[(size_t)(r0 + r) * F + f] : Cx<double>{0.0, 0.0};
-            },
-            [&](int i, Cx<double> v) { sq[i / BQ_CHUNK][i % BQ_CHUNK] = v; });
-        __syncthreads();
-        if (row < N) {
-            for (int j = lane; j < BQ_CHUNK && f0 + j < F; j += 32) {
-                const Cx<T> bv = B[(int64_t)row * F + f0 + j];
-                const double br = (double)bv.re, bi = (double)bv.im;
-#pragma unroll
-                for (int r = 0; r < BQ_RC; ++r) {
-                    const Cx<double> qv = sq[r][j];
-                    ar[r] += br * qv.re - bi * qv.im;
-                    ai[r] += br * qv.im + bi * qv.re;
-                }
-            }
-        }
-    }
-#pragma unroll
-    for (int r = 0; r < BQ_RC; ++r) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            ar[r] += __shfl_xor_sync(0xffffffffu, ar[r], o);
-            ai[r] += __shfl_xor_sync(0xffffffffu, ai[r], o);
-        }
-    }
-    if (row < N && lane < rc) {
-        double vr = 0, vi = 0;
-#pragma unroll
-        for (int r = 0; r < BQ_RC; ++r)
-            if (r == lane) {
-                vr = ar[r];
-                vi = ai[r];
-            }
-        b[(size_t)(r0 + lane) * N + row] = Cx<double>{vr, vi};
-    }
-}
-
-// ---------------------------------------------------------------------------
 // host driver
 // ---------------------------------------------------------------------------
 template <typename T, int Q> static void launch_regular(beat_b200_ctx *c, double k, double eta) {
@@ -536,10 +478,9 @@ template <typename T> static void assemble_t(beat_b200_ctx *c, double k, double 
     identity_kernel<T><<<(F + 255) / 256, 256, 0, c->stream>>>(c->d_faces.as<int>(), c->d_areas.as<double>(), F,
                                                                c->Q, eta, w.A.as<Cx<T>>(), w.ld, w.B.as<Cx<T>>());
     BB_CUDA(cudaGetLastError());
-    for (int r0 = 0; r0 < R; r0 += BQ_RC)
-        rhs_apply_kernel<T><<<(N + BQ_ROWS - 1) / BQ_ROWS, 256, 0, c->stream>>>(w.B.as<Cx<T>>(), N, F, q, R, r0,
-                                                                                 w.b.as<Cx<double>>());
-    BB_CUDA(cudaGetLastError());
+    BB_CUDA(cudaMemsetAsync(w.b.p, 0, sizeof(Cx<double>) * (size_t)N * R, c->stream));
+    tall_gemm<T>(c->stream, c->sm_count, w.B.as<Cx<T>>(), F, N, F, reinterpret_cast<const double *>(q), w.b.as<double>(),
+                 R, 1.0);
     BB_CUDA(cudaEventRecord(c->ev[3], c->stream));
     if (ms_total || ms_singular) {
         BB_CUDA(cudaEventSynchronize(c->ev[3]));

@@ -14,6 +14,7 @@
 // in the answer (about 1e-7 relative on these systems).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <vector>
@@ -22,82 +23,100 @@
 
 namespace bb {
 
-constexpr int MV_ROWS_PER_WARP = 2, MV_WARPS = 8, MV_CHUNK = 128, MV_RC = 16;
+// ---------------------------------------------------------------------------
+// Y[:, r0:r0+16] += alpha * M X  with M complex (T, row-major, ld), X and Y
+// FP64 column-major (X: K x R, Y: rows x R).  A CTA owns 64 rows x 16 columns
+// over a slice of K and adds its partial sums with FP64 atomics.  Each thread
+// keeps a 2 x 4 complex block; M and X chunks go through shared memory.
+// ---------------------------------------------------------------------------
+constexpr int TG_ROWS = 64, TG_KC = 64, TG_RC = 16, TG_THREADS = 128;
 
-// Y[:, r0:r0+rc] = alpha * A X + beta * Y  (A: T row-major, X/Y FP64 col-major)
 template <typename T>
-__global__ void __launch_bounds__(256) matvec_kernel(const Cx<T> *A, int64_t ld, int n, const double2 *X,
-                                                     double2 *Y, int R, int r0, double alpha, double beta) {
-    __shared__ double2 sx[MV_RC][MV_CHUNK];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int row0 = (blockIdx.x * MV_WARPS + warp) * MV_ROWS_PER_WARP;
-    const int rc = min(MV_RC, R - r0);
-    double ar[MV_ROWS_PER_WARP][MV_RC], ai[MV_ROWS_PER_WARP][MV_RC];
-#pragma unroll
-    for (int a = 0; a < MV_ROWS_PER_WARP; ++a)
-#pragma unroll
-        for (int r = 0; r < MV_RC; ++r) ar[a][r] = ai[a][r] = 0.0;
-    for (int j0 = 0; j0 < n; j0 += MV_CHUNK) {
-        __syncthreads();
-        batched_copy<256, 8, double2>(
-            MV_RC * MV_CHUNK,
+__global__ void __launch_bounds__(TG_THREADS) tall_gemm_kernel(const Cx<T> *M, int64_t ld, int rows, int K,
+                                                               const double2 *X, double2 *Y, int R, int r0,
+                                                               double alpha, int kslice) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cx<T> *sM = reinterpret_cast<Cx<T> *>(smem_raw);                                // TG_ROWS x (TG_KC + 1)
+    double2 *sX = reinterpret_cast<double2 *>(smem_raw + sizeof(Cx<T>) * TG_ROWS * (TG_KC + 1));  // TG_KC x TG_RC
+    const int row0 = blockIdx.x * TG_ROWS;
+    const int kb = blockIdx.y * kslice, ke = min(K, kb + kslice);
+    const int rc = min(TG_RC, R - r0);
+    const int tr = threadIdx.x >> 2, tc = (threadIdx.x & 3) * 4;  // rows tr, tr + 32; columns tc..tc+3
+    double ar[2][4] = {}, ai[2][4] = {};
+    for (int k0 = kb; k0 < ke; k0 += TG_KC) {
+        const int kn = min(TG_KC, ke - k0);
+        batched_copy<TG_THREADS, 8, Cx<T>>(
+            TG_ROWS * TG_KC,
             [&](int i) {
-                const int r = i / MV_CHUNK, j = j0 + i % MV_CHUNK;
-                return (r < rc && j < n) ? X[(size_t)(r0 + r) * n + j] : make_double2(0, 0);
+                const int r = i / TG_KC, k = i % TG_KC;
+                return (row0 + r < rows && k < kn) ? M[(int64_t)(row0 + r) * ld + k0 + k] : Cx<T>{T(0), T(0)};
             },
-            [&](int i, double2 v) { sx[i / MV_CHUNK][i % MV_CHUNK] = v; });
+            [&](int i, Cx<T> v) { sM[(i / TG_KC) * (TG_KC + 1) + i % TG_KC] = v; });
+        batched_copy<TG_THREADS, 8, double2>(
+            TG_KC * TG_RC,
+            [&](int i) {
+                const int c = i / TG_KC, k = i % TG_KC;  // consecutive threads: consecutive k of one column
+                return (c < rc && k < kn) ? X[(size_t)(r0 + c) * K + k0 + k] : make_double2(0, 0);
+            },
+            [&](int i, double2 v) { sX[(i % TG_KC) * TG_RC + i / TG_KC] = v; });
         __syncthreads();
-        for (int jj = lane; jj < MV_CHUNK && j0 + jj < n; jj += 32) {
+#pragma unroll 4
+        for (int k = 0; k < TG_KC; ++k) {
+            const Cx<T> m0 = sM[tr * (TG_KC + 1) + k], m1 = sM[(tr + 32) * (TG_KC + 1) + k];
+            const double a0r = (double)m0.re, a0i = (double)m0.im, a1r = (double)m1.re, a1i = (double)m1.im;
 #pragma unroll
-            for (int a = 0; a < MV_ROWS_PER_WARP; ++a) {
-                const int row = row0 + a;
-                if (row >= n) break;
-                const Cx<T> v = A[(int64_t)row * ld + j0 + jj];
-                const double vr = (double)v.re, vi = (double)v.im;
-#pragma unroll
-                for (int r = 0; r < MV_RC; ++r) {
-                    const double2 x = sx[r][jj];
-                    ar[a][r] += vr * x.x - vi * x.y;
-                    ai[a][r] += vr * x.y + vi * x.x;
-                }
+            for (int e = 0; e < 4; ++e) {
+                const double2 x = sX[k * TG_RC + tc + e];
+                ar[0][e] += a0r * x.x - a0i * x.y;
+                ai[0][e] += a0r * x.y + a0i * x.x;
+                ar[1][e] += a1r * x.x - a1i * x.y;
+                ai[1][e] += a1r * x.y + a1i * x.x;
             }
         }
+        __syncthreads();
     }
 #pragma unroll
-    for (int a = 0; a < MV_ROWS_PER_WARP; ++a)
+    for (int h = 0; h < 2; ++h) {
+        const int row = row0 + tr + 32 * h;
+        if (row >= rows) continue;
 #pragma unroll
-        for (int r = 0; r < MV_RC; ++r)
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                ar[a][r] += __shfl_xor_sync(0xffffffffu, ar[a][r], o);
-                ai[a][r] += __shfl_xor_sync(0xffffffffu, ai[a][r], o);
+        for (int e = 0; e < 4; ++e)
+            if (tc + e < rc) {
+                double2 *y = &Y[(size_t)(r0 + tc + e) * rows + row];
+                atomicAdd(&y->x, alpha * ar[h][e]);
+                atomicAdd(&y->y, alpha * ai[h][e]);
             }
-#pragma unroll
-    for (int a = 0; a < MV_ROWS_PER_WARP; ++a) {
-        const int row = row0 + a;
-        if (row < n && lane < rc) {
-            double vr = 0, vi = 0;
-#pragma unroll
-            for (int r = 0; r < MV_RC; ++r)
-                if (r == lane) {
-                    vr = ar[a][r];
-                    vi = ai[a][r];
-                }
-            double2 &y = Y[(size_t)(r0 + lane) * n + row];
-            const double2 old = beta != 0.0 ? y : make_double2(0, 0);
-            y = make_double2(alpha * vr + beta * old.x, alpha * vi + beta * old.y);
-        }
     }
 }
 
+// Y += alpha * M X for all R columns (Y must hold its starting value)
+template <typename T>
+void tall_gemm(cudaStream_t st, int sm_count, const Cx<T> *M, int64_t ld, int rows, int K, const double *X, double *Y,
+               int R, double alpha) {
+    const size_t smem = sizeof(Cx<T>) * TG_ROWS * (TG_KC + 1) + sizeof(double2) * TG_KC * TG_RC;
+    BB_CUDA(cudaFuncSetAttribute(tall_gemm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int row_tiles = (rows + TG_ROWS - 1) / TG_ROWS;
+    // K slices so that the grid covers the GPU about four times
+    int slices = std::max(1, (4 * sm_count + row_tiles - 1) / row_tiles);
+    int kslice = (K + slices - 1) / slices;
+    kslice = (kslice + TG_KC - 1) / TG_KC * TG_KC;
+    slices = (K + kslice - 1) / kslice;
+    for (int r0 = 0; r0 < R; r0 += TG_RC)
+        tall_gemm_kernel<T><<<dim3(row_tiles, slices), TG_THREADS, smem, st>>>(
+            M, ld, rows, K, reinterpret_cast<const double2 *>(X), reinterpret_cast<double2 *>(Y), R, r0, alpha, kslice);
+    BB_CUDA(cudaGetLastError());
+}
+template void tall_gemm<float>(cudaStream_t, int, const Cx<float> *, int64_t, int, int, const double *, double *, int,
+                               double);
+template void tall_gemm<double>(cudaStream_t, int, const Cx<double> *, int64_t, int, int, const double *, double *,
+                                int, double);
+
+// Y = alpha * A X + beta * Y with beta in {0, 1}
 template <typename T> static void matvec(beat_b200_ctx *c, const Cx<T> *A, const double *X, double *Y, int R,
                                          double alpha, double beta) {
     const int n = c->V;
-    const int rows_per_cta = MV_WARPS * MV_ROWS_PER_WARP;
-    for (int r0 = 0; r0 < R; r0 += MV_RC)
-        matvec_kernel<T><<<(n + rows_per_cta - 1) / rows_per_cta, 256, 0, c->stream>>>(
-            A, c->ws.ld, n, reinterpret_cast<const double2 *>(X), reinterpret_cast<double2 *>(Y), R, r0, alpha, beta);
-    BB_CUDA(cudaGetLastError());
+    if (beta == 0.0) BB_CUDA(cudaMemsetAsync(Y, 0, sizeof(double2) * (size_t)n * R, c->stream));
+    tall_gemm<T>(c->stream, c->sm_count, A, c->ws.ld, n, n, X, Y, R, alpha);
 }
 
 // H[i*R + r] = sum_n conj(V_i[n, r]) W[n, r] for i < nv   (one CTA per (i, r))

@@ -204,7 +204,10 @@ void lu_factor(beat_b200_ctx *c, int precision, int nb, int split_terms);
 void lu_solve_fp64(beat_b200_ctx *c, int R, double *x_dev);          // in place, N x R col-major
 void lu_precond_fp32(beat_b200_ctx *c, int R, const double *in, double *out);
 
-// gmres.cu
+// gmres.cu: Y += alpha * M X (M complex row-major rows x K, X/Y FP64 column-major)
+template <typename T>
+void tall_gemm(cudaStream_t st, int sm_count, const Cx<T> *M, int64_t ld, int rows, int K, const double *X, double *Y,
+               int R, double alpha);
 struct IrResult {
     int iterations;
     int converged;
