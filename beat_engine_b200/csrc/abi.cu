@@ -242,7 +242,7 @@ int32_t beat_b200_solve(beat_b200_ctx *c, double k, double eta, int32_t R, const
         ensure_workspace(c, o.precision, R);
         Workspace &w = c->ws;
         BB_CUDA(cudaMemcpyAsync(w.q.p, q, (size_t)c->F * R * 16, cudaMemcpyHostToDevice, c->stream));
-        DevBuf out;
+        DevBuf &out = w.io;
         out.alloc((size_t)c->V * R * 16);
         try {
             solve_core(c, k, eta, R, w.q.as<double>(), o, out.as<double>(), diag);
@@ -250,10 +250,8 @@ int32_t beat_b200_solve(beat_b200_ctx *c, double k, double eta, int32_t R, const
             BB_CUDA(cudaStreamSynchronize(c->stream));
         } catch (...) {
             if (c->stream) cudaStreamSynchronize(c->stream);
-            out.free_();
             throw;
         }
-        out.free_();
     });
 }
 
@@ -264,7 +262,7 @@ static int32_t field_common(beat_b200_ctx *c, double k, int32_t M, const double 
         BB_REQUIRE(M >= 0 && R >= 1 && (M == 0 || (pts && p && q && out)), BEAT_B200_INVALID_ARG,
                    "field: bad arguments");
         if (M == 0) return;
-        DevBuf buf;
+        DevBuf &buf = c->ws.io;
         buf.alloc(16 * ((size_t)c->V * R + (size_t)c->F * R + (size_t)M * R));
         try {
             double *dp = buf.as<double>(), *dq = dp + 2 * (size_t)c->V * R, *dout = dq + 2 * (size_t)c->F * R;
@@ -274,10 +272,9 @@ static int32_t field_common(beat_b200_ctx *c, double k, int32_t M, const double 
             BB_CUDA(cudaMemcpyAsync(out, dout, (size_t)M * R * 16, cudaMemcpyDeviceToHost, c->stream));
             BB_CUDA(cudaStreamSynchronize(c->stream));
         } catch (...) {
-            buf.free_();
+            if (c->stream) cudaStreamSynchronize(c->stream);
             throw;
         }
-        buf.free_();
     });
 }
 

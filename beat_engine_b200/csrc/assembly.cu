@@ -71,7 +71,16 @@ void upload_rule_tables(const std::vector<double> &pts, const std::vector<double
 }
 
 __device__ __forceinline__ void sincos_t(double x, double *s, double *c) { sincos_cw(x, s, c); }
-__device__ __forceinline__ void sincos_t(float x, float *s, float *c) { sincos_cw(x, s, c); }
+// FP32 phase: reduced to [-pi, pi] by a two-part 2 pi (6.2831854820251465 is
+// 2 pi rounded to float, -1.7484555e-7 the remainder), then the hardware
+// approximation, whose absolute error on [-pi, pi] (about 2^-21.4) is below
+// the rounding error of the FP32 phase k r itself.
+__device__ __forceinline__ void sincos_t(float x, float *s, float *c) {
+    const float n = rintf(x * 0.15915493667125702f);
+    float r = fmaf(-n, 6.2831854820251465f, x);
+    r = fmaf(-n, -1.7484555314695172e-07f, r);
+    __sincosf(r, s, c);
+}
 __device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
 __device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
 
@@ -116,7 +125,9 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
     T *sn = sq + TS * Q * 3;                          // 3 x TS
     T *sc = sn + TS * 3;                              // 9 x TS
     T *sa = sc + TS * 9;                              // TS
-    int *tgv = reinterpret_cast<int *>(sa + TS);      // TT x 3
+    T *tpl = sa + TS;                                 // TT: plane offset x . n of each test face
+    T *spl = tpl + TT;                                // TS: plane offset y . n of each trial face
+    int *tgv = reinterpret_cast<int *>(spl + TS);     // TT x 3
     int *tlv = tgv + TT * 3;                          // TT x 3
     int *sgv = tlv + TT * 3;                          // 3 x TS
     int *slv = sgv + TS * 3;                          // 3 x TS
@@ -153,6 +164,12 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
     }
     for (int i = tid; i < ns; i += REG_THREADS) sa[i] = g.area[s0 + i];
     __syncthreads();
+    // every point y of a flat face has the same y . n
+    for (int i = tid; i < nt; i += REG_THREADS)
+        tpl[i] = tq[i * Q * 3] * tn[3 * i] + tq[i * Q * 3 + 1] * tn[3 * i + 1] + tq[i * Q * 3 + 2] * tn[3 * i + 2];
+    for (int i = tid; i < ns; i += REG_THREADS)
+        spl[i] = sq[i] * sn[i] + sq[TS + i] * sn[TS + i] + sq[2 * TS + i] * sn[2 * TS + i];
+    __syncthreads();
 
     const T k = g.k, eta = g.eta;
     const T inv4pi = T(0.07957747154594767);  // 1 / (4 pi)
@@ -168,6 +185,8 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
         const T ntx = tn[3 * tl], nty = tn[3 * tl + 1], ntz = tn[3 * tl + 2];
         const T nsx = sn[sl], nsy = sn[TS + sl], nsz = sn[2 * TS + sl];
         const T k2n = eta * g.k2 * (ntx * nsx + nty * nsy + ntz * nsz);
+        // with r = y - x:  r . n_s = ds - x . n_s  and  -r . n_t = dt - y . n_t
+        const T ds = spl[sl], dt = tpl[tl];
         T L[9][2], Rv[3][2], cr = T(0), ci = T(0);
 #pragma unroll
         for (int i = 0; i < 9; ++i) L[i][0] = L[i][1] = T(0);
@@ -177,31 +196,27 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
         for (int qt = 0; qt < Q; ++qt) {
             const T x0 = tq[(tl * Q + qt) * 3], x1 = tq[(tl * Q + qt) * 3 + 1], x2 = tq[(tl * Q + qt) * 3 + 2];
             const T wt = RuleRef<T>::w(RI, qt) * inv4pi;
-            T S0r = 0, S0i = 0, S1r = 0, S1i = 0, S2r = 0, S2i = 0, Ur = 0, Ui = 0;
+            const T xns = ds - (x0 * nsx + x1 * nsy + x2 * nsz);
+            T S0r = 0, S0i = 0, S1r = 0, S1i = 0, S2r = 0, S2i = 0, Gr = 0, Gi = 0, Wr = 0, Wi = 0;
 #pragma unroll
             for (int qs = 0; qs < Q; ++qs) {
-                const T rx = sq[(qs * 3) * TS + sl] - x0;
-                const T ry = sq[(qs * 3 + 1) * TS + sl] - x1;
-                const T rz = sq[(qs * 3 + 2) * TS + sl] - x2;
+                const T y0 = sq[(qs * 3) * TS + sl], y1 = sq[(qs * 3 + 1) * TS + sl], y2 = sq[(qs * 3 + 2) * TS + sl];
+                const T rx = y0 - x0, ry = y1 - x1, rz = y2 - x2;
                 const T r2 = rx * rx + ry * ry + rz * rz;
                 const T ir = rsqrt_t(r2);
-                const T rad = r2 * ir;
                 T sn_, cs_;
-                sincos_t(k * rad, &sn_, &cs_);
+                sincos_t(k * (r2 * ir), &sn_, &cs_);
                 const T scl = ir * (wt * RuleRef<T>::w(RI, qs));
                 const T gr = cs_ * scl, gi = sn_ * scl;           // weighted green
-                const T gsr = -gr * ir - gi * k;                  // weighted grad scale
+                const T gsr = -gr * ir - gi * k;                  // weighted d green / d r
                 const T gsi = gr * k - gi * ir;
-                const T dns = (rx * nsx + ry * nsy + rz * nsz) * ir;
-                const T dnt = -(rx * ntx + ry * nty + rz * ntz) * ir;
-                const T lr = -gsr * dns + k2n * gi;               // -grad*dn_s - i k2n g
-                const T li = -gsi * dns - k2n * gr;
-                const T rr = -gr + eta * (gsi * dnt);             // -g - i eta grad*dn_t
-                const T ri = -gi - eta * (gsr * dnt);
-                cr += gr;
-                ci += gi;
-                Ur += rr;
-                Ui += ri;
+                const T dns = xns * ir, dnt = (dt - (y0 * ntx + y1 * nty + y2 * ntz)) * ir;
+                const T lr = k2n * gi - gsr * dns;                // -grad*dn_s - i k2n g
+                const T li = -(gsi * dns + k2n * gr);
+                Gr += gr;
+                Gi += gi;
+                Wr += dnt * gsr;
+                Wi += dnt * gsi;
                 const T b0 = RuleRef<T>::b(RI, qs, 0), b1 = RuleRef<T>::b(RI, qs, 1), b2 = RuleRef<T>::b(RI, qs, 2);
                 S0r += b0 * lr;
                 S0i += b0 * li;
@@ -210,6 +225,10 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
                 S2r += b2 * lr;
                 S2i += b2 * li;
             }
+            // sum over the trial points of -g - i eta grad*dn_t
+            const T Ur = -Gr + eta * Wi, Ui = -Gi - eta * Wr;
+            cr += Gr;
+            ci += Gi;
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
                 const T ba = RuleRef<T>::b(RI, qt, a);
@@ -260,7 +279,7 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
 }
 
 template <typename T, int Q> static size_t regular_smem_bytes() {
-    return sizeof(Cx<T>) * (VT * VS + VT * TS) + sizeof(T) * (TT * (Q * 3 + 3 + 9 + 1) + TS * (Q * 3 + 3 + 9 + 1)) +
+    return sizeof(Cx<T>) * (VT * VS + VT * TS) + sizeof(T) * (TT * (Q * 3 + 3 + 9 + 2) + TS * (Q * 3 + 3 + 9 + 2)) +
            sizeof(int) * (TT * 6 + TS * 6);
 }
 

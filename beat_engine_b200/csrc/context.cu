@@ -516,7 +516,7 @@ void ensure_workspace(beat_b200_ctx *c, int precision, int R) {
 void release_workspace(beat_b200_ctx *c) {
     Workspace &w = c->ws;
     for (DevBuf *b : {&w.A, &w.Aop, &w.B, &w.b, &w.x, &w.ipiv, &w.perm, &w.panel_scratch, &w.stage, &w.krylov,
-                      &w.small, &w.q, &w.small_solve, &w.dinv})
+                      &w.small, &w.q, &w.small_solve, &w.dinv, &w.field, &w.io})
         b->free_();
     w.precision = -1;
     w.N = w.F = w.R = 0;
@@ -528,7 +528,7 @@ int64_t device_bytes(const beat_b200_ctx *c) {
     int64_t s = 0;
     const Workspace &w = c->ws;
     for (const DevBuf *b : {&w.A, &w.Aop, &w.B, &w.b, &w.x, &w.ipiv, &w.perm, &w.panel_scratch, &w.stage, &w.krylov,
-                            &w.small, &w.q, &w.small_solve, &w.dinv})
+                            &w.small, &w.q, &w.small_solve, &w.dinv, &w.field, &w.io})
         s += (int64_t)b->bytes;
     for (const DevBuf *b : {&c->pos_face, &c->pos_qpts64, &c->pos_qpts32, &c->pos_normal64, &c->pos_normal32,
                             &c->pos_curl64, &c->pos_curl32, &c->pos_area64, &c->pos_area32, &c->pos_gvert,

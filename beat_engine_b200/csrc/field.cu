@@ -151,13 +151,13 @@ void farfield(beat_b200_ctx *c, double k, int M, const double *pts_host, int R, 
         rw3[4 * q + 2] = c->rule_pts[2 * q];
         rw3[4 * q + 3] = c->rule_pts[2 * q + 1];
     }
-    DevBuf scratch;
+    DevBuf &scratch = c->ws.field;  // kept across calls: no allocation on the steady path
     // doubles before the double2 arrays, rounded up to an even count so the
     // double2 arrays start on a 16-byte boundary
     const size_t nd = (4 * (size_t)Q + 6 * (size_t)S + 3 * (size_t)M + 1) & ~(size_t)1;
     const size_t bytes = sizeof(double) * nd + sizeof(double2) * 2 * (size_t)S * R;
     scratch.alloc(bytes);
-    try {
+    {
         double *d_rw = scratch.as<double>();
         double *ys = d_rw + 4 * Q, *ns = ys + 3 * (size_t)S, *d_pts = ns + 3 * (size_t)S;
         double2 *ps = reinterpret_cast<double2 *>(d_rw + nd), *qs = ps + (size_t)S * R;
@@ -184,11 +184,7 @@ void farfield(beat_b200_ctx *c, double k, int M, const double *pts_host, int R, 
             BB_CUDA(cudaGetLastError());
         }
         BB_CUDA(cudaStreamSynchronize(c->stream));
-    } catch (...) {
-        scratch.free_();
-        throw;
     }
-    scratch.free_();
 }
 
 }  // namespace bb

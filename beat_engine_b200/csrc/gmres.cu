@@ -24,67 +24,73 @@
 namespace bb {
 
 // ---------------------------------------------------------------------------
-// Y[:, r0:r0+16] += alpha * M X  with M complex (T, row-major, ld), X and Y
-// FP64 column-major (X: K x R, Y: rows x R).  A CTA owns 64 rows x 16 columns
-// over a slice of K and adds its partial sums with FP64 atomics.  Each thread
-// keeps a 2 x 4 complex block; M and X chunks go through shared memory.
+// Tall-skinny complex product Y += alpha M X (M rows x K complex in the
+// workspace precision, row-major; X, Y FP64 column-major with R columns).
+// One thread per row of M, all TG_RC right-hand sides of a chunk in FP64
+// registers: an M entry read from shared memory feeds 4 TG_RC DFMA, the X
+// entries are warp-broadcast loads.  The K range is cut into slices so that
+// about two CTAs per SM are resident; slices add into Y with FP64 atomics.
+// Bound: FP64 FMA issue (4 DFMA per complex multiply-add).
 // ---------------------------------------------------------------------------
-constexpr int TG_ROWS = 64, TG_KC = 64, TG_RC = 16, TG_THREADS = 128;
+constexpr int TG_THREADS = 256, TG_RC = 16;
+template <typename T> struct TgChunk {
+    static constexpr int KC = 32;  // K entries per shared-memory chunk (c64 M)
+};
+template <> struct TgChunk<double> {
+    static constexpr int KC = 16;
+};
 
 template <typename T>
-__global__ void __launch_bounds__(TG_THREADS) tall_gemm_kernel(const Cx<T> *M, int64_t ld, int rows, int K,
-                                                               const double2 *X, double2 *Y, int R, int r0,
-                                                               double alpha, int kslice) {
+__global__ void __launch_bounds__(TG_THREADS, 2) tall_gemm_kernel(const Cx<T> *M, int64_t ld, int rows, int K,
+                                                                  const double2 *X, double2 *Y, int R, int r0,
+                                                                  double alpha, int kslice) {
+    constexpr int KC = TgChunk<T>::KC;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Cx<T> *sM = reinterpret_cast<Cx<T> *>(smem_raw);                                // TG_ROWS x (TG_KC + 1)
-    double2 *sX = reinterpret_cast<double2 *>(smem_raw + sizeof(Cx<T>) * TG_ROWS * (TG_KC + 1));  // TG_KC x TG_RC
-    const int row0 = blockIdx.x * TG_ROWS;
+    Cx<T> *sM = reinterpret_cast<Cx<T> *>(smem_raw);                                          // TG_THREADS x (KC + 1)
+    double2 *sX = reinterpret_cast<double2 *>(smem_raw + sizeof(Cx<T>) * TG_THREADS * (KC + 1));  // KC x TG_RC
+    const int row0 = blockIdx.x * TG_THREADS, row = row0 + (int)threadIdx.x;
     const int kb = blockIdx.y * kslice, ke = min(K, kb + kslice);
     const int rc = min(TG_RC, R - r0);
-    const int tr = threadIdx.x >> 2, tc = (threadIdx.x & 3) * 4;  // rows tr, tr + 32; columns tc..tc+3
-    double ar[2][4] = {}, ai[2][4] = {};
-    for (int k0 = kb; k0 < ke; k0 += TG_KC) {
-        const int kn = min(TG_KC, ke - k0);
-        batched_copy<TG_THREADS, 8, Cx<T>>(
-            TG_ROWS * TG_KC,
+    double ar[TG_RC], ai[TG_RC];
+#pragma unroll
+    for (int e = 0; e < TG_RC; ++e) ar[e] = ai[e] = 0.0;
+    for (int k0 = kb; k0 < ke; k0 += KC) {
+        const int kn = min(KC, ke - k0);
+        batched_copy<TG_THREADS, 4, Cx<T>>(
+            TG_THREADS * KC,
             [&](int i) {
-                const int r = i / TG_KC, k = i % TG_KC;
+                const int r = i / KC, k = i % KC;  // consecutive threads: consecutive k of one row
                 return (row0 + r < rows && k < kn) ? M[(int64_t)(row0 + r) * ld + k0 + k] : Cx<T>{T(0), T(0)};
             },
-            [&](int i, Cx<T> v) { sM[(i / TG_KC) * (TG_KC + 1) + i % TG_KC] = v; });
-        batched_copy<TG_THREADS, 8, double2>(
-            TG_KC * TG_RC,
+            [&](int i, Cx<T> v) { sM[(i / KC) * (KC + 1) + i % KC] = v; });
+        batched_copy<TG_THREADS, 2, double2>(
+            KC * TG_RC,
             [&](int i) {
-                const int c = i / TG_KC, k = i % TG_KC;  // consecutive threads: consecutive k of one column
+                const int c = i / KC, k = i % KC;
                 return (c < rc && k < kn) ? X[(size_t)(r0 + c) * K + k0 + k] : make_double2(0, 0);
             },
-            [&](int i, double2 v) { sX[(i % TG_KC) * TG_RC + i / TG_KC] = v; });
+            [&](int i, double2 v) { sX[(i % KC) * TG_RC + i / KC] = v; });
         __syncthreads();
-#pragma unroll 4
-        for (int k = 0; k < TG_KC; ++k) {
-            const Cx<T> m0 = sM[tr * (TG_KC + 1) + k], m1 = sM[(tr + 32) * (TG_KC + 1) + k];
-            const double a0r = (double)m0.re, a0i = (double)m0.im, a1r = (double)m1.re, a1i = (double)m1.im;
+#pragma unroll 2
+        for (int k = 0; k < KC; ++k) {
+            const Cx<T> m = sM[threadIdx.x * (KC + 1) + k];
+            const double mr = (double)m.re, mi = (double)m.im;
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const double2 x = sX[k * TG_RC + tc + e];
-                ar[0][e] += a0r * x.x - a0i * x.y;
-                ai[0][e] += a0r * x.y + a0i * x.x;
-                ar[1][e] += a1r * x.x - a1i * x.y;
-                ai[1][e] += a1r * x.y + a1i * x.x;
+            for (int e = 0; e < TG_RC; ++e) {
+                const double2 x = sX[k * TG_RC + e];
+                ar[e] = fma(mr, x.x, fma(-mi, x.y, ar[e]));
+                ai[e] = fma(mr, x.y, fma(mi, x.x, ai[e]));
             }
         }
         __syncthreads();
     }
+    if (row < rows) {
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int row = row0 + tr + 32 * h;
-        if (row >= rows) continue;
-#pragma unroll
-        for (int e = 0; e < 4; ++e)
-            if (tc + e < rc) {
-                double2 *y = &Y[(size_t)(r0 + tc + e) * rows + row];
-                atomicAdd(&y->x, alpha * ar[h][e]);
-                atomicAdd(&y->y, alpha * ai[h][e]);
+        for (int e = 0; e < TG_RC; ++e)
+            if (e < rc) {
+                double2 *y = &Y[(size_t)(r0 + e) * rows + row];
+                atomicAdd(&y->x, alpha * ar[e]);
+                atomicAdd(&y->y, alpha * ai[e]);
             }
     }
 }
@@ -93,13 +99,14 @@ __global__ void __launch_bounds__(TG_THREADS) tall_gemm_kernel(const Cx<T> *M, i
 template <typename T>
 void tall_gemm(cudaStream_t st, int sm_count, const Cx<T> *M, int64_t ld, int rows, int K, const double *X, double *Y,
                int R, double alpha) {
-    const size_t smem = sizeof(Cx<T>) * TG_ROWS * (TG_KC + 1) + sizeof(double2) * TG_KC * TG_RC;
+    constexpr int KC = TgChunk<T>::KC;
+    const size_t smem = sizeof(Cx<T>) * TG_THREADS * (KC + 1) + sizeof(double2) * KC * TG_RC;
     BB_CUDA(cudaFuncSetAttribute(tall_gemm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int row_tiles = (rows + TG_ROWS - 1) / TG_ROWS;
-    // K slices so that the grid covers the GPU about four times
-    int slices = std::max(1, (4 * sm_count + row_tiles - 1) / row_tiles);
+    const int row_tiles = (rows + TG_THREADS - 1) / TG_THREADS;
+    // K slices so that about two CTAs per SM run
+    int slices = std::max(1, (2 * sm_count + row_tiles / 2) / row_tiles);
     int kslice = (K + slices - 1) / slices;
-    kslice = (kslice + TG_KC - 1) / TG_KC * TG_KC;
+    kslice = (kslice + KC - 1) / KC * KC;
     slices = (K + kslice - 1) / kslice;
     for (int r0 = 0; r0 < R; r0 += TG_RC)
         tall_gemm_kernel<T><<<dim3(row_tiles, slices), TG_THREADS, smem, st>>>(

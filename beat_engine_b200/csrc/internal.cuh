@@ -118,6 +118,8 @@ struct Workspace {
     DevBuf q;             // F x R FP64 Neumann data (column-major)
     DevBuf small_solve;   // block-substitution claim counter and per-block flags
     DevBuf dinv;          // FP64 inverses of the 64 x 64 diagonal blocks of L and U
+    DevBuf field;         // field sources and evaluation points (grow-only)
+    DevBuf io;            // device staging of the host-buffer entry points (grow-only)
     int solve_epoch = 0;  // flag value of the latest substitution launch
     int lu_valid = 0;     // factors match the current operator
 };

@@ -39,6 +39,9 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
 }
 
 template <typename T> __device__ __forceinline__ T cabs1(Cx<T> v) { return fabs(v.re) + fabs(v.im); }
+template <typename T> __device__ __forceinline__ Cx<T> cms(Cx<T> x, Cx<T> l, Cx<T> u) {  // x - l u
+    return Cx<T>{x.re - (l.re * u.re - l.im * u.im), x.im - (l.re * u.im + l.im * u.re)};
+}
 
 // L2-coherent loads of values other CTAs published before a grid barrier
 __device__ __forceinline__ Cx<double> ldcg(const Cx<double> *p) {
@@ -254,7 +257,7 @@ __global__ void laswp_kernel(Cx<T> *A, int64_t ld, int n, int k, int nb, const i
     if (c == -1) {
         for (int j = 0; j < jmax; ++j) {
             const int p = sp[j];
-            if (p != k + j) {
+            if (p > k + j && p < n) {
                 const int t = perm[k + j];
                 perm[k + j] = perm[p];
                 perm[p] = t;
@@ -265,7 +268,7 @@ __global__ void laswp_kernel(Cx<T> *A, int64_t ld, int n, int k, int nb, const i
     if (c >= n || (c >= k && c < k + nb)) return;
     for (int j = 0; j < jmax; ++j) {
         const int p = sp[j];
-        if (p != k + j) {
+        if (p > k + j && p < n) {  // an interchange always names a later row
             const Cx<T> t = A[(int64_t)(k + j) * ld + c];
             A[(int64_t)(k + j) * ld + c] = A[(int64_t)p * ld + c];
             A[(int64_t)p * ld + c] = t;
@@ -313,6 +316,122 @@ __global__ void __launch_bounds__(256) trsm_kernel(Cx<T> *A, int64_t ld, int n, 
     for (int i = threadIdx.x; i < kb * TRSM_COLS; i += blockDim.x) {
         const int r = i / TRSM_COLS, c = i % TRSM_COLS;
         if (c < nc) A[(int64_t)(k + r) * ld + c0 + c] = X[r * TRSM_COLS + c];
+    }
+}
+
+// Inverse of a unit lower triangular kb x kb block (kb <= W <= 32), by one
+// warp: lane c forward-substitutes column c of the inverse with four partial
+// sums per row.  L holds the strictly lower part (row stride ldl), Y is W x
+// (W + 1) scratch, D receives the W x W inverse row-major (identity past kb).
+template <typename T>
+__device__ __forceinline__ void warp_unit_lower_inverse(const Cx<T> *L, int ldl, int kb, int W, Cx<T> *Y, Cx<T> *D) {
+    const int c = threadIdx.x & 31, ldy = W + 1;
+    if (c < W) {
+        for (int i = 0; i < W; ++i) {
+            Cx<T> s0{T(i == c), T(0)}, s1{T(0), T(0)}, s2{T(0), T(0)}, s3{T(0), T(0)};
+            if (i > c && i < kb) {
+                int t = c;
+                for (; t + 4 <= i; t += 4) {
+                    s0 = cms(s0, L[i * ldl + t], Y[t * ldy + c]);
+                    s1 = cms(s1, L[i * ldl + t + 1], Y[(t + 1) * ldy + c]);
+                    s2 = cms(s2, L[i * ldl + t + 2], Y[(t + 2) * ldy + c]);
+                    s3 = cms(s3, L[i * ldl + t + 3], Y[(t + 3) * ldy + c]);
+                }
+                for (; t < i; ++t) s0 = cms(s0, L[i * ldl + t], Y[t * ldy + c]);
+            }
+            Y[i * ldy + c] = Cx<T>{(s0.re + s1.re) + (s2.re + s3.re), (s0.im + s1.im) + (s2.im + s3.im)};
+        }
+        for (int i = 0; i < W; ++i) D[(size_t)i * W + c] = Y[i * ldy + c];
+    }
+}
+
+// The same for the diagonal block A[k:k+kb, k:k+kb] (kb = min(W, n - k)) of
+// a sub-panel factored by the grid-wide panel kernel.
+template <typename T>
+__global__ void __launch_bounds__(32) diag_block_inverse_kernel(const Cx<T> *A, int64_t ld, int n, int k, int W, Cx<T> *D) {
+    __shared__ Cx<T> L[32 * 33];
+    __shared__ Cx<T> Y[32 * 33];
+    const int kb = min(W, n - k);
+    batched_copy<32, 32, Cx<T>>(
+        kb * kb, [&](int i) { return A[(int64_t)(k + i / kb) * ld + k + i % kb]; },
+        [&](int i, Cx<T> v) { L[(i / kb) * 33 + i % kb] = v; });
+    __syncwarp();
+    warp_unit_lower_inverse(L, 33, kb, W, Y, D);
+}
+
+// Blocked U12 = L11^-1 A12 for L11 = A[k:k+kb, k:k+kb] (kb = S W) with the
+// inverses D_s of its W x W diagonal blocks:  X_s = D_s (A_s - sum_{t<s}
+// L_st X_t), s = 0..S-1.  32 columns per CTA, 256 threads, each thread W/8
+// complex outputs of a W x 32 block per product; one barrier per block step
+// instead of one per row.
+constexpr int TB_COLS = 32;
+template <typename T, int W>
+__global__ void __launch_bounds__(256) trsm_blocked_kernel(Cx<T> *A, int64_t ld, int k, int S, const Cx<T> *D,
+                                                            int c_begin, int c_end) {
+    constexpr int OPT = W * TB_COLS / 256;  // outputs per thread: 4 (W = 32) or 2 (W = 16)
+    constexpr int CG = TB_COLS / OPT;       // column groups
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int kb = S * W;
+    Cx<T> *X = reinterpret_cast<Cx<T> *>(smem_raw);  // kb x TB_COLS
+    Cx<T> *Dt = X + (size_t)kb * TB_COLS;             // W x (W + 1)
+    Cx<T> *Lt = Dt + W * (W + 1);                     // W x (r0 + 1), r0 <= kb - W
+    const int tid = threadIdx.x, r = tid / CG, cg = tid % CG;
+    const int c0 = c_begin + blockIdx.x * TB_COLS;
+    const int nc = min(TB_COLS, c_end - c0);
+    batched_copy<256, 8, Cx<T>>(
+        kb * TB_COLS,
+        [&](int i) {
+            const int c = i % TB_COLS;
+            return c < nc ? A[(int64_t)(k + i / TB_COLS) * ld + c0 + c] : Cx<T>{T(0), T(0)};
+        },
+        [&](int i, Cx<T> v) { X[i] = v; });
+    for (int s = 0; s < S; ++s) {
+        const int r0 = s * W;
+        batched_copy<256, 4, Cx<T>>(
+            W * W, [&](int i) { return D[(size_t)s * W * W + i]; },
+            [&](int i, Cx<T> v) { Dt[(i / W) * (W + 1) + i % W] = v; });
+        if (s > 0)
+            batched_copy<256, 8, Cx<T>>(
+                W * r0, [&](int i) { return A[(int64_t)(k + r0 + i / r0) * ld + k + i % r0]; },
+                [&](int i, Cx<T> v) { Lt[(i / r0) * (r0 + 1) + i % r0] = v; });
+        __syncthreads();
+        Cx<T> acc[OPT];
+#pragma unroll
+        for (int o = 0; o < OPT; ++o) acc[o] = X[(r0 + r) * TB_COLS + cg * OPT + o];
+        for (int t = 0; t < r0; ++t) {  // A_s - L_s,<s X_<s
+            const Cx<T> l = Lt[r * (r0 + 1) + t];
+#pragma unroll
+            for (int o = 0; o < OPT; ++o) {
+                const Cx<T> x = X[t * TB_COLS + cg * OPT + o];
+                acc[o].re -= l.re * x.re - l.im * x.im;
+                acc[o].im -= l.re * x.im + l.im * x.re;
+            }
+        }
+        __syncthreads();  // every thread has read block s of X
+#pragma unroll
+        for (int o = 0; o < OPT; ++o) X[(r0 + r) * TB_COLS + cg * OPT + o] = acc[o];
+        __syncthreads();
+        Cx<T> y[OPT];
+#pragma unroll
+        for (int o = 0; o < OPT; ++o) y[o] = Cx<T>{T(0), T(0)};
+        for (int t = 0; t <= r; ++t) {  // D_s is lower triangular
+            const Cx<T> d = Dt[r * (W + 1) + t];
+#pragma unroll
+            for (int o = 0; o < OPT; ++o) {
+                const Cx<T> x = X[(r0 + t) * TB_COLS + cg * OPT + o];
+                y[o].re += d.re * x.re - d.im * x.im;
+                y[o].im += d.re * x.im + d.im * x.re;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int o = 0; o < OPT; ++o) X[(r0 + r) * TB_COLS + cg * OPT + o] = y[o];
+        // the next block step's loads of Dt / Lt follow the next barrier
+        __syncthreads();
+    }
+    for (int i = tid; i < kb * TB_COLS; i += 256) {
+        const int rr = i / TB_COLS, c = i % TB_COLS;
+        if (c < nc) A[(int64_t)(k + rr) * ld + c0 + c] = X[rr * TB_COLS + c];
     }
 }
 
@@ -386,45 +505,158 @@ __global__ void __launch_bounds__(256, 2) gemm_update_kernel(Cx<T> *A, int64_t l
 
 // ---------------------------------------------------------------------------
 // Sub-panel factorisation on one thread-block cluster.  CP_CTAS CTAs hold all
-// rows of a W-column sub-panel in shared memory.  Per column: local pivot
-// candidate, candidate value/row written into every CTA's shared memory
-// (distributed shared memory stores), the candidate's row and the current
-// diagonal row copied to a local publish buffer, one hardware cluster
-// barrier, every CTA picks the same winner from its own copy of the
-// candidates and reads the winner's row from the winner CTA's publish buffer.
-// Publish buffers and candidate slots alternate with the column parity, so
-// one barrier per column suffices.
+// rows of a w-column sub-panel (256-byte rows) in shared memory; rows never
+// move: each row carries its logical position, and an interchange only swaps
+// two positions.  Per column j:
+//   1. wait on this CTA's mbarrier until every CTA's candidate for column j
+//      (magnitude, position, and the whole candidate row, finished through
+//      step j - 1) has landed in this CTA's shared memory;
+//   2. every warp picks the same winner from the CP_CTAS candidates
+//      (redux.sync on the magnitude bits, then the smallest position);
+//   3. look-ahead: multipliers of column j and column j + 1 of every
+//      remaining row, each thread's best row, each warp's best row finished
+//      through step j into a staging buffer by the warp's lanes;
+//   4. one CTA barrier, the CTA's best row among the warps' rows, and warp q
+//      pushes it to CTA q (one 16-byte st.async per lane, complete_tx on the
+//      receiver's mbarrier);
+//   5. the remaining columns of step j are eliminated while the pushes fly.
+// Candidate slots and mbarriers rotate over three columns: a CTA still
+// eliminating column j - 1 reads that column's slot after it has pushed its
+// candidate for column j, so a peer that holds every candidate for j may push
+// j + 1, but never j + 2, before the slot of j - 1 is free.  The staging
+// buffers and the warp results alternate with the column parity: the one CTA
+// barrier of a column separates their writers from the previous readers.
+// Every wait is bounded.
 // ---------------------------------------------------------------------------
-constexpr int CP_CTAS = 16, CP_THREADS = 256;
+constexpr int CP_CTAS = 16, CP_THREADS = 512, CP_WARPS = CP_THREADS / 32, CP_RMAX = 2, CP_ROW_BYTES = 272,
+              CP_SLOTS = 3;
+static_assert(CP_WARPS == CP_CTAS, "warp q pushes to CTA q");
+constexpr int CP_NONE = 0x7fffffff;  // position of "no candidate"
+
+struct alignas(16) PivKey {
+    uint32_t w[4];  // magnitude bits (lo, hi), position, unused
+};
 
 __device__ __forceinline__ uint32_t cl_rank() {
     uint32_t r;
     asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
     return r;
 }
-__device__ __forceinline__ uint32_t cl_map(const void *p, uint32_t rank) {
-    uint32_t a = (uint32_t)__cvta_generic_to_shared(p), r;
+__device__ __forceinline__ uint32_t sm_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ uint32_t cl_map(uint32_t a, uint32_t rank) {
+    uint32_t r;
     asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
     return r;
 }
 __device__ __forceinline__ void cl_sync() {
     asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
-__device__ __forceinline__ void cl_st(uint32_t addr, double v) {
-    asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(addr), "d"(v) : "memory");
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
 }
-__device__ __forceinline__ void cl_st(uint32_t addr, int v) {
-    asm volatile("st.shared::cluster.b32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+__device__ __forceinline__ void mb_init(uint64_t *b, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sm_addr(b)), "r"(count) : "memory");
 }
-__device__ __forceinline__ Cx<double> cl_ld(uint32_t addr, const Cx<double> *) {
-    double x, y;
-    asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(x), "=d"(y) : "r"(addr) : "memory");
-    return Cx<double>{x, y};
+__device__ __forceinline__ void mb_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mb_arrive_expect(uint64_t *b, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sm_addr(b)), "r"(bytes) : "memory");
 }
-__device__ __forceinline__ Cx<float> cl_ld(uint32_t addr, const Cx<float> *) {
-    float x, y;
-    asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(x), "=f"(y) : "r"(addr) : "memory");
-    return Cx<float>{x, y};
+// true once the phase of the given parity completed (the thread may be
+// suspended up to about a microsecond inside)
+__device__ __forceinline__ bool mb_try(uint64_t *b, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(sm_addr(b)), "r"(parity), "r"(1000u)
+        : "memory");
+    return ok != 0;
+}
+// one row of 16-byte-aligned bytes between global and shared memory by the
+// bulk-copy engine (no multicast); the load completes on an mbarrier
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_s2g(void *dst, uint32_t src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_commit_wait_all() {
+    asm volatile("cp.async.bulk.commit_group;\n\tcp.async.bulk.wait_group 0;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void st_async16(uint32_t addr, uint4 v, uint32_t bar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, [%5];" ::"r"(
+                     addr),
+                 "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w), "r"(bar)
+                 : "memory");
+}
+
+// ordered bits of a non-negative magnitude (0 also stands for "none")
+__device__ __forceinline__ uint64_t mag_bits(float v) { return (uint64_t)__float_as_uint(v); }
+__device__ __forceinline__ uint64_t mag_bits(double v) { return (uint64_t)__double_as_longlong(v); }
+template <typename T> __device__ __forceinline__ T mag_value(uint64_t b);
+template <> __device__ __forceinline__ float mag_value<float>(uint64_t b) { return __uint_as_float((uint32_t)b); }
+template <> __device__ __forceinline__ double mag_value<double>(uint64_t b) { return __longlong_as_double((long long)b); }
+
+// lane holding the largest magnitude, the smallest position among equals
+// (all 32 lanes take part; the result is the same in every lane)
+template <typename T> __device__ __forceinline__ int warp_argbest(uint64_t m, int pos) {
+    bool tie;
+    if (sizeof(T) == 8) {
+        const uint32_t hi = (uint32_t)(m >> 32), lo = (uint32_t)m;
+        const uint32_t mhi = __reduce_max_sync(0xffffffffu, hi);
+        const uint32_t mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+        tie = hi == mhi && lo == mlo;
+    } else {
+        const uint32_t mm = __reduce_max_sync(0xffffffffu, (uint32_t)m);
+        tie = (uint32_t)m == mm;
+    }
+    const int mpos = __reduce_min_sync(0xffffffffu, tie ? pos : CP_NONE);
+    return __ffs(__ballot_sync(0xffffffffu, tie && pos == mpos)) - 1;
+}
+
+// 16 bytes of a row: 2 c64 or 1 c128 entries
+__device__ __forceinline__ float4 v16_ld(const Cx<float> *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ double2 v16_ld(const Cx<double> *p) { return *reinterpret_cast<const double2 *>(p); }
+__device__ __forceinline__ void v16_st(Cx<float> *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
+__device__ __forceinline__ void v16_st(Cx<double> *p, double2 v) { *reinterpret_cast<double2 *>(p) = v; }
+__device__ __forceinline__ float4 v16_cms(float4 x, Cx<float> l, float4 u) {
+    const Cx<float> a = cms(Cx<float>{x.x, x.y}, l, Cx<float>{u.x, u.y});
+    const Cx<float> b = cms(Cx<float>{x.z, x.w}, l, Cx<float>{u.z, u.w});
+    return make_float4(a.re, a.im, b.re, b.im);
+}
+__device__ __forceinline__ double2 v16_cms(double2 x, Cx<double> l, double2 u) {
+    const Cx<double> a = cms(Cx<double>{x.x, x.y}, l, Cx<double>{u.x, u.y});
+    return make_double2(a.re, a.im);
+}
+
+// row[c] -= l prow[c] for c in [c0, w); row and prow 16-byte aligned, w even
+// for c64 entries
+template <typename T> __device__ __forceinline__ void row_update(Cx<T> *row, const Cx<T> *prow, Cx<T> l, int c0, int w) {
+    constexpr int E = 16 / sizeof(Cx<T>);
+    int c = c0;
+    if (E == 2 && (c & 1) && c < w) {
+        row[c] = cms(row[c], l, prow[c]);
+        ++c;
+    }
+    for (; c < w; c += 4 * E) {
+        decltype(v16_ld(row)) x[4], u[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+            if (c + t * E < w) {
+                x[t] = v16_ld(row + c + t * E);
+                u[t] = v16_ld(prow + c + t * E);
+            }
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+            if (c + t * E < w) v16_st(row + c + t * E, v16_cms(x[t], l, u[t]));
+    }
 }
 
 template <typename T> struct ClusterPanelArgs {
@@ -434,150 +666,274 @@ template <typename T> struct ClusterPanelArgs {
     int rpc;      // rows per CTA
     int *ipiv;
     int *status;
+    Cx<T> *dinv;  // inverse of the unit lower w x w diagonal block (nullptr: not wanted)
+    uint64_t timeout_ns;
 };
-
-// combine two pivot candidates: larger |re|+|im|, then the smaller row
-template <typename T> __device__ __forceinline__ void better(T &v, int &i, T ov, int oi) {
-    if (oi >= 0 && (ov > v || (ov == v && (i < 0 || oi < i)))) {
-        v = ov;
-        i = oi;
-    }
-}
 
 template <typename T>
 __global__ void __launch_bounds__(CP_THREADS) cluster_panel_kernel(ClusterPanelArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int w = a.w, wp = a.w + 1, tid = threadIdx.x;  // row stride padded by one entry
-    Cx<T> *P = reinterpret_cast<Cx<T> *>(smem_raw);       // rpc x wp
-    Cx<T> *pub = P + (size_t)a.rpc * wp;                   // [2][w] candidate rows
-    Cx<T> *pdg = pub + 2 * w;                              // [2][w] diagonal rows
-    Cx<T> *prow = pdg + 2 * w;                             // w
-    Cx<T> *drow = prow + w;                                // w
-    __shared__ double cand_v[2][CP_CTAS];
-    __shared__ int cand_i[2][CP_CTAS];
-    __shared__ T red_v[CP_THREADS / 32];
-    __shared__ int red_i[CP_THREADS / 32];
-    __shared__ int s_mine;
-    __shared__ T s_val;
+    constexpr int RS = CP_ROW_BYTES / sizeof(Cx<T>);  // padded row stride (entries)
+    const int w = a.w, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    Cx<T> *P = reinterpret_cast<Cx<T> *>(smem_raw);                                    // rpc x RS
+    Cx<T> *slot_row = P + (size_t)a.rpc * RS;                                           // [CP_SLOTS][CP_CTAS][w]
+    Cx<T> *wbuf = slot_row + CP_SLOTS * CP_CTAS * w;                                    // [2][CP_WARPS][w]
+    Cx<T> *ublk = wbuf + 2 * CP_WARPS * w;                                              // w x (w + 1): L11^-1 (CTA 0)
+    PivKey *slot_key = reinterpret_cast<PivKey *>(ublk + w * (w + 1));                 // [CP_SLOTS][CP_CTAS]
+    __shared__ uint64_t mbar[CP_SLOTS];
+    __shared__ uint64_t ldbar;  // the sub-panel's rows landed in shared memory
+    __shared__ uint64_t red_m[2][CP_WARPS];
+    __shared__ int red_pos[2][CP_WARPS];
+    __shared__ int s_abort[2];
     const uint32_t rank = cl_rank();
     const int gr0 = a.k + (int)rank * a.rpc;
     const int nrows = max(0, min(a.rpc, a.n - gr0));
-    batched_copy<CP_THREADS, 8, Cx<T>>(
-        nrows * w, [&](int i) { return a.A[(int64_t)(gr0 + i / w) * a.ld + a.k + i % w]; },
-        [&](int i, Cx<T> v) { P[(i / w) * wp + i % w] = v; });
-    __syncthreads();
-    // block-wide candidate of column `col` over rows >= row_min: thread-local
-    // (bv, bi) in, s_mine / s_val out
-    auto reduce_candidate = [&](T bv, int bi) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const T ov = __shfl_xor_sync(0xffffffffu, bv, o);
-            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-            better(bv, bi, ov, oi);
-        }
-        if ((tid & 31) == 0) {
-            red_v[tid >> 5] = bv;
-            red_i[tid >> 5] = bi;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            for (int q = 1; q < CP_THREADS / 32; ++q) better(bv, bi, red_v[q], red_i[q]);
-            s_mine = bi;
-            s_val = bv;
-        }
-        __syncthreads();
-    };
-    {
-        T bv = T(-1);
-        int bi = -1;
-        for (int i = tid; i < nrows; i += CP_THREADS) better(bv, bi, cabs1(P[i * wp]), gr0 + i);
-        reduce_candidate(bv, bi);
+    const int jmax = min(w, a.n - a.k);
+    const int nd = w * (int)sizeof(Cx<T>) / 16;  // data lanes of a push
+    const unsigned step_bytes = CP_CTAS * (unsigned)(w * sizeof(Cx<T>) + sizeof(PivKey));
+    const uint32_t row_bytes = (uint32_t)(w * sizeof(Cx<T>));
+    if (tid == 0) {
+        mb_init(&ldbar, 1);
+        for (int b = 0; b < CP_SLOTS; ++b) mb_init(&mbar[b], 1);
+        mb_init_fence();
+        mb_arrive_expect(&ldbar, (unsigned)nrows * row_bytes);
+        for (int b = 0; b < CP_SLOTS; ++b) mb_arrive_expect(&mbar[b], step_bytes);  // columns 0, 1, 2
+        s_abort[0] = s_abort[1] = 0;
     }
-    cl_sync();  // every CTA of the cluster is running before any remote access
-    for (int j = 0; j < w && a.k + j < a.n; ++j) {
-        const int jr = a.k + j, par = j & 1;
-        const int mine = s_mine;
-        if (tid < CP_CTAS) {
-            // this CTA's candidate into slot [par][rank] of CTA `tid`
-            cl_st(cl_map(&cand_v[par][rank], tid), (double)s_val);
-            cl_st(cl_map(&cand_i[par][rank], tid), mine);
-        }
-        for (int c = tid; c < w; c += CP_THREADS) {
-            if (mine >= 0) pub[par * w + c] = P[(mine - gr0) * wp + c];
-            if (jr >= gr0 && jr < gr0 + nrows) pdg[par * w + c] = P[(jr - gr0) * wp + c];
-        }
-        cl_sync();
-        // every thread picks the winner from its CTA's copy of the candidates
-        double wv = -1.0;
-        int p = -1, wc = -1;
+    __syncthreads();
+    for (int i = tid; i < nrows; i += CP_THREADS)  // rows in flight all at once
+        bulk_g2s(sm_addr(P + (size_t)i * RS), a.A + (int64_t)(gr0 + i) * a.ld + a.k, row_bytes, sm_addr(&ldbar));
+    if (!mb_try(&ldbar, 0u)) {
+        const uint64_t t0 = global_ns();
+        while (!mb_try(&ldbar, 0u))
+            if (global_ns() - t0 > a.timeout_ns) {
+                atomicOr(a.status, (int)DEV_BARRIER_TIMEOUT);
+                break;
+            }
+    }
+    int mp[CP_RMAX];  // logical position of local rows tid + r * CP_THREADS (-1: none)
 #pragma unroll
-        for (int q = 0; q < CP_CTAS; ++q) {
-            const int i = cand_i[par][q];
-            const double v = cand_v[par][q];
-            if (i >= 0 && (v > wv || (v == wv && (p < 0 || i < p)))) {
-                wv = v;
-                p = i;
-                wc = q;
+    for (int r = 0; r < CP_RMAX; ++r) {
+        const int i = tid + r * CP_THREADS;
+        mp[r] = i < nrows ? gr0 + i : -1;
+    }
+
+    // the warp's best row (given each thread's best) into the staging buffer
+    // `pb`, finished through step jprev (multiplier in column jprev, written by
+    // its owner lane), and the warp's result into red_*[pb]
+    auto warp_stage = [&](uint64_t m, int pos, int li, int pb, int jprev, const Cx<T> *prow_prev) -> int {
+        const int wl = warp_argbest<T>(m, pos);
+        const int wpos = __shfl_sync(0xffffffffu, pos, wl);
+        const int wli = __shfl_sync(0xffffffffu, li, wl);
+        const uint64_t wm = __shfl_sync(0xffffffffu, m, wl);
+        __syncwarp();
+        if (wpos != CP_NONE) {
+            Cx<T> *row = P + (size_t)wli * RS;
+            Cx<T> *dst = wbuf + (size_t)(pb * CP_WARPS + warp) * w;
+            for (int c = lane; c < w; c += 32) {
+                Cx<T> x = row[c];
+                if (jprev >= 0 && c >= jprev + 2) {
+                    x = cms(x, row[jprev], prow_prev[c]);
+                    row[c] = x;
+                }
+                dst[c] = x;
             }
         }
-        if (p < 0) p = jr;
+        if (lane == 0) {
+            red_m[pb][warp] = wm;
+            red_pos[pb][warp] = wpos;
+        }
+        return wpos != CP_NONE ? wli : -1;
+    };
+    // after the CTA barrier: the CTA's best among the warps' rows; warp q
+    // pushes it (slot of column s) to CTA q
+    auto push = [&](int s, int pb) {
+        const uint64_t m = lane < CP_WARPS ? red_m[pb][lane] : 0ull;
+        const int pos = lane < CP_WARPS ? red_pos[pb][lane] : CP_NONE;
+        const int bw = warp_argbest<T>(m, pos);
+        const uint64_t cm = __shfl_sync(0xffffffffu, m, bw);
+        const int cpos = __shfl_sync(0xffffffffu, pos, bw);
+        const int ps = s % CP_SLOTS;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        uint32_t dst = 0;
+        if (lane < nd) {
+            if (cpos != CP_NONE) v = reinterpret_cast<const uint4 *>(wbuf + (size_t)(pb * CP_WARPS + bw) * w)[lane];
+            dst = sm_addr(slot_row + (size_t)(ps * CP_CTAS + rank) * w) + 16u * lane;
+        } else if (lane == nd) {
+            v = make_uint4((uint32_t)cm, (uint32_t)(cm >> 32), (uint32_t)cpos, 0u);
+            dst = sm_addr(&slot_key[ps * CP_CTAS + rank]);
+        }
+        if (lane <= nd) st_async16(cl_map(dst, warp), v, cl_map(sm_addr(&mbar[ps]), warp));
+    };
+
+    // candidate of column 0
+    {
+        uint64_t m = 0;
+        int pos = CP_NONE, li = -1;
+#pragma unroll
+        for (int r = 0; r < CP_RMAX; ++r) {
+            const int i = tid + r * CP_THREADS;
+            if (mp[r] >= 0) {
+                const uint64_t mr = mag_bits(cabs1(P[i * RS]));
+                if (pos == CP_NONE || mr > m || (mr == m && mp[r] < pos)) {
+                    m = mr;
+                    pos = mp[r];
+                    li = i;
+                }
+            }
+        }
+        warp_stage(m, pos, li, 1, -1, nullptr);
+        __syncthreads();
+        cl_sync();  // every CTA's mbarriers are initialised before any remote store
+        if (jmax > 0) push(0, 1);
+    }
+
+    for (int j = 0; j < jmax; ++j) {
+        const int jr = a.k + j, par = j % CP_SLOTS, pb = j & 1;
+        if (!mb_try(&mbar[par], (unsigned)(j / CP_SLOTS) & 1u)) {
+            const uint64_t t0 = global_ns();
+            while (!mb_try(&mbar[par], (unsigned)(j / CP_SLOTS) & 1u)) {
+                if (global_ns() - t0 > a.timeout_ns) {
+                    s_abort[pb] = 1;
+                    atomicOr(a.status, (int)DEV_BARRIER_TIMEOUT);
+                    break;
+                }
+            }
+        }
+        if (tid == 0 && !s_abort[pb]) mb_arrive_expect(&mbar[par], step_bytes);  // next phase: column j + 3
+        // the same winner in every warp
+        int p, wc;
+        T wv;
+        {
+            const PivKey kq = slot_key[par * CP_CTAS + (lane & (CP_CTAS - 1))];
+            const uint64_t m = lane < CP_CTAS ? ((uint64_t)kq.w[1] << 32 | kq.w[0]) : 0ull;
+            const int pos = lane < CP_CTAS ? (int)kq.w[2] : CP_NONE;
+            wc = warp_argbest<T>(m, pos) & (CP_CTAS - 1);
+            p = __shfl_sync(0xffffffffu, pos, wc);
+            wv = mag_value<T>(__shfl_sync(0xffffffffu, m, wc));
+        }
+        if (p < jr || p >= a.n) {  // no candidate (or a damaged slot): keep the row in place
+            p = jr;
+            wv = T(0);
+        }
+        const Cx<T> *prow = slot_row + (size_t)(par * CP_CTAS + wc) * w;
         if (tid == 0) {
-            if (!(wv > 0.0)) atomicOr(a.status, (int)DEV_ZERO_PIVOT);
+            if (!(wv > T(0))) atomicOr(a.status, (int)DEV_ZERO_PIVOT);
             if (rank == 0) a.ipiv[jr] = p;
         }
-        const int jr_owner = (jr - a.k) / a.rpc;
-        const bool own_p = p != jr && p >= gr0 && p < gr0 + nrows;
-        for (int c = tid; c < w; c += CP_THREADS) {
-            prow[c] = wc >= 0 ? cl_ld(cl_map(&pub[par * w + c], wc), pub) : Cx<T>{T(0), T(0)};
-            if (own_p) drow[c] = cl_ld(cl_map(&pdg[par * w + c], jr_owner), pdg);
-        }
-        __syncthreads();
-        // rows: jr takes the pivot row (it is U); p (if here and distinct)
-        // takes the old row jr and is eliminated like the others
         const Cx<T> pv = prow[j];
         const T den = pv.re * pv.re + pv.im * pv.im;
-        const Cx<T> inv = den > T(0) ? Cx<T>{pv.re / den, -pv.im / den} : Cx<T>{T(0), T(0)};
-        T bv = T(-1);
-        int bi = -1;
-        for (int i = tid; i < nrows; i += CP_THREADS) {
-            const int gi = gr0 + i;
-            Cx<T> *row = P + (size_t)i * wp;
-            if (gi == jr) {
-                if (p != jr)
-                    for (int c = 0; c < w; ++c) row[c] = prow[c];  // L entries of row p move with it
-                continue;
-            }
-            if (gi < jr) continue;
-            const Cx<T> *src = gi == p ? drow : row;
-            const Cx<T> l = cmul(src[j], inv);
-            if (gi == p)
-                for (int c = 0; c < j; ++c) row[c] = drow[c];
-            row[j] = l;
-            for (int c = j + 1; c < w; ++c) {
-                const Cx<T> u = prow[c], x = src[c];
-                row[c] = Cx<T>{x.re - (l.re * u.re - l.im * u.im), x.im - (l.re * u.im + l.im * u.re)};
-            }
-            if (j + 1 < w) better(bv, bi, cabs1(row[j + 1]), gi);
+        const T rd = den > T(0) ? T(1) / den : T(0);
+        const Cx<T> inv{pv.re * rd, -pv.im * rd};
+        // interchange of positions jr and p; the pivot row retires at jr
+#pragma unroll
+        for (int r = 0; r < CP_RMAX; ++r) {
+            if (mp[r] == p)
+                mp[r] = jr;
+            else if (mp[r] == jr)
+                mp[r] = p;
         }
-        reduce_candidate(bv, bi);
+        // look-ahead: multipliers and column j + 1, with each thread's best row
+        const bool more = j + 1 < jmax;
+        uint64_t m = 0;
+        int pos = CP_NONE, li = -1;
+        {
+            Cx<T> xj[CP_RMAX], xn[CP_RMAX];
+#pragma unroll
+            for (int r = 0; r < CP_RMAX; ++r)
+                if (mp[r] > jr) {
+                    const Cx<T> *row = P + (size_t)(tid + r * CP_THREADS) * RS;
+                    xj[r] = row[j];
+                    if (more) xn[r] = row[j + 1];
+                }
+            const Cx<T> u = more ? prow[j + 1] : Cx<T>{T(0), T(0)};
+#pragma unroll
+            for (int r = 0; r < CP_RMAX; ++r)
+                if (mp[r] > jr) {
+                    const int i = tid + r * CP_THREADS;
+                    Cx<T> *row = P + (size_t)i * RS;
+                    const Cx<T> l = cmul(xj[r], inv);
+                    row[j] = l;
+                    if (more) {
+                        const Cx<T> y = cms(xn[r], l, u);
+                        row[j + 1] = y;
+                        const uint64_t mr = mag_bits(cabs1(y));
+                        if (pos == CP_NONE || mr > m || (mr == m && mp[r] < pos)) {
+                            m = mr;
+                            pos = mp[r];
+                            li = i;
+                        }
+                    }
+                }
+        }
+        int staged = -1;  // local row finished by this warp for the push
+        if (more) staged = warp_stage(m, pos, li, pb, j, prow);
+        __syncthreads();
+        if (s_abort[pb]) break;  // read after the barrier: uniform
+        if (more) push(j + 1, pb);
+        // rest of step j
+        const int c0 = more ? j + 2 : j + 1;
+#pragma unroll
+        for (int r = 0; r < CP_RMAX; ++r) {
+            const int i = tid + r * CP_THREADS;
+            if (mp[r] > jr && i != staged) {
+                Cx<T> *row = P + (size_t)i * RS;
+                row_update(row, prow, row[j], c0, w);
+            }
+        }
+        if (rank == 0 && warp == CP_WARPS - 1 && a.dinv && lane < w) {
+            // row j of the inverse of the unit lower diagonal block, whose row
+            // j is prow[0:j]:  Y[j][c] = delta_jc - sum_{t<j} prow[t] Y[t][c]
+            Cx<T> s0{T(lane == j), T(0)}, s1{T(0), T(0)}, s2{T(0), T(0)}, s3{T(0), T(0)};
+            int t = 0;
+            for (; t + 4 <= j; t += 4) {
+                s0 = cms(s0, prow[t], ublk[t * (w + 1) + lane]);
+                s1 = cms(s1, prow[t + 1], ublk[(t + 1) * (w + 1) + lane]);
+                s2 = cms(s2, prow[t + 2], ublk[(t + 2) * (w + 1) + lane]);
+                s3 = cms(s3, prow[t + 3], ublk[(t + 3) * (w + 1) + lane]);
+            }
+            for (; t < j; ++t) s0 = cms(s0, prow[t], ublk[t * (w + 1) + lane]);
+            ublk[j * (w + 1) + lane] = Cx<T>{(s0.re + s1.re) + (s2.re + s3.re), (s0.im + s1.im) + (s2.im + s3.im)};
+        }
     }
-    for (int i = tid; i < nrows * w; i += CP_THREADS) a.A[(int64_t)(gr0 + i / w) * a.ld + a.k + i % w] = P[(i / w) * wp + i % w];
-    cl_sync();  // no CTA leaves while others may still read its shared memory
+    // each row to its final position, by the bulk-copy engine
+    fence_proxy_async_smem();
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < CP_RMAX; ++r) {
+        const int i = tid + r * CP_THREADS;
+        if (i < nrows && mp[r] >= a.k && mp[r] < a.n)
+            bulk_s2g(a.A + (int64_t)mp[r] * a.ld + a.k, sm_addr(P + (size_t)i * RS), row_bytes);
+    }
+    bulk_commit_wait_all();
+    if (rank == 0 && warp == 0 && a.dinv && lane < w)  // the inverse, identity past jmax
+        for (int i = 0; i < w; ++i)
+            a.dinv[(size_t)i * w + lane] = i < jmax ? ublk[i * (w + 1) + lane] : Cx<T>{T(i == lane), T(0)};
+    cl_sync();  // no CTA leaves while a peer may still store into its shared memory
+}
+
+// shared memory of the cluster kernel for rpc rows of width w
+template <typename T> static size_t cluster_panel_smem(int rpc, int w) {
+    return (size_t)rpc * CP_ROW_BYTES + sizeof(Cx<T>) * ((CP_SLOTS * CP_CTAS + 2 * CP_WARPS) * (size_t)w + w * (w + 1)) +
+           sizeof(PivKey) * CP_SLOTS * CP_CTAS;
 }
 
 // Launches the cluster kernel for a sub-panel; false when the rows do not fit
 // the cluster's shared memory or no cluster of CP_CTAS can be scheduled.
 template <typename T>
-static bool cluster_panel(beat_b200_ctx *c, Cx<T> *A, int64_t ld, int n, int k, int w, int *ipiv) {
+static bool cluster_panel(beat_b200_ctx *c, Cx<T> *A, int64_t ld, int n, int k, int w, int *ipiv, Cx<T> *dinv) {
     const int m = n - k;
     const int rpc = (m + CP_CTAS - 1) / CP_CTAS;
-    const size_t smem = sizeof(Cx<T>) * ((size_t)rpc * (w + 1) + 6 * (size_t)w);
-    if (smem > 200 * 1024) return false;
+    constexpr size_t cap = 220 * 1024;
+    if (w * sizeof(Cx<T>) > 256 || (w * sizeof(Cx<T>)) % 16 != 0 || rpc > CP_RMAX * CP_THREADS || n >= (1 << 30))
+        return false;
+    const size_t smem = cluster_panel_smem<T>(rpc, w);
+    if (smem > cap) return false;
     static bool attr_done[2] = {false, false};
     const int ti = sizeof(T) == 8;
     if (!attr_done[ti]) {
         BB_CUDA(cudaFuncSetAttribute(cluster_panel_kernel<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-        BB_CUDA(cudaFuncSetAttribute(cluster_panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        BB_CUDA(cudaFuncSetAttribute(cluster_panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap));
         attr_done[ti] = true;
     }
     ClusterPanelArgs<T> a;
@@ -589,6 +945,8 @@ static bool cluster_panel(beat_b200_ctx *c, Cx<T> *A, int64_t ld, int n, int k, 
     a.rpc = rpc;
     a.ipiv = ipiv;
     a.status = c->status.as<int>();
+    a.dinv = dinv;
+    a.timeout_ns = 100000000ull;  // 0.1 s per column wait
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(CP_CTAS);
     cfg.blockDim = dim3(CP_THREADS);
@@ -603,7 +961,9 @@ static bool cluster_panel(beat_b200_ctx *c, Cx<T> *A, int64_t ld, int n, int k, 
     cfg.numAttrs = 1;
     if (!c->cluster_checked) {
         int nclusters = 0;
+        cfg.dynamicSmemBytes = cap;  // the largest request any sub-panel makes
         cudaError_t e = cudaOccupancyMaxActiveClusters(&nclusters, (void *)cluster_panel_kernel<T>, &cfg);
+        cfg.dynamicSmemBytes = smem;
         c->cluster_ok = (e == cudaSuccess && nclusters >= 1);
         cudaGetLastError();
         c->cluster_checked = true;
@@ -633,26 +993,38 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
     BB_REQUIRE(smem <= smem_cap, BEAT_B200_INVALID_ARG,
                "LU: system of order " + std::to_string(n) + " exceeds the shared-memory panel limit");
     // scratch: [2][G] pivot records, [2][G][nb] candidate rows, [2][nb] diagonal rows
+    // and the inverses of the sub-panels' W x W diagonal blocks
+    const int W = std::min(nb, (int)(256 / sizeof(Cx<T>)));
     const size_t rec_bytes = sizeof(PivotRec) * 2 * (size_t)G;
     const size_t scratch = rec_bytes + sizeof(Cx<T>) * (2 * (size_t)G * nb + 2 * nb);
-    w.panel_scratch.alloc(scratch + 256);
+    const size_t dinv_off = (scratch + 255) / 256 * 256;
+    const size_t dinv_bytes = sizeof(Cx<T>) * (size_t)W * W * ((n + W - 1) / W);
+    w.panel_scratch.alloc(dinv_off + dinv_bytes);
     PivotRec *recs = w.panel_scratch.as<PivotRec>();
     Cx<T> *pub_rows = reinterpret_cast<Cx<T> *>(recs + 2 * G);
     Cx<T> *pub_diag = pub_rows + 2 * (size_t)G * nb;
+    Cx<T> *dinv = reinterpret_cast<Cx<T> *>(w.panel_scratch.as<unsigned char>() + dinv_off);
+    // blocked U12 solves need whole W-column sub-panels of 256-byte rows
+    constexpr int WF = 256 / sizeof(Cx<T>);
+    const bool blocked = W == WF && nb % W == 0;
+    const size_t tb_smem = sizeof(Cx<T>) * ((size_t)nb * TB_COLS + (size_t)W * (W + 1) + (size_t)W * (nb - W + 1));
+    if (blocked)
+        BB_CUDA(cudaFuncSetAttribute(trsm_blocked_kernel<T, WF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)tb_smem));
     c->barrier.alloc(sizeof(unsigned) * 4096);
     BB_CUDA(cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
     const size_t trsm_smem = sizeof(Cx<T>) * ((size_t)nb * nb + (size_t)nb * TRSM_COLS);
     BB_CUDA(cudaFuncSetAttribute(trsm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
     iota_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(w.perm.as<int>(), n);
     BB_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream));
-    // sub-panel width: 256-byte rows in the cluster kernel
-    const int W = std::min(nb, (int)(256 / sizeof(Cx<T>)));
     const size_t trsm_w_smem = sizeof(Cx<T>) * ((size_t)W * W + (size_t)W * TRSM_COLS);
     for (int k = 0; k < n; k += nb) {
         const int pe = std::min(k + nb, n);  // end of this panel
         for (int ks = k; ks < pe; ks += W) {
             const int m = n - ks;
-            if (!cluster_panel<T>(c, A, ld, n, ks, W, w.ipiv.as<int>())) {
+            Cx<T> *dinv_s = blocked ? dinv + (size_t)(ks / W) * W * W : nullptr;
+            const bool on_cluster = cluster_panel<T>(c, A, ld, n, ks, W, w.ipiv.as<int>(), dinv_s);
+            if (!on_cluster) {
                 // grid-wide panel kernel on the sub-panel
                 int g = std::min(G, std::max(1, (m + 15) / 16));
                 int rows = (m + g - 1) / g;
@@ -679,11 +1051,19 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
             laswp_kernel<T><<<(n + 1 + 255) / 256, 256, 0, c->stream>>>(A, ld, n, ks, W, w.ipiv.as<int>(),
                                                                         w.perm.as<int>());
             BB_CUDA(cudaGetLastError());
+            if (blocked && !on_cluster) {
+                diag_block_inverse_kernel<T><<<1, 32, 0, c->stream>>>(A, ld, n, ks, W, dinv_s);
+                BB_CUDA(cudaGetLastError());
+            }
             if (ks + W < pe) {
                 // rest of this panel: U row block, then the panel's own trailing update
                 const int cols = pe - ks - W;
-                trsm_kernel<T><<<(cols + TRSM_COLS - 1) / TRSM_COLS, 256, trsm_w_smem, c->stream>>>(
-                    A, ld, n, ks, W, ks + W, pe);
+                if (blocked)
+                    trsm_blocked_kernel<T, WF><<<(cols + TB_COLS - 1) / TB_COLS, 256, tb_smem, c->stream>>>(
+                        A, ld, ks, 1, dinv + (size_t)(ks / W) * W * W, ks + W, pe);
+                else
+                    trsm_kernel<T><<<(cols + TRSM_COLS - 1) / TRSM_COLS, 256, trsm_w_smem, c->stream>>>(
+                        A, ld, n, ks, W, ks + W, pe);
                 dim3 grid((cols + GT - 1) / GT, (n - ks - W + GT - 1) / GT);
                 gemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(A, ld, n, ks, W, ks + W, ks + W, pe);
                 BB_CUDA(cudaGetLastError());
@@ -691,8 +1071,12 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
         }
         const int rest = n - k - nb;
         if (rest > 0) {
-            trsm_kernel<T><<<(rest + TRSM_COLS - 1) / TRSM_COLS, 256, trsm_smem, c->stream>>>(A, ld, n, k, nb, k + nb,
-                                                                                           n);
+            if (blocked)
+                trsm_blocked_kernel<T, WF><<<(rest + TB_COLS - 1) / TB_COLS, 256, tb_smem, c->stream>>>(
+                    A, ld, k, nb / W, dinv + (size_t)(k / W) * W * W, k + nb, n);
+            else
+                trsm_kernel<T><<<(rest + TRSM_COLS - 1) / TRSM_COLS, 256, trsm_smem, c->stream>>>(A, ld, n, k, nb,
+                                                                                               k + nb, n);
             BB_CUDA(cudaGetLastError());
             if (!(sizeof(T) == 4 && tc_trailing_update(c, k, nb, split_terms))) {
                 dim3 grid((rest + GT - 1) / GT, (rest + GT - 1) / GT);
