@@ -360,26 +360,38 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "fallback"}
 
 
+# DRAM traffic of regular_pairs_kernel<float, 6> measured by ncu on the F = 5,120 icosphere
+# (profiles/regular_pairs_kernel_F5120.md): dram read + write bytes per launch and the
+# algorithmic output of that launch (A: N^2 c64, B: N x F c64).  Traffic grows with the output
+# written (the zeroed A and B are read back by the red.global.add flush), so a launch on another
+# mesh is scaled by its output bytes.
+REGULAR_TRAFFIC_F5120 = {"bytes": 158.676736e6 + 112.227840e6, "output_bytes": 2562 * 2562 * 8 + 2562 * 5120 * 8}
+
+
 def roofline(args, mesh, stages, peaks):
     """Roofline of the regular element-pair assembly kernel (the dominant
-    kernel of the mixed form).  achieved = algorithmic bytes per launch / its
-    CUDA-event duration; algorithmic bytes = the system it produces, N^2
-    complex entries plus N x R right-hand sides (c64 entries in the mixed
-    form, c128 in FP64).  The kernel is bound by FP32 FMA/SFU issue, not HBM:
-    the compute fraction is reported beside it."""
-    F, N, R = mesh.num_faces, mesh.num_vertices, args.rhs
+    kernel of the step).  achieved = algorithmic bytes per launch / its
+    CUDA-event duration; algorithmic bytes = the output it produces, A (N^2)
+    and the RHS operator B (N x F), c64 entries in the mixed form, c128 in
+    FP64.  The kernel is bound by FP32 FMA/SFU issue, not HBM: the compute
+    fraction is reported beside it."""
+    F, N = mesh.num_faces, mesh.num_vertices
     esz = 16 if args.precision == "fp64" else 8
     regular_pairs = F * F - (13 * F - 60)
     point_pairs = 36 * regular_pairs
-    alg_bytes = N * N * esz + N * R * 16
+    alg_bytes = N * N * esz + N * F * esz
     t = stages["regular_ms"] / 1e3
     achieved = alg_bytes / t / 1e9 if t > 0 else None
     peak = peaks["hbm_gbs"]
+    traffic = None
+    if esz == 8:
+        traffic = REGULAR_TRAFFIC_F5120["bytes"] * alg_bytes / REGULAR_TRAFFIC_F5120["output_bytes"]
     flops = point_pairs * 72.0
     fp_peak = 148 * 128 * 2 * 1.965e9 / (2 if args.precision == "fp64" else 1)
     return {"kernel": "regular_pairs_kernel (element-pair Galerkin assembly)", "bound": "hbm",
             "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": (achieved / peak) if achieved else None, "traffic": None,
+            "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+            "traffic_basis": "ncu dram read+write of the F=5,120 launch scaled by output bytes" if traffic else None,
             "peak_source": f"{peaks['source']} hbm_gbs (MEASURED_PEAKS.json)" if peaks["source"] == "measured"
             else "fallback 6.65 TB/s",
             "algorithmic_bytes_per_launch": alg_bytes,
