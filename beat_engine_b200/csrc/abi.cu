@@ -203,7 +203,7 @@ int32_t beat_b200_destroy(beat_b200_ctx *c) {
                       &c->d_faces, &c->d_normals, &c->d_areas, &c->d_curls, &c->d_qpts, &c->sp_test, &c->sp_trial,
                       &c->sp_rule, &c->sp_jac, &c->sp_nn, &c->rule_start, &c->rule_data, &c->status, &c->barrier})
         b->free_();
-    for (Tiling *t : {&c->test_tiles, &c->trial_tiles}) {
+    for (Tiling *t : {&c->test_tiles, &c->trial_tiles, &c->sym_tiles}) {
         t->face_start.free_();
         t->vert_start.free_();
         t->verts.free_();

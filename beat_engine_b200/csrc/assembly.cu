@@ -284,6 +284,250 @@ template <typename T, int Q> static size_t regular_smem_bytes() {
 }
 
 // ---------------------------------------------------------------------------
+// Symmetric element-pair kernel (FP32 form).  G(x, y) = G(y, x), so the two
+// ordered pairs (tau, sigma) and (sigma, tau) of two elements share r, the
+// phase, e^{ikr}/r and dG/dr at every point pair; only the normal
+// derivatives swap roles: with r = y - x,
+//   order 1 (test tau at x, trial sigma at y): dn_s =  r.n_sigma / r = a,
+//                                               dn_t = -r.n_tau / r   = c,
+//   order 2 (test sigma at y, trial tau at x): dn_s = c, dn_t = a.
+// One CTA integrates an unordered pair of square tiles (I <= J; pairs of
+// elements tau < sigma inside a diagonal tile) for both orders; each order
+// has its own shared-memory accumulators, flushed like the one-order kernel.
+// ---------------------------------------------------------------------------
+constexpr int SYM_F = 32, SYM_V = 40;  // square tile: faces, distinct vertices (context.cu)
+// accumulators as separate re / im planes with odd row strides: a warp's
+// lanes (one tau, 32 sigma) hit rows spread over all banks
+constexpr int SYM_AS = SYM_V + 1, SYM_BS = SYM_F + 1;
+constexpr int SYM_ACC = 2 * SYM_V * SYM_AS + 2 * SYM_V * SYM_BS;  // floats per plane
+
+template <int Q> static size_t sym_smem_bytes() {
+    return sizeof(float) * 2 * SYM_ACC + sizeof(float) * 2 * SYM_F * (Q * 3 + 3 + 9 + 2) +
+           sizeof(int) * 4 * 3 * SYM_F;
+}
+
+template <int Q>
+__global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float> g) {
+    using T = float;
+    constexpr int RI = Q == 1 ? 0 : Q == 3 ? 1 : 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *acc_re = reinterpret_cast<T *>(smem_raw), *acc_im = acc_re + SYM_ACC;
+    constexpr int A1 = 0;                      // [vI][vJ]: test vertex of tau, trial vertex of sigma
+    constexpr int A2 = A1 + SYM_V * SYM_AS;    // [vJ][vI]: test vertex of sigma, trial vertex of tau
+    constexpr int B1 = A2 + SYM_V * SYM_AS;    // [vI][sigma]
+    constexpr int B2 = B1 + SYM_V * SYM_BS;    // [vJ][tau]
+    T *xq = acc_im + SYM_ACC;                  // tile I: [tau][Q][3]
+    T *xn = xq + SYM_F * Q * 3;                // [tau][3]
+    T *xc = xn + SYM_F * 3;                    // [tau][9]
+    T *xa = xc + SYM_F * 9;                    // [tau]
+    T *xp = xa + SYM_F;                        // [tau]: plane offset x . n_tau
+    T *yq = xp + SYM_F;                        // tile J, transposed: [Q * 3][sigma]
+    T *yn = yq + SYM_F * Q * 3;                // [3][sigma]
+    T *yc = yn + 3 * SYM_F;                    // [9][sigma]
+    T *ya = yc + 9 * SYM_F;                    // [sigma]
+    T *yp = ya + SYM_F;                        // [sigma]: plane offset y . n_sigma
+    int *xgv = reinterpret_cast<int *>(yp + SYM_F);  // [tau][3] global vertex ids
+    int *xlv = xgv + 3 * SYM_F;                      // [tau][3] tile-local vertex ids
+    int *ygv = xlv + 3 * SYM_F;                      // [3][sigma]
+    int *ylv = ygv + 3 * SYM_F;                      // [3][sigma]
+
+    // unordered tile pair (I, J), I <= J, from the linear block index
+    const int64_t bi = blockIdx.x;
+    int J = (int)((sqrt(8.0 * (double)bi + 1.0) - 1.0) * 0.5);
+    while ((int64_t)J * (J + 1) / 2 > bi) --J;
+    while ((int64_t)(J + 1) * (J + 2) / 2 <= bi) ++J;
+    const int I = (int)(bi - (int64_t)J * (J + 1) / 2);
+    const bool diag = I == J;
+
+    const int tid = threadIdx.x;
+    const int t0 = g.t_fstart[I], nI = g.t_fstart[I + 1] - t0;
+    const int s0 = g.t_fstart[J], nJ = g.t_fstart[J + 1] - s0;
+    const int tv0 = g.t_vstart[I], nvI = g.t_vstart[I + 1] - tv0;
+    const int sv0 = g.t_vstart[J], nvJ = g.t_vstart[J + 1] - sv0;
+
+    for (int i = tid; i < 2 * SYM_ACC; i += REG_THREADS) acc_re[i] = T(0);
+    for (int i = tid; i < nI * Q * 3; i += REG_THREADS) xq[i] = g.qpts[(size_t)t0 * Q * 3 + i];
+    for (int i = tid; i < nI * 3; i += REG_THREADS) {
+        xn[i] = g.normal[(size_t)t0 * 3 + i];
+        xgv[i] = g.gvert[(size_t)t0 * 3 + i];
+        xlv[i] = g.t_local[(size_t)t0 * 3 + i];
+    }
+    for (int i = tid; i < nI * 9; i += REG_THREADS) xc[i] = g.curl[(size_t)t0 * 9 + i];
+    for (int i = tid; i < nI; i += REG_THREADS) xa[i] = g.area[t0 + i];
+    for (int i = tid; i < nJ * Q * 3; i += REG_THREADS) {
+        const int s = i / (Q * 3), j = i % (Q * 3);
+        yq[j * SYM_F + s] = g.qpts[(size_t)s0 * Q * 3 + i];
+    }
+    for (int i = tid; i < nJ * 3; i += REG_THREADS) {
+        const int s = i / 3, j = i % 3;
+        yn[j * SYM_F + s] = g.normal[(size_t)s0 * 3 + i];
+        ygv[j * SYM_F + s] = g.gvert[(size_t)s0 * 3 + i];
+        ylv[j * SYM_F + s] = g.t_local[(size_t)s0 * 3 + i];
+    }
+    for (int i = tid; i < nJ * 9; i += REG_THREADS) {
+        const int s = i / 9, j = i % 9;
+        yc[j * SYM_F + s] = g.curl[(size_t)s0 * 9 + i];
+    }
+    for (int i = tid; i < nJ; i += REG_THREADS) ya[i] = g.area[s0 + i];
+    __syncthreads();
+    for (int i = tid; i < nI; i += REG_THREADS)
+        xp[i] = xq[i * Q * 3] * xn[3 * i] + xq[i * Q * 3 + 1] * xn[3 * i + 1] + xq[i * Q * 3 + 2] * xn[3 * i + 2];
+    for (int i = tid; i < nJ; i += REG_THREADS)
+        yp[i] = yq[i] * yn[i] + yq[SYM_F + i] * yn[SYM_F + i] + yq[2 * SYM_F + i] * yn[2 * SYM_F + i];
+    __syncthreads();
+
+    const T k = g.k, eta = g.eta;
+    const T inv4pi = T(0.07957747154594767);  // 1 / (4 pi)
+    for (int p = tid; p < SYM_F * SYM_F; p += REG_THREADS) {
+        const int ti = p / SYM_F, sj = p % SYM_F;  // a warp: one tau, every sigma
+        if (ti >= nI || sj >= nJ || (diag && sj <= ti)) continue;
+        const int ga = xgv[3 * ti], gb = xgv[3 * ti + 1], gc = xgv[3 * ti + 2];
+        const int ha = ygv[sj], hb = ygv[SYM_F + sj], hc = ygv[2 * SYM_F + sj];
+        if (ga == ha || ga == hb || ga == hc || gb == ha || gb == hb || gb == hc || gc == ha || gc == hb ||
+            gc == hc)
+            continue;  // touching pair: the Duffy kernel integrates both orders
+        const T ntx = xn[3 * ti], nty = xn[3 * ti + 1], ntz = xn[3 * ti + 2];
+        const T nsx = yn[sj], nsy = yn[SYM_F + sj], nsz = yn[2 * SYM_F + sj];
+        const T k2n = eta * g.k2 * (ntx * nsx + nty * nsy + ntz * nsz);
+        const T dtau = xp[ti], dsig = yp[sj];
+        T L1[9][2], L2[9][2], R1[3][2], U2[Q][2], cr = T(0), ci = T(0);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) L1[i][0] = L1[i][1] = L2[i][0] = L2[i][1] = T(0);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) R1[i][0] = R1[i][1] = T(0);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) U2[i][0] = U2[i][1] = T(0);
+#pragma unroll 1
+        for (int qt = 0; qt < Q; ++qt) {
+            const T x0 = xq[(ti * Q + qt) * 3], x1 = xq[(ti * Q + qt) * 3 + 1], x2 = xq[(ti * Q + qt) * 3 + 2];
+            const T wt = RuleRef<T>::w(RI, qt) * inv4pi;
+            const T xns = dsig - (x0 * nsx + x1 * nsy + x2 * nsz);  // r . n_sigma for every y on sigma
+            T S0r = 0, S0i = 0, S1r = 0, S1i = 0, S2r = 0, S2i = 0;  // order 1: sum over trial points
+            T P0r = 0, P0i = 0, P1r = 0, P1i = 0, P2r = 0, P2i = 0;  // order 2: sum over test points
+            T Gr = 0, Gi = 0, Wr = 0, Wi = 0;
+#pragma unroll
+            for (int qs = 0; qs < Q; ++qs) {
+                const T y0 = yq[(qs * 3) * SYM_F + sj], y1 = yq[(qs * 3 + 1) * SYM_F + sj],
+                        y2 = yq[(qs * 3 + 2) * SYM_F + sj];
+                const T rx = y0 - x0, ry = y1 - x1, rz = y2 - x2;
+                const T r2 = rx * rx + ry * ry + rz * rz;
+                const T ir = rsqrt_t(r2);
+                T sn_, cs_;
+                sincos_t(k * (r2 * ir), &sn_, &cs_);
+                const T scl = ir * (wt * RuleRef<T>::w(RI, qs));
+                const T gr = cs_ * scl, gi = sn_ * scl;
+                const T gsr = -gr * ir - gi * k;
+                const T gsi = gr * k - gi * ir;
+                const T a = xns * ir;                                         // r . n_sigma / r
+                const T c = (dtau - (y0 * ntx + y1 * nty + y2 * ntz)) * ir;  // -r . n_tau / r
+                const T b0 = RuleRef<T>::b(RI, qs, 0), b1v = RuleRef<T>::b(RI, qs, 1),
+                        b2v = RuleRef<T>::b(RI, qs, 2);
+                // order 1
+                const T lr1 = k2n * gi - gsr * a, li1 = -(gsi * a + k2n * gr);
+                Gr += gr;
+                Gi += gi;
+                Wr += c * gsr;
+                Wi += c * gsi;
+                S0r += b0 * lr1;
+                S0i += b0 * li1;
+                S1r += b1v * lr1;
+                S1i += b1v * li1;
+                S2r += b2v * lr1;
+                S2i += b2v * li1;
+                // order 2
+                const T lr2 = k2n * gi - gsr * c, li2 = -(gsi * c + k2n * gr);
+                P0r += b0 * lr2;
+                P0i += b0 * li2;
+                P1r += b1v * lr2;
+                P1i += b1v * li2;
+                P2r += b2v * lr2;
+                P2i += b2v * li2;
+                const T ea = eta * a;
+                U2[qs][0] += ea * gsi - gr;  // -g - i eta grad*dn_t with dn_t = a
+                U2[qs][1] -= ea * gsr + gi;
+            }
+            const T Ur = -Gr + eta * Wi, Ui = -Gi - eta * Wr;
+            cr += Gr;
+            ci += Gi;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const T ba = RuleRef<T>::b(RI, qt, a);
+                L1[3 * a + 0][0] += ba * S0r;
+                L1[3 * a + 0][1] += ba * S0i;
+                L1[3 * a + 1][0] += ba * S1r;
+                L1[3 * a + 1][1] += ba * S1i;
+                L1[3 * a + 2][0] += ba * S2r;
+                L1[3 * a + 2][1] += ba * S2i;
+                R1[a][0] += ba * Ur;
+                R1[a][1] += ba * Ui;
+                // order 2: row = test vertex of sigma (P index), column = trial vertex of tau (a)
+                L2[0 * 3 + a][0] += ba * P0r;
+                L2[0 * 3 + a][1] += ba * P0i;
+                L2[1 * 3 + a][0] += ba * P1r;
+                L2[1 * 3 + a][1] += ba * P1i;
+                L2[2 * 3 + a][0] += ba * P2r;
+                L2[2 * 3 + a][1] += ba * P2i;
+            }
+        }
+        // hypersingular curl term: eta * sum(g w) * curl_test . curl_trial (same sum for both orders)
+        const T ccr = -eta * ci, cci = eta * cr;
+        const T jac = T(4) * xa[ti] * ya[sj];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int ra = xlv[3 * ti + a];      // vertex a of tau, tile I local
+            const int sa = ylv[a * SYM_F + sj];  // vertex a of sigma, tile J local
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const T d = xc[9 * ti + 3 * a] * yc[(3 * b) * SYM_F + sj] +
+                            xc[9 * ti + 3 * a + 1] * yc[(3 * b + 1) * SYM_F + sj] +
+                            xc[9 * ti + 3 * a + 2] * yc[(3 * b + 2) * SYM_F + sj];  // curl_tau[a] . curl_sigma[b]
+                const int o1 = A1 + ra * SYM_AS + ylv[b * SYM_F + sj];
+                red_add(&acc_re[o1], (L1[3 * a + b][0] + d * ccr) * jac);
+                red_add(&acc_im[o1], (L1[3 * a + b][1] + d * cci) * jac);
+                // order 2 entry (sigma vertex b, tau vertex a) uses curl_sigma[b] . curl_tau[a] = d
+                const int o2 = A2 + ylv[b * SYM_F + sj] * SYM_AS + ra;
+                red_add(&acc_re[o2], (L2[3 * b + a][0] + d * ccr) * jac);
+                red_add(&acc_im[o2], (L2[3 * b + a][1] + d * cci) * jac);
+            }
+            const int e1 = B1 + ra * SYM_BS + sj;
+            red_add(&acc_re[e1], R1[a][0] * jac);
+            red_add(&acc_im[e1], R1[a][1] * jac);
+            T r2r = T(0), r2i = T(0);
+#pragma unroll
+            for (int qs = 0; qs < Q; ++qs) {
+                const T bq = RuleRef<T>::b(RI, qs, a);
+                r2r += bq * U2[qs][0];
+                r2i += bq * U2[qs][1];
+            }
+            const int e2 = B2 + sa * SYM_BS + ti;
+            red_add(&acc_re[e2], r2r * jac);
+            red_add(&acc_im[e2], r2i * jac);
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < nvI * nvJ; i += REG_THREADS) {
+        const int li = i / nvJ, lj = i % nvJ;
+        const Cx<T> v{acc_re[A1 + li * SYM_AS + lj], acc_im[A1 + li * SYM_AS + lj]};
+        const Cx<T> u{acc_re[A2 + lj * SYM_AS + li], acc_im[A2 + lj * SYM_AS + li]};
+        const int gi_ = g.t_verts[tv0 + li], gj_ = g.t_verts[sv0 + lj];
+        if (v.re != T(0) || v.im != T(0)) red_add_cx(&g.A[(int64_t)gi_ * g.ld + gj_], v.re, v.im);
+        if (u.re != T(0) || u.im != T(0)) red_add_cx(&g.A[(int64_t)gj_ * g.ld + gi_], u.re, u.im);
+    }
+    for (int i = tid; i < nvI * nJ; i += REG_THREADS) {
+        const int li = i / nJ, sj = i % nJ;
+        const Cx<T> v{acc_re[B1 + li * SYM_BS + sj], acc_im[B1 + li * SYM_BS + sj]};
+        if (v.re != T(0) || v.im != T(0))
+            red_add_cx(&g.B[(int64_t)g.t_verts[tv0 + li] * g.F + g.face_id[s0 + sj]], v.re, v.im);
+    }
+    for (int i = tid; i < nvJ * nI; i += REG_THREADS) {
+        const int lj = i / nI, ti = i % nI;
+        const Cx<T> v{acc_re[B2 + lj * SYM_BS + ti], acc_im[B2 + lj * SYM_BS + ti]};
+        if (v.re != T(0) || v.im != T(0))
+            red_add_cx(&g.B[(int64_t)g.t_verts[sv0 + lj] * g.F + g.face_id[t0 + ti]], v.re, v.im);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // touching pairs: one warp per pair, FP64, Duffy points over the lanes
 // ---------------------------------------------------------------------------
 template <typename T> struct SingArgs {
@@ -455,6 +699,36 @@ template <typename T, int Q> static void launch_regular(beat_b200_ctx *c, double
     BB_CUDA(cudaGetLastError());
 }
 
+// FP32 form: the symmetric kernel over unordered pairs of square tiles
+template <int Q> static void launch_sym(beat_b200_ctx *c, double k, double eta) {
+    RegArgs<float> g;
+    g.qpts = c->pos_qpts32.as<float>();
+    g.normal = c->pos_normal32.as<float>();
+    g.curl = c->pos_curl32.as<float>();
+    g.area = c->pos_area32.as<float>();
+    g.gvert = c->pos_gvert.as<int>();
+    g.face_id = c->pos_face.as<int>();
+    g.t_fstart = c->sym_tiles.face_start.as<int>();
+    g.t_vstart = c->sym_tiles.vert_start.as<int>();
+    g.t_verts = c->sym_tiles.verts.as<int>();
+    g.t_local = c->sym_tiles.local_vert.as<int>();
+    g.s_fstart = g.s_vstart = g.s_verts = g.s_local = nullptr;
+    g.A = c->ws.A.as<Cx<float>>();
+    g.B = c->ws.B.as<Cx<float>>();
+    g.ld = c->ws.ld;
+    g.F = c->F;
+    g.k = (float)k;
+    g.eta = (float)eta;
+    g.k2 = (float)(k * k);
+    const size_t smem = sym_smem_bytes<Q>();
+    BB_CUDA(cudaFuncSetAttribute(sym_pairs_kernel<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int64_t nt = c->sym_tiles.ntiles;
+    const int64_t blocks = nt * (nt + 1) / 2;
+    BB_REQUIRE(blocks < (1ll << 31), BEAT_B200_INVALID_ARG, "assembly: mesh too large for the tile-pair grid");
+    sym_pairs_kernel<Q><<<(unsigned)blocks, REG_THREADS, smem, c->stream>>>(g);
+    BB_CUDA(cudaGetLastError());
+}
+
 template <typename T> static void assemble_t(beat_b200_ctx *c, double k, double eta, int R, const Cx<double> *q,
                                              float *ms_total, float *ms_singular) {
     Workspace &w = c->ws;
@@ -463,10 +737,18 @@ template <typename T> static void assemble_t(beat_b200_ctx *c, double k, double 
     BB_CUDA(cudaMemsetAsync(w.A.p, 0, (size_t)N * w.ld * sizeof(Cx<T>), c->stream));
     BB_CUDA(cudaMemsetAsync(w.B.p, 0, (size_t)N * F * sizeof(Cx<T>), c->stream));
     BB_CUDA(cudaEventRecord(c->ev[8], c->stream));
-    switch (c->Q) {
-        case 1: launch_regular<T, 1>(c, k, eta); break;
-        case 3: launch_regular<T, 3>(c, k, eta); break;
-        default: launch_regular<T, 6>(c, k, eta); break;
+    if (sizeof(T) == 4) {
+        switch (c->Q) {
+            case 1: launch_sym<1>(c, k, eta); break;
+            case 3: launch_sym<3>(c, k, eta); break;
+            default: launch_sym<6>(c, k, eta); break;
+        }
+    } else {
+        switch (c->Q) {
+            case 1: launch_regular<T, 1>(c, k, eta); break;
+            case 3: launch_regular<T, 3>(c, k, eta); break;
+            default: launch_regular<T, 6>(c, k, eta); break;
+        }
     }
     BB_CUDA(cudaEventRecord(c->ev[1], c->stream));
     if (c->npairs > 0) {

@@ -255,6 +255,7 @@ static void build_tiling(Tiling &t, int max_faces, int max_verts, const std::vec
 // element-pair kernel tile shapes (must match assembly.cu)
 constexpr int TEST_TILE_FACES = 64, TEST_TILE_VERTS = 80;
 constexpr int TRIAL_TILE_FACES = 16, TRIAL_TILE_VERTS = 32;
+constexpr int SYM_TILE_FACES = 32, SYM_TILE_VERTS = 40;  // both roles of the symmetric kernel
 
 void set_mesh(beat_b200_ctx *c, int V, const double *verts, int F, const int32_t *faces,
               int quad_order, int sing_order) {
@@ -380,6 +381,7 @@ void set_mesh(beat_b200_ctx *c, int V, const double *verts, int F, const int32_t
     upload(c->pos_gvert, pos_gv);
     build_tiling(c->test_tiles, TEST_TILE_FACES, TEST_TILE_VERTS, pos_gv, F);
     build_tiling(c->trial_tiles, TRIAL_TILE_FACES, TRIAL_TILE_VERTS, pos_gv, F);
+    build_tiling(c->sym_tiles, SYM_TILE_FACES, SYM_TILE_VERTS, pos_gv, F);
 
     upload(c->d_verts, c->verts);
     upload(c->d_faces, c->faces);
@@ -536,7 +538,7 @@ int64_t device_bytes(const beat_b200_ctx *c) {
                             &c->sp_test, &c->sp_trial, &c->sp_rule, &c->sp_jac, &c->sp_nn, &c->rule_start,
                             &c->rule_data, &c->status, &c->barrier})
         s += (int64_t)b->bytes;
-    for (const Tiling *t : {&c->test_tiles, &c->trial_tiles})
+    for (const Tiling *t : {&c->test_tiles, &c->trial_tiles, &c->sym_tiles})
         s += (int64_t)(t->face_start.bytes + t->vert_start.bytes + t->verts.bytes + t->local_vert.bytes);
     return s;
 }

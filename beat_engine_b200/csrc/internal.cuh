@@ -156,6 +156,7 @@ struct beat_b200_ctx {
     bb::DevBuf pos_area32;
     bb::DevBuf pos_gvert;         // F x 3 global vertex ids
     bb::Tiling test_tiles, trial_tiles;
+    bb::Tiling sym_tiles;         // square tiles of the symmetric element-pair kernel
 
     // device mesh data by original face id
     bb::DevBuf d_verts;           // V x 3 double
