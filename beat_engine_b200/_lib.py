@@ -25,6 +25,7 @@ EXPORTS = (
     "beat_b200_last_error", "beat_b200_set_mesh", "beat_b200_solve", "beat_b200_solve_device",
     "beat_b200_field", "beat_b200_farfield", "beat_b200_farfield_device", "beat_b200_assemble",
     "beat_b200_release_workspace", "beat_b200_device_bytes", "beat_b200_stream", "beat_b200_resolve_noalloc",
+    "beat_b200_sweep", "beat_b200_sweep_device",
 )
 
 
@@ -99,6 +100,12 @@ def load(path: str = LIB_PATH):
     L.beat_b200_stream.restype = vp
     L.beat_b200_resolve_noalloc.argtypes = [vp, i32, vp, vp]
     L.beat_b200_resolve_noalloc.restype = i32
+    L.beat_b200_sweep.argtypes = [vp, i32, dp, dp, i32, dp, ctypes.POINTER(Opts), dp, i32, dp, dp,
+                                  ctypes.POINTER(Diag)]
+    L.beat_b200_sweep.restype = i32
+    L.beat_b200_sweep_device.argtypes = [vp, i32, dp, dp, i32, vp, ctypes.POINTER(Opts), vp, i32, dp, vp,
+                                         ctypes.POINTER(Diag)]
+    L.beat_b200_sweep_device.restype = i32
     _lib = L
     return L
 
@@ -221,6 +228,47 @@ class Context:
         self._check(self.lib.beat_b200_farfield_device(self.handle, float(k_signed), dirs.shape[0], _dp(dirs), R,
                                                        ctypes.c_void_p(d_p_ptr), ctypes.c_void_p(d_q_ptr),
                                                        ctypes.c_void_p(d_out_ptr)))
+
+    def sweep(self, k_signed, eta, q, opts: Opts | None = None, dirs=None):
+        """Frequency sweep through beat_b200_sweep: q is F x R x nfreq complex128
+        (frequency f's Neumann data in q[:, :, f]).  Returns (p: N x R x nfreq,
+        far field: M x R x nfreq or None, per-frequency diagnostics)."""
+        k_signed = np.ascontiguousarray(k_signed, dtype=np.float64).ravel()
+        eta = np.ascontiguousarray(eta, dtype=np.float64).ravel()
+        nf = k_signed.size
+        if eta.size != nf:
+            raise ValueError("k_signed and eta must have one entry per frequency")
+        q = np.asfortranarray(np.asarray(q, dtype=np.complex128).reshape(self.F, -1, nf))
+        R = q.shape[1]
+        p = np.zeros((self.V, R, nf), dtype=np.complex128, order="F")
+        M = 0
+        dd = None
+        ff = None
+        if dirs is not None:
+            dd = np.ascontiguousarray(dirs, dtype=np.float64).reshape(-1, 3)
+            M = dd.shape[0]
+            ff = np.zeros((M, R, nf), dtype=np.complex128, order="F")
+        diags = (Diag * max(nf, 1))()
+        self._check(self.lib.beat_b200_sweep(
+            self.handle, nf, _dp(k_signed), _dp(eta), R, _dp(q), ctypes.byref(opts) if opts is not None else None,
+            _dp(p), M, _dp(dd) if dd is not None else None, _dp(ff) if ff is not None else None, diags))
+        return p, ff, [diags[i].as_dict() for i in range(nf)]
+
+    def sweep_device(self, k_signed, eta, d_q_ptr: int, R: int, d_p_ptr: int, opts: Opts | None = None,
+                     dirs=None, d_ff_ptr: int = 0) -> list:
+        """beat_b200_sweep_device: q, p and the far field in device memory
+        (F x R, N x R and M x R complex128 slices, one per frequency)."""
+        k_signed = np.ascontiguousarray(k_signed, dtype=np.float64).ravel()
+        eta = np.ascontiguousarray(eta, dtype=np.float64).ravel()
+        nf = k_signed.size
+        dd = np.ascontiguousarray(dirs, dtype=np.float64).reshape(-1, 3) if dirs is not None else None
+        M = 0 if dd is None else dd.shape[0]
+        diags = (Diag * max(nf, 1))()
+        self._check(self.lib.beat_b200_sweep_device(
+            self.handle, nf, _dp(k_signed), _dp(eta), R, ctypes.c_void_p(d_q_ptr),
+            ctypes.byref(opts) if opts is not None else None, ctypes.c_void_p(d_p_ptr), M,
+            _dp(dd) if dd is not None else None, ctypes.c_void_p(d_ff_ptr), diags))
+        return [diags[i].as_dict() for i in range(nf)]
 
     def release_workspace(self):
         self._check(self.lib.beat_b200_release_workspace(self.handle))

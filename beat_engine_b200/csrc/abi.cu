@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstring>
 #include <new>
+#include <thread>
 
 #include "internal.cuh"
 
@@ -142,6 +143,64 @@ void solve_core(beat_b200_ctx *c, double k, double eta, int R, const double *d_q
                "GMRES refinement missed its tolerance (worst relative residual " + std::to_string(ir.residual) + ")");
 }
 
+// ---------------------------------------------------------------------------
+// frequency sweep over solve lanes
+// ---------------------------------------------------------------------------
+constexpr int SWEEP_LANES = 2;
+
+// lane i of c (lane 0 is c itself); created on first use with c's mesh
+beat_b200_ctx *sweep_lane(beat_b200_ctx *c, int i) {
+    if (i == 0) return c;
+    while ((int)c->lanes.size() < i) {
+        beat_b200_ctx *l = nullptr;
+        const int32_t st = beat_b200_create(c->device, &l);
+        BB_REQUIRE(st == BEAT_B200_OK, st, "sweep: could not create a solve lane");
+        c->lanes.push_back(l);
+        std::vector<int32_t> faces1(c->faces.size());
+        for (size_t j = 0; j < faces1.size(); ++j) faces1[j] = c->faces[j] + 1;
+        BB_CUDA(cudaSetDevice(c->device));
+        set_mesh(l, c->V, c->verts.data(), c->F, faces1.data(), c->quad_order, c->sing_order);
+    }
+    return c->lanes[i - 1];
+}
+
+// Runs work(lane_ctx, f) for f = 0..nfreq-1, frequency f on lane f % L, one
+// host thread per lane (lane 0 on the calling thread).  The first error (by
+// frequency) is rethrown after every lane has stopped.
+template <typename W> void run_sweep(beat_b200_ctx *c, int nfreq, W &&work) {
+    const int L = std::min(SWEEP_LANES, nfreq);
+    std::vector<beat_b200_ctx *> lane(L);
+    for (int i = 0; i < L; ++i) lane[i] = sweep_lane(c, i);
+    std::vector<Error> err(L);
+    std::vector<int> err_f(L, -1);
+    auto body = [&](int i) {
+        try {
+            BB_CUDA(cudaSetDevice(c->device));
+            for (int f = i; f < nfreq; f += L) {
+                err_f[i] = f;
+                work(lane[i], f);
+            }
+            err_f[i] = -1;
+        } catch (const Error &e) {
+            err[i] = e;
+        } catch (const std::bad_alloc &) {
+            err[i] = Error{BEAT_B200_OOM, "host allocation failed"};
+        } catch (...) {
+            err[i] = Error{BEAT_B200_CUDA_ERROR, "unexpected exception"};
+        }
+        if (err_f[i] >= 0 && lane[i]->stream) cudaStreamSynchronize(lane[i]->stream);
+    };
+    std::vector<std::thread> th;
+    for (int i = 1; i < L; ++i) th.emplace_back(body, i);
+    body(0);
+    for (auto &t : th) t.join();
+    int first = -1;
+    for (int i = 0; i < L; ++i)
+        if (err_f[i] >= 0 && (first < 0 || err_f[i] < err_f[first])) first = i;
+    if (first >= 0)
+        throw Error{err[first].code, "frequency " + std::to_string(err_f[first]) + ": " + err[first].msg};
+}
+
 }  // namespace
 
 extern "C" {
@@ -195,6 +254,8 @@ int32_t beat_b200_create(int32_t device, beat_b200_ctx **out) {
 
 int32_t beat_b200_destroy(beat_b200_ctx *c) {
     if (!c) return BEAT_B200_OK;
+    for (beat_b200_ctx *l : c->lanes) beat_b200_destroy(l);
+    c->lanes.clear();
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     release_workspace(c);
@@ -221,7 +282,11 @@ const char *beat_b200_last_error(const beat_b200_ctx *c) { return c ? c->last_er
 
 int32_t beat_b200_set_mesh(beat_b200_ctx *c, int32_t V, const double *vertices, int32_t F, const int32_t *faces,
                            int32_t quad_order, int32_t singular_order) {
-    return guarded(c, [&] { set_mesh(c, V, vertices, F, faces, quad_order, singular_order); });
+    return guarded(c, [&] {
+        for (beat_b200_ctx *l : c->lanes) beat_b200_destroy(l);  // lanes hold the previous mesh
+        c->lanes.clear();
+        set_mesh(c, V, vertices, F, faces, quad_order, singular_order);
+    });
 }
 
 int32_t beat_b200_solve_device(beat_b200_ctx *c, double k, double eta, int32_t R, const void *d_q,
@@ -339,10 +404,66 @@ int32_t beat_b200_release_workspace(beat_b200_ctx *c) {
     return guarded(c, [&] {
         BB_CUDA(cudaStreamSynchronize(c->stream));
         release_workspace(c);
+        for (beat_b200_ctx *l : c->lanes) {
+            BB_CUDA(cudaStreamSynchronize(l->stream));
+            release_workspace(l);
+        }
     });
 }
 
-int64_t beat_b200_device_bytes(const beat_b200_ctx *c) { return c ? device_bytes(c) : 0; }
+int64_t beat_b200_device_bytes(const beat_b200_ctx *c) {
+    if (!c) return 0;
+    int64_t s = device_bytes(c);
+    for (const beat_b200_ctx *l : c->lanes) s += device_bytes(l);
+    return s;
+}
+
+int32_t beat_b200_sweep_device(beat_b200_ctx *c, int32_t nfreq, const double *k_signed, const double *eta_im,
+                               int32_t R, const void *d_q, const beat_b200_opts *opts, void *d_p, int32_t M,
+                               const double *dirs, void *d_ff, beat_b200_diag *diags) {
+    return guarded(c, [&] {
+        BB_REQUIRE(nfreq >= 0 && R >= 1, BEAT_B200_INVALID_ARG, "sweep: nfreq must be >= 0 and R >= 1");
+        if (nfreq == 0) return;
+        BB_REQUIRE(k_signed && eta_im && d_q && d_p, BEAT_B200_INVALID_ARG, "sweep: null pointer");
+        BB_REQUIRE(M >= 0 && (M == 0 || (dirs && d_ff)), BEAT_B200_INVALID_ARG, "sweep: bad far-field arguments");
+        BB_REQUIRE(c->F > 0, BEAT_B200_STATE, "no mesh: call beat_b200_set_mesh first");
+        const beat_b200_opts o = resolve_opts(opts);
+        const size_t qs = (size_t)c->F * R * 2, ps = (size_t)c->V * R * 2, fs = (size_t)M * R * 2;
+        run_sweep(c, nfreq, [&](beat_b200_ctx *l, int f) {
+            const double *q = (const double *)d_q + f * qs;
+            double *p = (double *)d_p + f * ps;
+            solve_core(l, k_signed[f], eta_im[f], R, q, o, p, diags ? diags + f : nullptr);
+            if (M > 0) farfield(l, k_signed[f], M, dirs, R, p, q, (double *)d_ff + f * fs, true);
+        });
+    });
+}
+
+int32_t beat_b200_sweep(beat_b200_ctx *c, int32_t nfreq, const double *k_signed, const double *eta_im, int32_t R,
+                        const double *q, const beat_b200_opts *opts, double *p_out, int32_t M, const double *dirs,
+                        double *ff_out, beat_b200_diag *diags) {
+    return guarded(c, [&] {
+        BB_REQUIRE(nfreq >= 0 && R >= 1, BEAT_B200_INVALID_ARG, "sweep: nfreq must be >= 0 and R >= 1");
+        if (nfreq == 0) return;
+        BB_REQUIRE(k_signed && eta_im && q && p_out, BEAT_B200_INVALID_ARG, "sweep: null pointer");
+        BB_REQUIRE(M >= 0 && (M == 0 || (dirs && ff_out)), BEAT_B200_INVALID_ARG, "sweep: bad far-field arguments");
+        BB_REQUIRE(c->F > 0, BEAT_B200_STATE, "no mesh: call beat_b200_set_mesh first");
+        const beat_b200_opts o = resolve_opts(opts);
+        const size_t qs = (size_t)c->F * R * 2, ps = (size_t)c->V * R * 2, fs = (size_t)M * R * 2;
+        run_sweep(c, nfreq, [&](beat_b200_ctx *l, int f) {
+            ensure_workspace(l, o.precision, R);
+            Workspace &w = l->ws;
+            BB_CUDA(cudaMemcpyAsync(w.q.p, q + f * qs, qs * sizeof(double), cudaMemcpyHostToDevice, l->stream));
+            w.io.alloc((ps + fs) * sizeof(double));
+            double *dp = w.io.as<double>(), *dff = dp + ps;
+            solve_core(l, k_signed[f], eta_im[f], R, w.q.as<double>(), o, dp, diags ? diags + f : nullptr);
+            if (M > 0) farfield(l, k_signed[f], M, dirs, R, dp, w.q.as<double>(), dff, true);
+            BB_CUDA(cudaMemcpyAsync(p_out + f * ps, dp, ps * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
+            if (M > 0)
+                BB_CUDA(cudaMemcpyAsync(ff_out + f * fs, dff, fs * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
+            BB_CUDA(cudaStreamSynchronize(l->stream));
+        });
+    });
+}
 
 void *beat_b200_stream(const beat_b200_ctx *c) { return c ? (void *)c->stream : nullptr; }
 

@@ -183,6 +183,10 @@ struct beat_b200_ctx {
     float last_regular_ms = 0.f;
     bool cluster_checked = false;  // can a 16-CTA cluster of the panel kernel be scheduled?
     bool cluster_ok = false;
+
+    // extra solve lanes of a frequency sweep: each a full context (own stream,
+    // workspace and status words) over a copy of this mesh
+    std::vector<beat_b200_ctx *> lanes;
 };
 
 namespace bb {

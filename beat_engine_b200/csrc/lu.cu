@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 
 #include "internal.cuh"
@@ -929,7 +930,7 @@ static bool cluster_panel(beat_b200_ctx *c, Cx<T> *A, int64_t ld, int n, int k, 
         return false;
     const size_t smem = cluster_panel_smem<T>(rpc, w);
     if (smem > cap) return false;
-    static bool attr_done[2] = {false, false};
+    static std::atomic<bool> attr_done[2] = {false, false};  // sweep lanes call this from several threads
     const int ti = sizeof(T) == 8;
     if (!attr_done[ti]) {
         BB_CUDA(cudaFuncSetAttribute(cluster_panel_kernel<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));

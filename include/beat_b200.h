@@ -162,6 +162,31 @@ int64_t beat_b200_device_bytes(const beat_b200_ctx *ctx);
  * stream capture.  Synchronises the context's stream before returning. */
 int32_t beat_b200_resolve_noalloc(beat_b200_ctx *ctx, int32_t R, const void *d_b, void *d_x);
 
+/* Frequency sweep: nfreq independent solves of this mesh, each followed by
+ * its far field at M directions (M = 0: none).  Replaces the per-frequency
+ * loop of solve_exterior_request (BeatEngineCompiledDriver.jl:1269-1592),
+ * which calls solve_exterior_direct_cuda once per frequency (:1338) and
+ * overlaps the next frequency's assembly with the current solve only on its
+ * Metal path (start_sweep_assembly_pipeline, :1265).  Frequencies are
+ * pipelined over two solve lanes (each with its own stream and workspace, the
+ * second created on first use with a copy of the mesh), driven by two host
+ * threads: one frequency's assembly runs beside the other's factorisation.
+ * Frequency f uses k_signed[f], eta_im[f], q + f F R, p_out + f N R and
+ * ff_out + f M R (complex doubles, column-major slices as in
+ * beat_b200_solve); diags (NULL or nfreq entries) receives each solve's
+ * diagnostics.  The first failing frequency's status is returned. */
+int32_t beat_b200_sweep(beat_b200_ctx *ctx, int32_t nfreq, const double *k_signed,
+                        const double *eta_im, int32_t R, const double *q,
+                        const beat_b200_opts *opts, double *p_out, int32_t M, const double *dirs,
+                        double *ff_out, beat_b200_diag *diags);
+
+/* As beat_b200_sweep with q, p_out and ff_out in device memory (dirs, k and
+ * eta stay host). */
+int32_t beat_b200_sweep_device(beat_b200_ctx *ctx, int32_t nfreq, const double *k_signed,
+                               const double *eta_im, int32_t R, const void *d_q,
+                               const beat_b200_opts *opts, void *d_p, int32_t M,
+                               const double *dirs, void *d_ff, beat_b200_diag *diags);
+
 /* The CUDA stream (cudaStream_t) every kernel of this context is launched
  * on, so a caller can order its own work or record timing events on it.
  * Entry points return only after their work on it has completed. */
