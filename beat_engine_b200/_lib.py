@@ -25,7 +25,7 @@ EXPORTS = (
     "beat_b200_last_error", "beat_b200_set_mesh", "beat_b200_solve", "beat_b200_solve_device",
     "beat_b200_field", "beat_b200_farfield", "beat_b200_farfield_device", "beat_b200_assemble",
     "beat_b200_release_workspace", "beat_b200_device_bytes", "beat_b200_stream", "beat_b200_resolve_noalloc",
-    "beat_b200_sweep", "beat_b200_sweep_device",
+    "beat_b200_sweep", "beat_b200_sweep_device", "beat_b200_set_admittance", "beat_b200_adjoint",
 )
 
 
@@ -106,6 +106,10 @@ def load(path: str = LIB_PATH):
     L.beat_b200_sweep_device.argtypes = [vp, i32, dp, dp, i32, vp, ctypes.POINTER(Opts), vp, i32, dp, vp,
                                          ctypes.POINTER(Diag)]
     L.beat_b200_sweep_device.restype = i32
+    L.beat_b200_set_admittance.argtypes = [vp, dp]
+    L.beat_b200_set_admittance.restype = i32
+    L.beat_b200_adjoint.argtypes = [vp, f64, i32, dp, i32, dp, dp, ctypes.POINTER(Opts), dp, dp]
+    L.beat_b200_adjoint.restype = i32
     _lib = L
     return L
 
@@ -269,6 +273,35 @@ class Context:
             ctypes.byref(opts) if opts is not None else None, ctypes.c_void_p(d_p_ptr), M,
             _dp(dd) if dd is not None else None, ctypes.c_void_p(d_ff_ptr), diags))
         return [diags[i].as_dict() for i in range(nf)]
+
+    def set_admittance(self, a=None):
+        """Per-face admittance coefficients a (F complex): later solves use
+        q = q0 - a (P p).  None clears them."""
+        if a is None:
+            self._check(self.lib.beat_b200_set_admittance(self.handle, None))
+            return
+        a = np.ascontiguousarray(np.asarray(a, dtype=np.complex128).ravel())
+        if a.size != self.F:
+            raise ValueError(f"expected {self.F} coefficients, got {a.size}")
+        self._check(self.lib.beat_b200_set_admittance(self.handle, _dp(a)))
+
+    def adjoint(self, k_signed: float, dirs, p, g, opts: Opts | None = None, want_admittance: bool = True):
+        """Gradients of a real far-field functional after a solve at k_signed:
+        g = dJ/d conj(p_inf) (M x R).  Returns (dJ/d conj(q0): F x R,
+        dJ/d conj(a): F or None)."""
+        dd = np.ascontiguousarray(dirs, dtype=np.float64).reshape(-1, 3)
+        M = dd.shape[0]
+        pf = _c128_f(p, self.V)
+        R = pf.shape[1]
+        gf = _c128_f(g, M)
+        if gf.shape[1] != R:
+            raise ValueError("p and g need the same number of columns")
+        w = np.zeros((self.F, R), dtype=np.complex128, order="F")
+        ga = np.zeros(self.F, dtype=np.complex128) if want_admittance else None
+        self._check(self.lib.beat_b200_adjoint(self.handle, float(k_signed), M, _dp(dd), R, _dp(pf), _dp(gf),
+                                               ctypes.byref(opts) if opts is not None else None, _dp(w),
+                                               _dp(ga) if ga is not None else None))
+        return w, ga
 
     def release_workspace(self):
         self._check(self.lib.beat_b200_release_workspace(self.handle))

@@ -90,12 +90,14 @@ void solve_core(beat_b200_ctx *c, double k, double eta, int R, const double *d_q
     const int n = c->V;
     float ms_asm = 0, ms_sing = 0, ms_lu = 0, ms_solve = 0, ms_ir = 0;
     assemble(c, k, eta, o.precision, R, d_q, &ms_asm, &ms_sing);
+    apply_admittance_lhs(c, o.precision);  // A += B diag(a) P when an admittance is set
     if (o.precision != BEAT_B200_FP64)
         BB_CUDA(cudaMemcpyAsync(w.Aop.p, w.A.p, (size_t)n * w.ld * 8, cudaMemcpyDeviceToDevice, c->stream));
     BB_CUDA(cudaEventRecord(c->ev[4], c->stream));
     lu_factor(c, o.precision, o.lu_block, o.lu_split_terms);
     BB_CUDA(cudaEventRecord(c->ev[5], c->stream));
     const int st = read_status(c);
+    c->last_k = k;
     BB_REQUIRE(!(st & DEV_BARRIER_TIMEOUT), BEAT_B200_TIMEOUT, "LU panel: grid barrier ran out of its wait budget");
     BB_REQUIRE(!(st & DEV_ZERO_PIVOT), BEAT_B200_SINGULAR, "LU: exact zero pivot (singular system)");
     IrResult ir{0, 1, 0.0};
@@ -171,6 +173,14 @@ template <typename W> void run_sweep(beat_b200_ctx *c, int nfreq, W &&work) {
     const int L = std::min(SWEEP_LANES, nfreq);
     std::vector<beat_b200_ctx *> lane(L);
     for (int i = 0; i < L; ++i) lane[i] = sweep_lane(c, i);
+    for (int i = 1; i < L; ++i) {  // the lanes solve with this context's admittance
+        lane[i]->adm_set = c->adm_set;
+        if (c->adm_set) {
+            lane[i]->adm.alloc(c->adm.bytes);
+            BB_CUDA(cudaMemcpy(lane[i]->adm.p, c->adm.p, c->adm.bytes, cudaMemcpyDeviceToDevice));
+        }
+        lane[i]->ws.lu_valid = 0;
+    }
     std::vector<Error> err(L);
     std::vector<int> err_f(L, -1);
     auto body = [&](int i) {
@@ -261,7 +271,8 @@ int32_t beat_b200_destroy(beat_b200_ctx *c) {
     release_workspace(c);
     for (DevBuf *b : {&c->pos_face, &c->pos_qpts64, &c->pos_qpts32, &c->pos_normal64, &c->pos_normal32,
                       &c->pos_curl64, &c->pos_curl32, &c->pos_area64, &c->pos_area32, &c->pos_gvert, &c->d_verts,
-                      &c->d_faces, &c->d_normals, &c->d_areas, &c->d_curls, &c->d_qpts, &c->sp_test, &c->sp_trial,
+                      &c->d_faces, &c->d_normals, &c->d_areas, &c->d_curls, &c->d_qpts, &c->vf_start, &c->vf_face,
+                      &c->adm, &c->sp_test, &c->sp_trial,
                       &c->sp_rule, &c->sp_jac, &c->sp_nn, &c->rule_start, &c->rule_data, &c->status, &c->barrier})
         b->free_();
     for (Tiling *t : {&c->test_tiles, &c->trial_tiles, &c->sym_tiles}) {
@@ -462,6 +473,50 @@ int32_t beat_b200_sweep(beat_b200_ctx *c, int32_t nfreq, const double *k_signed,
                 BB_CUDA(cudaMemcpyAsync(ff_out + f * fs, dff, fs * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
             BB_CUDA(cudaStreamSynchronize(l->stream));
         });
+    });
+}
+
+int32_t beat_b200_set_admittance(beat_b200_ctx *c, const double *a) {
+    return guarded(c, [&] {
+        BB_REQUIRE(c->F > 0, BEAT_B200_STATE, "no mesh: call beat_b200_set_mesh first");
+        BB_CUDA(cudaStreamSynchronize(c->stream));
+        if (!a) {
+            c->adm_set = false;
+        } else {
+            for (size_t i = 0; i < 2 * (size_t)c->F; ++i)
+                BB_REQUIRE(std::isfinite(a[i]), BEAT_B200_INVALID_ARG, "admittance: non-finite coefficient");
+            c->adm.alloc(sizeof(double) * 2 * (size_t)c->F);
+            BB_CUDA(cudaMemcpy(c->adm.p, a, sizeof(double) * 2 * (size_t)c->F, cudaMemcpyHostToDevice));
+            c->adm_set = true;
+        }
+        c->ws.lu_valid = 0;  // the factors belong to the previous operator
+    });
+}
+
+int32_t beat_b200_adjoint(beat_b200_ctx *c, double k_signed, int32_t M, const double *dirs, int32_t R,
+                          const double *p, const double *g, const beat_b200_opts *opts, double *w_out,
+                          double *ga_out) {
+    return guarded(c, [&] {
+        BB_REQUIRE(dirs && p && g && w_out, BEAT_B200_INVALID_ARG, "adjoint: null pointer");
+        BB_REQUIRE(c->F > 0, BEAT_B200_STATE, "no mesh: call beat_b200_set_mesh first");
+        BB_REQUIRE(M >= 1 && R >= 1, BEAT_B200_INVALID_ARG, "adjoint: M and R must be >= 1");
+        const beat_b200_opts o = resolve_opts(opts);
+        const size_t np = (size_t)c->V * R, ng = (size_t)M * R, nw = (size_t)c->F * R;
+        DevBuf &io = c->ws.io;
+        io.alloc(sizeof(double2) * (np + ng + nw + c->F));
+        double2 *dp = io.as<double2>(), *dg = dp + np, *dw = dg + ng, *dga = dw + nw;
+        BB_CUDA(cudaMemcpyAsync(dp, p, sizeof(double2) * np, cudaMemcpyHostToDevice, c->stream));
+        BB_CUDA(cudaMemcpyAsync(dg, g, sizeof(double2) * ng, cudaMemcpyHostToDevice, c->stream));
+        IrResult ir{0, 1, 0.0};
+        adjoint(c, k_signed, M, dirs, R, (const double *)dp, (const double *)dg, (double *)dw,
+                ga_out ? (double *)dga : nullptr, o, &ir);
+        BB_CUDA(cudaMemcpyAsync(w_out, dw, sizeof(double2) * nw, cudaMemcpyDeviceToHost, c->stream));
+        if (ga_out)
+            BB_CUDA(cudaMemcpyAsync(ga_out, dga, sizeof(double2) * c->F, cudaMemcpyDeviceToHost, c->stream));
+        BB_CUDA(cudaStreamSynchronize(c->stream));
+        BB_REQUIRE(ir.converged, BEAT_B200_NOT_CONVERGED,
+                   "adjoint refinement missed its tolerance (worst relative residual " + std::to_string(ir.residual) +
+                       ")");
     });
 }
 

@@ -385,6 +385,20 @@ void set_mesh(beat_b200_ctx *c, int V, const double *verts, int F, const int32_t
 
     upload(c->d_verts, c->verts);
     upload(c->d_faces, c->faces);
+    {
+        // vertex -> incident faces (CSR), for the admittance terms
+        std::vector<int> vstart(V + 1, 0), vface(3 * (size_t)F);
+        for (int f = 0; f < F; ++f)
+            for (int a = 0; a < 3; ++a) ++vstart[c->faces[3 * f + a] + 1];
+        for (int v = 0; v < V; ++v) vstart[v + 1] += vstart[v];
+        std::vector<int> fill(vstart.begin(), vstart.end() - 1);
+        for (int f = 0; f < F; ++f)
+            for (int a = 0; a < 3; ++a) vface[fill[c->faces[3 * f + a]]++] = f;
+        upload(c->vf_start, vstart);
+        upload(c->vf_face, vface);
+    }
+    c->adm.free_();
+    c->adm_set = false;
     upload(c->d_normals, c->normals);
     upload(c->d_areas, c->areas);
     upload(c->d_curls, curls);
@@ -518,7 +532,7 @@ void ensure_workspace(beat_b200_ctx *c, int precision, int R) {
 void release_workspace(beat_b200_ctx *c) {
     Workspace &w = c->ws;
     for (DevBuf *b : {&w.A, &w.Aop, &w.B, &w.b, &w.x, &w.ipiv, &w.perm, &w.panel_scratch, &w.stage, &w.krylov,
-                      &w.small, &w.q, &w.small_solve, &w.dinv, &w.field, &w.io})
+                      &w.small, &w.q, &w.small_solve, &w.dinv, &w.field, &w.io, &w.qeff})
         b->free_();
     w.precision = -1;
     w.N = w.F = w.R = 0;
@@ -530,11 +544,12 @@ int64_t device_bytes(const beat_b200_ctx *c) {
     int64_t s = 0;
     const Workspace &w = c->ws;
     for (const DevBuf *b : {&w.A, &w.Aop, &w.B, &w.b, &w.x, &w.ipiv, &w.perm, &w.panel_scratch, &w.stage, &w.krylov,
-                            &w.small, &w.q, &w.small_solve, &w.dinv, &w.field, &w.io})
+                            &w.small, &w.q, &w.small_solve, &w.dinv, &w.field, &w.io, &w.qeff})
         s += (int64_t)b->bytes;
     for (const DevBuf *b : {&c->pos_face, &c->pos_qpts64, &c->pos_qpts32, &c->pos_normal64, &c->pos_normal32,
                             &c->pos_curl64, &c->pos_curl32, &c->pos_area64, &c->pos_area32, &c->pos_gvert,
                             &c->d_verts, &c->d_faces, &c->d_normals, &c->d_areas, &c->d_curls, &c->d_qpts,
+                            &c->vf_start, &c->vf_face, &c->adm,
                             &c->sp_test, &c->sp_trial, &c->sp_rule, &c->sp_jac, &c->sp_nn, &c->rule_start,
                             &c->rule_data, &c->status, &c->barrier})
         s += (int64_t)b->bytes;

@@ -143,6 +143,11 @@ void farfield(beat_b200_ctx *c, double k, int M, const double *pts_host, int R, 
     BB_REQUIRE(M >= 0 && R >= 1, BEAT_B200_INVALID_ARG, "field: M must be >= 0 and R >= 1");
     if (M == 0) return;
     const int F = c->F, Q = c->Q, S = F * Q, N = c->V;
+    if (c->adm_set) {  // the boundary's Neumann data include the admittance term
+        c->ws.qeff.alloc(sizeof(double2) * (size_t)F * R);
+        effective_neumann(c, R, p_dev, q_dev, c->ws.qeff.as<double>());
+        q_dev = c->ws.qeff.as<double>();
+    }
     // rule weight + basis per point
     std::vector<double> rw3(4 * (size_t)Q);
     for (int q = 0; q < Q; ++q) {

@@ -118,12 +118,89 @@ template void tall_gemm<float>(cudaStream_t, int, const Cx<float> *, int64_t, in
 template void tall_gemm<double>(cudaStream_t, int, const Cx<double> *, int64_t, int, int, const double *, double *,
                                 int, double);
 
+// ---------------------------------------------------------------------------
+// Conjugate-transposed tall product Y += alpha M^H X: M complex row-major
+// rows x cols, X FP64 column-major rows x R, Y FP64 column-major cols x R.
+// One thread per column of M (consecutive threads read consecutive entries of
+// a row), all TG_RC right-hand sides in FP64 registers, rows of X staged
+// through shared memory; row slices add into Y with FP64 atomics.  Used by
+// the adjoint (B^H, and A^H inside the adjoint refinement).
+// ---------------------------------------------------------------------------
+constexpr int TGH_KC = 32;
+
+template <typename T>
+__global__ void __launch_bounds__(TG_THREADS, 2) tall_gemm_h_kernel(const Cx<T> *M, int64_t ld, int rows, int cols,
+                                                                    const double2 *X, double2 *Y, int R, int r0,
+                                                                    double alpha, int islice) {
+    __shared__ double2 sX[TGH_KC][TG_RC];
+    const int j = blockIdx.x * TG_THREADS + (int)threadIdx.x;
+    const int ib = blockIdx.y * islice, ie = min(rows, ib + islice);
+    const int rc = min(TG_RC, R - r0);
+    double ar[TG_RC], ai[TG_RC];
+#pragma unroll
+    for (int e = 0; e < TG_RC; ++e) ar[e] = ai[e] = 0.0;
+    for (int i0 = ib; i0 < ie; i0 += TGH_KC) {
+        const int kn = min(TGH_KC, ie - i0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < TGH_KC * TG_RC; t += TG_THREADS) {
+            const int cidx = t / TGH_KC, k = t % TGH_KC;
+            sX[k][cidx] = (cidx < rc && k < kn) ? X[(size_t)(r0 + cidx) * rows + i0 + k] : make_double2(0, 0);
+        }
+        __syncthreads();
+        if (j < cols) {
+#pragma unroll 4
+            for (int k = 0; k < kn; ++k) {
+                const Cx<T> m = M[(int64_t)(i0 + k) * ld + j];
+                const double mr = (double)m.re, mi = -(double)m.im;  // conj(M[i][j])
+#pragma unroll
+                for (int e = 0; e < TG_RC; ++e) {
+                    const double2 x = sX[k][e];
+                    ar[e] = fma(mr, x.x, fma(-mi, x.y, ar[e]));
+                    ai[e] = fma(mr, x.y, fma(mi, x.x, ai[e]));
+                }
+            }
+        }
+    }
+    if (j < cols) {
+#pragma unroll
+        for (int e = 0; e < TG_RC; ++e)
+            if (e < rc) {
+                double2 *y = &Y[(size_t)(r0 + e) * cols + j];
+                atomicAdd(&y->x, alpha * ar[e]);
+                atomicAdd(&y->y, alpha * ai[e]);
+            }
+    }
+}
+
+template <typename T>
+void tall_gemm_h(cudaStream_t st, int sm_count, const Cx<T> *M, int64_t ld, int rows, int cols, const double *X,
+                 double *Y, int R, double alpha) {
+    const int col_tiles = (cols + TG_THREADS - 1) / TG_THREADS;
+    int slices = std::max(1, (2 * sm_count + col_tiles / 2) / col_tiles);
+    int islice = (rows + slices - 1) / slices;
+    islice = (islice + TGH_KC - 1) / TGH_KC * TGH_KC;
+    slices = (rows + islice - 1) / islice;
+    for (int r0 = 0; r0 < R; r0 += TG_RC)
+        tall_gemm_h_kernel<T><<<dim3(col_tiles, slices), TG_THREADS, 0, st>>>(
+            M, ld, rows, cols, reinterpret_cast<const double2 *>(X), reinterpret_cast<double2 *>(Y), R, r0, alpha,
+            islice);
+    BB_CUDA(cudaGetLastError());
+}
+template void tall_gemm_h<float>(cudaStream_t, int, const Cx<float> *, int64_t, int, int, const double *, double *,
+                                 int, double);
+template void tall_gemm_h<double>(cudaStream_t, int, const Cx<double> *, int64_t, int, int, const double *,
+                                  double *, int, double);
+
 // Y = alpha * A X + beta * Y with beta in {0, 1}
-template <typename T> static void matvec(beat_b200_ctx *c, const Cx<T> *A, const double *X, double *Y, int R,
-                                         double alpha, double beta) {
+// (with ADJ: Y = alpha * A^H X + beta * Y)
+template <typename T, bool ADJ = false>
+static void matvec(beat_b200_ctx *c, const Cx<T> *A, const double *X, double *Y, int R, double alpha, double beta) {
     const int n = c->V;
     if (beta == 0.0) BB_CUDA(cudaMemsetAsync(Y, 0, sizeof(double2) * (size_t)n * R, c->stream));
-    tall_gemm<T>(c->stream, c->sm_count, A, c->ws.ld, n, n, X, Y, R, alpha);
+    if (ADJ)
+        tall_gemm_h<T>(c->stream, c->sm_count, A, c->ws.ld, n, n, X, Y, R, alpha);
+    else
+        tall_gemm<T>(c->stream, c->sm_count, A, c->ws.ld, n, n, X, Y, R, alpha);
 }
 
 // H[i*R + r] = sum_n conj(V_i[n, r]) W[n, r] for i < nv   (one CTA per (i, r))
@@ -223,7 +300,9 @@ __global__ void update_x_kernel(const double2 *Z, size_t zstride, int nz, double
 
 using cd = std::complex<double>;
 
-template <typename T>
+// FGMRES on A (ADJ: on A^H) with the FP32 LU (ADJ: its conjugate transpose)
+// as right preconditioner
+template <typename T, bool ADJ>
 static IrResult gmres_t(beat_b200_ctx *c, int R, double *x_dev, const double *b_dev, int m, int max_iters,
                         double rtol) {
     Workspace &w = c->ws;
@@ -257,7 +336,7 @@ static IrResult gmres_t(beat_b200_ctx *c, int R, double *x_dev, const double *b_
     while (iters < max_iters) {
         // r = b - A x
         BB_CUDA(cudaMemcpyAsync(W, b_dev, sizeof(double2) * vs, cudaMemcpyDeviceToDevice, c->stream));
-        matvec<T>(c, A, x_dev, reinterpret_cast<double *>(W), R, -1.0, 1.0);
+        matvec<T, ADJ>(c, A, x_dev, reinterpret_cast<double *>(W), R, -1.0, 1.0);
         col_norm2_kernel<<<R, 256, 0, c->stream>>>(W, n, R, dH);
         BB_CUDA(cudaMemcpyAsync(hbuf.data(), dH, sizeof(double2) * R, cudaMemcpyDeviceToHost, c->stream));
         BB_CUDA(cudaStreamSynchronize(c->stream));
@@ -276,8 +355,14 @@ static IrResult gmres_t(beat_b200_ctx *c, int R, double *x_dev, const double *b_
         col_scale_kernel<<<blocks_nr, th, 0, c->stream>>>(W, V, n, R, dscale);
         int j = 0;
         for (; j < m && iters < max_iters; ++j, ++iters) {
-            lu_precond_fp32(c, R, reinterpret_cast<const double *>(V + vs * j), reinterpret_cast<double *>(Z + vs * j));
-            matvec<T>(c, A, reinterpret_cast<const double *>(Z + vs * j), reinterpret_cast<double *>(W), R, 1.0, 0.0);
+            if (ADJ)
+                lu_solve_adjoint(c, R, reinterpret_cast<const double *>(V + vs * j),
+                                 reinterpret_cast<double *>(Z + vs * j));
+            else
+                lu_precond_fp32(c, R, reinterpret_cast<const double *>(V + vs * j),
+                                reinterpret_cast<double *>(Z + vs * j));
+            matvec<T, ADJ>(c, A, reinterpret_cast<const double *>(Z + vs * j), reinterpret_cast<double *>(W), R, 1.0,
+                           0.0);
             // CGS2
             BB_CUDA(cudaMemsetAsync(dH2, 0, sizeof(double2) * (size_t)(j + 1) * R, c->stream));
             for (int pass = 0; pass < 2; ++pass) {
@@ -343,7 +428,7 @@ static IrResult gmres_t(beat_b200_ctx *c, int R, double *x_dev, const double *b_
     if (!converged) {
         // final true residual
         BB_CUDA(cudaMemcpyAsync(W, b_dev, sizeof(double2) * vs, cudaMemcpyDeviceToDevice, c->stream));
-        matvec<T>(c, A, x_dev, reinterpret_cast<double *>(W), R, -1.0, 1.0);
+        matvec<T, ADJ>(c, A, x_dev, reinterpret_cast<double *>(W), R, -1.0, 1.0);
         col_norm2_kernel<<<R, 256, 0, c->stream>>>(W, n, R, dH);
         BB_CUDA(cudaMemcpyAsync(hbuf.data(), dH, sizeof(double2) * R, cudaMemcpyDeviceToHost, c->stream));
         BB_CUDA(cudaStreamSynchronize(c->stream));
@@ -362,7 +447,14 @@ IrResult gmres_refine(beat_b200_ctx *c, int R, double *x_dev, const double *b_de
                       double rtol) {
     BB_REQUIRE(restart >= 1 && restart <= 200, BEAT_B200_INVALID_ARG, "GMRES restart must be in 1..200");
     BB_REQUIRE(rtol > 0 && std::isfinite(rtol), BEAT_B200_INVALID_ARG, "GMRES tolerance must be positive");
-    return gmres_t<float>(c, R, x_dev, b_dev, restart, max_iters, rtol);
+    return gmres_t<float, false>(c, R, x_dev, b_dev, restart, max_iters, rtol);
+}
+
+IrResult gmres_refine_adjoint(beat_b200_ctx *c, int R, double *x_dev, const double *b_dev, int restart, int max_iters,
+                              double rtol) {
+    BB_REQUIRE(restart >= 1 && restart <= 200, BEAT_B200_INVALID_ARG, "GMRES restart must be in 1..200");
+    BB_REQUIRE(rtol > 0 && std::isfinite(rtol), BEAT_B200_INVALID_ARG, "GMRES tolerance must be positive");
+    return gmres_t<float, true>(c, R, x_dev, b_dev, restart, max_iters, rtol);
 }
 
 }  // namespace bb

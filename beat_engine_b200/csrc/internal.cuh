@@ -120,6 +120,7 @@ struct Workspace {
     DevBuf dinv;          // FP64 inverses of the 64 x 64 diagonal blocks of L and U
     DevBuf field;         // field sources and evaluation points (grow-only)
     DevBuf io;            // device staging of the host-buffer entry points (grow-only)
+    DevBuf qeff;          // Neumann data with the admittance term, for the field (grow-only)
     int solve_epoch = 0;  // flag value of the latest substitution launch
     int lu_valid = 0;     // factors match the current operator
 };
@@ -165,6 +166,12 @@ struct beat_b200_ctx {
     bb::DevBuf d_areas;           // F double
     bb::DevBuf d_curls;           // F x 9 double
     bb::DevBuf d_qpts;            // F x Q x 3 double (field sources)
+    bb::DevBuf vf_start, vf_face; // vertex -> incident faces (CSR: V + 1 offsets, 3F face ids)
+
+    // admittance boundary condition q = q0 - a (P p), P = face average of P1 p
+    bb::DevBuf adm;               // F complex FP64 coefficients a_f
+    bool adm_set = false;
+    double last_k = 0.0;          // signed wavenumber of the factors in the workspace
 
     // singular (touching) pairs
     int64_t npairs = 0;
@@ -222,6 +229,20 @@ struct IrResult {
 };
 IrResult gmres_refine(beat_b200_ctx *c, int R, double *x_dev, const double *b_dev, int restart,
                       int max_iters, double rtol);
+
+// adjoint.cu
+void apply_admittance_lhs(beat_b200_ctx *c, int precision);  // A += B diag(a) P
+// q_eff = q - a (P p) (F x R, FP64 column-major); a copy of q when no admittance is set
+void effective_neumann(beat_b200_ctx *c, int R, const double *p_dev, const double *q_dev, double *q_eff);
+void lu_solve_adjoint(beat_b200_ctx *c, int R, const double *in, double *out);  // out = A^-H in (stored factors)
+void adjoint(beat_b200_ctx *c, double k, int M, const double *dirs_host, int R, const double *p_dev,
+             const double *g_dev, double *w_dev, double *ga_dev, const beat_b200_opts &o, IrResult *ir);
+// gmres.cu: Y (cols x R) += alpha M^H X (X: rows x R); M complex row-major rows x cols
+template <typename T>
+void tall_gemm_h(cudaStream_t st, int sm_count, const Cx<T> *M, int64_t ld, int rows, int cols, const double *X,
+                 double *Y, int R, double alpha);
+IrResult gmres_refine_adjoint(beat_b200_ctx *c, int R, double *x_dev, const double *b_dev, int restart,
+                              int max_iters, double rtol);
 
 // field.cu
 void farfield(beat_b200_ctx *c, double k, int M, const double *dirs_host, int R, const double *p_dev,

@@ -187,6 +187,29 @@ int32_t beat_b200_sweep_device(beat_b200_ctx *ctx, int32_t nfreq, const double *
                                const beat_b200_opts *opts, void *d_p, int32_t M,
                                const double *dirs, void *d_ff, beat_b200_diag *diags);
 
+/* Admittance boundary condition (row a19 of the path; the reference's
+ * exterior solve has none, its admittance is a coupled-FEM wall model,
+ * BeatEngineCoupled.jl:594-623).  With coefficients a (F complex, one per
+ * face) every later solve on this context uses q = q0 - a (P p), where P is
+ * the face average of the P1 pressure:  (A + B diag(a) P) p = B q0, and the
+ * field evaluators apply the same q.  For a normal-velocity admittance Y
+ * (v = v0 - Y p, exp(-i omega t)) pass a = neumann_scale * Y.  a = NULL
+ * clears it (the reference's solve). */
+int32_t beat_b200_set_admittance(beat_b200_ctx *ctx, const double *a);
+
+/* Adjoint gradients of a real far-field functional J after a solve on this
+ * context with the same k_signed (row a19; no reference counterpart):
+ * g = dJ/d conj(p_inf) at the M directions (M x R), p the solve's pressures
+ * (N x R).  Returns w_out = dJ/d conj(q0) (F x R: the gradient with respect
+ * to the Neumann data; dJ = 2 Re sum conj(w) dq0) and, if ga_out is not NULL,
+ * ga_out = dJ/d conj(a) (F).  The conjugate-transposed system uses the
+ * stored factors (FP64 form) or the FP32 factors plus FP64 GMRES refinement
+ * on the stored operator (mixed form, opts' tolerances).  Gradients with
+ * respect to the vertices are not provided. */
+int32_t beat_b200_adjoint(beat_b200_ctx *ctx, double k_signed, int32_t M, const double *dirs,
+                          int32_t R, const double *p, const double *g, const beat_b200_opts *opts,
+                          double *w_out, double *ga_out);
+
 /* The CUDA stream (cudaStream_t) every kernel of this context is launched
  * on, so a caller can order its own work or record timing events on it.
  * Entry points return only after their work on it has completed. */
