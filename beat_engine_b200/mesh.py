@@ -228,3 +228,74 @@ def equator_meridian_directions(n_equator: int = 360, n_meridian: int = 181) -> 
     th = np.linspace(0.0, math.pi, n_meridian)
     me = np.stack([np.sin(th), np.zeros(n_meridian), np.cos(th)], axis=1)
     return np.concatenate([eq, me], axis=0)
+
+
+def uv_sphere_patch(radius: float, n_theta: int, n_phi: int, phi0: float, phi1: float,
+                    centre=(0.0, 0.0, 0.0), tag: int = 1) -> BoundaryMesh:
+    """Latitude-longitude patch of a sphere: polar angle 0..pi in n_theta
+    bands, azimuth phi0..phi1 in n_phi bands (both poles included, outward
+    normals).  With phi in [-pi/2, pi/2] it is the x >= 0 half; in [0, pi/2]
+    the x, y >= 0 quarter; the boundary meridians lie exactly on the planes."""
+    c = np.asarray(centre, dtype=float)
+    verts = [c + (0.0, 0.0, radius)]
+    full = abs((phi1 - phi0) - 2 * np.pi) < 1e-12
+    ncol = n_phi if full else n_phi + 1
+    for i in range(1, n_theta):
+        th = np.pi * i / n_theta
+        for j in range(ncol):
+            ph = phi0 + (phi1 - phi0) * j / n_phi
+            x, y = np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph)
+            # exact zeros on the planes x = 0 / y = 0 of the patch boundary
+            if abs(np.cos(ph)) < 1e-12:
+                x = 0.0
+            if abs(np.sin(ph)) < 1e-12:
+                y = 0.0
+            verts.append(c + radius * np.array([x, y, np.cos(th)]))
+    verts.append(c + (0.0, 0.0, -radius))
+    V = len(verts)
+
+    def ring(i, j):
+        return 1 + (i - 1) * ncol + (j % ncol if full else j)
+
+    faces = []
+    for j in range(n_phi):
+        faces.append((0, ring(1, j), ring(1, j + 1)))
+        faces.append((V - 1, ring(n_theta - 1, j + 1), ring(n_theta - 1, j)))
+    for i in range(1, n_theta - 1):
+        for j in range(n_phi):
+            a, b, d, e = ring(i, j), ring(i, j + 1), ring(i + 1, j), ring(i + 1, j + 1)
+            faces.append((a, d, e))
+            faces.append((a, e, b))
+    verts = np.array(verts)
+    faces = np.array(faces, dtype=np.int64)
+    # orient outward
+    for f in range(len(faces)):
+        p0, p1, p2 = verts[faces[f]]
+        n = np.cross(p1 - p0, p2 - p0)
+        if np.dot(n, (p0 + p1 + p2) / 3 - c) < 0:
+            faces[f] = faces[f][[0, 2, 1]]
+    return BoundaryMesh(verts, faces, np.full(len(faces), tag, dtype=np.int64))
+
+
+def mirror(mesh: BoundaryMesh, axis: int, tol: float = 1e-12) -> BoundaryMesh:
+    """The mesh together with its mirror image across the plane x[axis] = 0:
+    vertices on the plane are shared, mirrored faces are reversed so that the
+    normals stay outward.  Mirrored copies keep the order of the originals
+    (vertex v at V + v unless it lies on the plane; face f at F + f)."""
+    v = np.asarray(mesh.vertices, dtype=float)
+    V = v.shape[0]
+    on = np.abs(v[:, axis]) <= tol
+    idx = np.empty(V, dtype=np.int64)
+    extra = []
+    for i in range(V):
+        if on[i]:
+            idx[i] = i
+        else:
+            idx[i] = V + len(extra)
+            w = v[i].copy()
+            w[axis] = -w[axis]
+            extra.append(w)
+    verts = np.vstack([v, np.array(extra)]) if extra else v.copy()
+    f = np.asarray(mesh.faces)
+    mf = idx[f][:, [0, 2, 1]]
+    return BoundaryMesh(verts, np.vstack([f, mf]), np.concatenate([mesh.physical_tags, mesh.physical_tags]))

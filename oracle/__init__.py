@@ -49,6 +49,11 @@ def lib():
         L.bo_duffy_rule.argtypes = [c_int, c_int, dp, dp, dp]
         L.bo_singular_pairs.argtypes = [c_int, dp, c_int, ip, c_int, c_int, ip, ip, ip, ip, ip]
         L.bo_mesh_geometry.argtypes = [c_int, dp, c_int, ip, dp, dp, dp]
+        L.bo_symmetry_snap.argtypes = [c_int, dp, c_int]
+        L.bo_assemble_sym.argtypes = [c_int, dp, c_int, ip, c_int, c_int, c_double, c_double,
+                                      c_int, dp, dp, dp, c_int, c_int]
+        L.bo_field_sym.argtypes = [c_int, dp, c_int, ip, c_int, c_double, c_int, dp, c_int, dp, dp, dp, c_int,
+                                   c_int, c_int]
         _lib = L
     return _lib
 
@@ -171,3 +176,61 @@ def mesh_geometry(mesh):
     if st != 0:
         raise RuntimeError("invalid mesh")
     return n.reshape(F, 3), a, c.reshape(F, 3, 3)
+
+
+# symmetry modes (normalized_symmetry_mode, BeatEngineCore.jl:448-454)
+SYMMETRY_MODES = {"off": 0, "x": 1, "xy": 2, "ground": 3}
+
+
+def symmetry_snap(vertices, mode):
+    """Vertices snapped onto the active symmetry planes (a copy); raises when a
+    vertex lies outside the positive fundamental domain."""
+    v = np.ascontiguousarray(vertices, dtype=np.float64).copy()
+    st = lib().bo_symmetry_snap(v.shape[0], _dp(v), SYMMETRY_MODES[mode])
+    if st != 0:
+        raise ValueError(f"mesh is not in the fundamental domain of symmetry {mode}")
+    return v
+
+
+def assemble_sym(mesh, k_signed, eta, q, mode, quad_order=4, sing_order=4, threads=0):
+    """``(A, b)`` of the fundamental-domain mesh with symmetry images (mode
+    ``off``, ``x``, ``xy`` or ``ground``); the mesh's vertices are snapped first."""
+    v = symmetry_snap(mesh.vertices, mode)
+    f = np.ascontiguousarray(mesh.faces, dtype=np.int32)
+    N, F = mesh.num_vertices, mesh.num_faces
+    q = np.asarray(q, dtype=np.complex128)
+    if q.ndim == 1:
+        q = q[:, None]
+    R = q.shape[1]
+    qf = np.asfortranarray(q)
+    A = np.zeros((N, N), dtype=np.complex128, order="F")
+    b = np.zeros((N, max(R, 1)), dtype=np.complex128, order="F")
+    st = lib().bo_assemble_sym(N, _dp(v), F, _ip(f), quad_order, sing_order, float(k_signed), float(eta), R,
+                               qf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                               A.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                               b.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), threads, SYMMETRY_MODES[mode])
+    if st != 0:
+        raise RuntimeError(f"oracle symmetric assembly failed with status {st}")
+    return A, b[:, :R]
+
+
+def field_sym(mesh, k_signed, pts, p, q, mode, far=False, quad_order=4, threads=0):
+    """Field (or far field) of the fundamental-domain solution with its images."""
+    v = symmetry_snap(mesh.vertices, mode)
+    f = np.ascontiguousarray(mesh.faces, dtype=np.int32)
+    pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+    p = np.asarray(p, dtype=np.complex128)
+    q = np.asarray(q, dtype=np.complex128)
+    if p.ndim == 1:
+        p, q = p[:, None], q[:, None]
+    R, M = p.shape[1], pts.shape[0]
+    pf, qf = np.asfortranarray(p), np.asfortranarray(q)
+    out = np.zeros((M, R), dtype=np.complex128, order="F")
+    st = lib().bo_field_sym(mesh.num_vertices, _dp(v), mesh.num_faces, _ip(f), quad_order, float(k_signed), M,
+                            _dp(pts), R, pf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                            qf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                            out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), threads, SYMMETRY_MODES[mode],
+                            1 if far else 0)
+    if st != 0:
+        raise RuntimeError(f"oracle field failed with status {st}")
+    return out

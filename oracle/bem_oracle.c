@@ -913,4 +913,254 @@ int bo_farfield(int V, const double *verts, int F, const int *faces, int quad_or
     return BO_OK;
 }
 
+/* ------------------------------------------------------------------------ */
+/* symmetry images (symmetry_transforms, BeatEngineCore.jl:463-482;          */
+/* reflect_point / reflect_normal / reflect_curl, :487-496; plane snapping   */
+/* and orbit weights, :504-582; image passes and image-singular deltas,      */
+/* BeatEngineCudaBurtonMiller.jl:475-493 and BeatEngineCudaSingular.jl:140-  */
+/* 278, 590-897).  Modes: 0 off, 1 x, 2 xy, 3 ground.                        */
+/* ------------------------------------------------------------------------ */
+typedef struct { double s[3]; double det; } bo_xf;
+
+static int sym_images(int mode, bo_xf *out)
+{
+    int n = 0;
+    if (mode == 1 || mode == 2) { out[n].s[0] = -1; out[n].s[1] = 1; out[n].s[2] = 1; out[n].det = -1; ++n; }
+    if (mode == 2) {
+        out[n].s[0] = 1; out[n].s[1] = -1; out[n].s[2] = 1; out[n].det = -1; ++n;
+        out[n].s[0] = -1; out[n].s[1] = -1; out[n].s[2] = 1; out[n].det = 1; ++n;
+    }
+    if (mode == 3) { out[n].s[0] = 1; out[n].s[1] = -1; out[n].s[2] = 1; out[n].det = -1; ++n; }
+    return n;
+}
+
+/* symmetry_plane_tolerance: max(1e-9, 1e-6 x bounding-box diagonal) */
+static double sym_plane_tol(int V, const double *verts)
+{
+    double lo[3] = {verts[0], verts[1], verts[2]}, hi[3] = {verts[0], verts[1], verts[2]};
+    for (int v = 1; v < V; ++v)
+        for (int c = 0; c < 3; ++c) {
+            if (verts[3 * v + c] < lo[c]) lo[c] = verts[3 * v + c];
+            if (verts[3 * v + c] > hi[c]) hi[c] = verts[3 * v + c];
+        }
+    double d = sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) + (hi[2] - lo[2]) * (hi[2] - lo[2]));
+    double t = d * 1e-6;
+    return t > 1e-9 ? t : 1e-9;
+}
+
+static inline v3 reflect(const bo_xf *x, v3 p) { v3 r = {x->s[0] * p.x, x->s[1] * p.y, x->s[2] * p.z}; return r; }
+
+/* regular pair with the trial element reflected by x (all pairs, touching or not) */
+static void regular_pair_x(const bo_mesh *m, int t, int s, const bo_xf *x, double k, double eta, double *lhs, double *rhs)
+{
+    v3 nt = v3make(m->normals + 3 * t), ns = reflect(x, v3make(m->normals + 3 * s));
+    double jac = 4.0 * m->areas[t] * m->areas[s];
+    double k2n_im = eta * (k * k * v3dot(nt, ns));
+    double curl[2] = {0.0, 0.0}, cs[9];
+    for (int a = 0; a < 3; ++a)
+        for (int c = 0; c < 3; ++c) cs[3 * a + c] = x->det * x->s[c] * m->curls[9 * s + 3 * a + c];
+    memset(lhs, 0, sizeof(double) * 18); memset(rhs, 0, sizeof(double) * 6);
+    int Q = m->Q;
+    for (int a = 0; a < Q; ++a) {
+        v3 xp = v3make(m->qpts + 3 * (t * Q + a));
+        for (int b = 0; b < Q; ++b) {
+            v3 y = reflect(x, v3make(m->qpts + 3 * (s * Q + b)));
+            bm_point(xp, y, m->basis + 3 * a, m->basis + 3 * b, m->rw[a] * m->rw[b] * jac, nt, ns, k, eta, k2n_im,
+                     lhs, rhs, curl);
+        }
+    }
+    bm_finish(m->curls + 9 * t, cs, eta, curl, lhs);
+}
+
+/* geometric_adjacency_info, BeatEngineCore.jl:624-650, on vertex positions */
+static int geometric_adjacency(const v3 *tv, const v3 *sv, double tol, int *ta, int *tb, int *sa, int *sb)
+{
+    int sh_a[3], sh_b[3], n = 0;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            if (v3norm(v3sub(tv[i], sv[j])) <= tol && n < 3) { sh_a[n] = i + 1; sh_b[n] = j + 1; ++n; }
+    *ta = *tb = *sa = *sb = 0;
+    if (n == 3) return BO_COINCIDENT;
+    if (n == 2) {
+        if (sh_b[1] < sh_b[0]) {
+            int t = sh_a[0]; sh_a[0] = sh_a[1]; sh_a[1] = t;
+            t = sh_b[0]; sh_b[0] = sh_b[1]; sh_b[1] = t;
+        }
+        *ta = sh_a[0]; *tb = sh_a[1]; *sa = sh_b[0]; *sb = sh_b[1];
+        return BO_EDGE;
+    }
+    if (n == 1) { *ta = sh_a[0]; *sa = sh_b[0]; return BO_VERTEX; }
+    return 0;
+}
+
+/* image-singular delta of a touching (test, reflected trial) pair: the
+ * remapped Duffy integral minus the regular-rule integral the image pass
+ * already added (_cuda_image_singular_delta_blocks_kernel!) */
+static void image_delta_pair(const bo_mesh *m, int t, int s, const bo_xf *x, int kind, int ta, int tb, int sa, int sb,
+                             int sing_order, double k, double eta, double *lhs, double *rhs)
+{
+    int nb = sing_order * sing_order * sing_order * sing_order * 6;
+    double *bt = malloc(sizeof(double) * 2 * nb), *bs = malloc(sizeof(double) * 2 * nb), *bw = malloc(sizeof(double) * nb);
+    int nq = bo_duffy_rule(sing_order, kind, bt, bs, bw);
+    const int *ft = m->faces + 3 * t, *fs = m->faces + 3 * s;
+    v3 tv[3], sv[3];
+    for (int a = 0; a < 3; ++a) { tv[a] = v3make(m->verts + 3 * ft[a]); sv[a] = reflect(x, v3make(m->verts + 3 * fs[a])); }
+    v3 nt = v3make(m->normals + 3 * t), ns = reflect(x, v3make(m->normals + 3 * s));
+    double jac = (2.0 * m->areas[t]) * (2.0 * m->areas[s]);
+    double k2n_im = eta * (k * k * v3dot(nt, ns));
+    double curl[2] = {0.0, 0.0}, cs[9];
+    for (int a = 0; a < 3; ++a)
+        for (int c = 0; c < 3; ++c) cs[3 * a + c] = x->det * x->s[c] * m->curls[9 * s + 3 * a + c];
+    memset(lhs, 0, sizeof(double) * 18); memset(rhs, 0, sizeof(double) * 6);
+    for (int q = 0; q < nq; ++q) {
+        double pt[2], ps[2];
+        remap_point(kind, ta, tb, bt + 2 * q, pt);
+        remap_point(kind, sa, sb, bs + 2 * q, ps);
+        double b1[3] = {1.0 - pt[0] - pt[1], pt[0], pt[1]}, b2[3] = {1.0 - ps[0] - ps[1], ps[0], ps[1]};
+        v3 xp = {b1[0] * tv[0].x + b1[1] * tv[1].x + b1[2] * tv[2].x, b1[0] * tv[0].y + b1[1] * tv[1].y + b1[2] * tv[2].y,
+                 b1[0] * tv[0].z + b1[1] * tv[1].z + b1[2] * tv[2].z};
+        v3 y = {b2[0] * sv[0].x + b2[1] * sv[1].x + b2[2] * sv[2].x, b2[0] * sv[0].y + b2[1] * sv[1].y + b2[2] * sv[2].y,
+                b2[0] * sv[0].z + b2[1] * sv[1].z + b2[2] * sv[2].z};
+        bm_point(xp, y, b1, b2, bw[q] * jac, nt, ns, k, eta, k2n_im, lhs, rhs, curl);
+    }
+    bm_finish(m->curls + 9 * t, cs, eta, curl, lhs);
+    double rl[18], rr[6];
+    regular_pair_x(m, t, s, x, k, eta, rl, rr);
+    for (int i = 0; i < 18; ++i) lhs[i] -= rl[i];
+    for (int i = 0; i < 6; ++i) rhs[i] -= rr[i];
+    free(bt); free(bs); free(bw);
+}
+
+/* Snap vertices within the plane tolerance onto the active symmetry planes
+ * (snap_symmetry_plane_vertices); returns BO_EINVAL when a vertex lies on the
+ * negative side (validate_symmetry_fundamental_domain!). */
+int bo_symmetry_snap(int V, double *verts, int mode)
+{
+    double tol = sym_plane_tol(V, verts);
+    int axes[2], na = 0;
+    if (mode == 1 || mode == 2) axes[na++] = 0;
+    if (mode == 2) axes[na++] = 1;
+    for (int v = 0; v < V; ++v)
+        for (int i = 0; i < na; ++i) {
+            double *c = verts + 3 * v + axes[i];
+            if (*c < -tol) return BO_EINVAL;
+            if (fabs(*c) <= tol) *c = 0.0;
+        }
+    return BO_OK;
+}
+
+/* The system with symmetry images: the one-copy assembly, one reflected-trial
+ * pass per image, the image-singular deltas, then the orbit row weights
+ * (2 per active plane a row's vertex lies on; p1_symmetry_orbit_weights).
+ * verts must already be snapped (bo_symmetry_snap). */
+int bo_assemble_sym(int V, const double *verts, int F, const int *faces, int quad_order, int sing_order, double k,
+                    double eta, int R, const double *q, double *A, double *b, int nthreads, int mode)
+{
+    int st = bo_assemble_range(V, verts, F, faces, quad_order, sing_order, k, eta, R, q, A, b, nthreads, 0, 0, F);
+    if (st != BO_OK || mode == 0) return st;
+    bo_mesh m;
+    st = mesh_init(&m, V, verts, F, faces, quad_order);
+    if (st != BO_OK) { mesh_free(&m); return st; }
+    bo_xf xf[4];
+    int nimg = sym_images(mode, xf);
+    int *order = malloc(sizeof(int) * F), *start = malloc(sizeof(int) * 65);
+    int ncol = colour_groups(&m, order, start);
+    const double tol_pair = 1e-8;
+    for (int ix = 0; ix < nimg; ++ix) {
+        for (int c = 0; c < ncol; ++c) {
+#pragma omp parallel for schedule(dynamic, 1)
+            for (int i = start[c]; i < start[c + 1]; ++i) {
+                int t = order[i];
+                double lhs[18], rhs[6];
+                v3 tv[3];
+                for (int a = 0; a < 3; ++a) tv[a] = v3make(verts + 3 * faces[3 * t + a]);
+                for (int s = 0; s < F; ++s) {
+                    regular_pair_x(&m, t, s, &xf[ix], k, eta, lhs, rhs);
+                    scatter(&m, t, s, lhs, rhs, R, q, A, b);
+                    v3 sv[3];
+                    for (int a = 0; a < 3; ++a) sv[a] = reflect(&xf[ix], v3make(verts + 3 * faces[3 * s + a]));
+                    int ta, tb, sa, sb;
+                    int kind = geometric_adjacency(tv, sv, tol_pair, &ta, &tb, &sa, &sb);
+                    if (kind == 0) continue;
+                    image_delta_pair(&m, t, s, &xf[ix], kind, ta, tb, sa, sb, sing_order, k, eta, lhs, rhs);
+                    scatter(&m, t, s, lhs, rhs, R, q, A, b);
+                }
+            }
+        }
+    }
+    free(order); free(start);
+    double tol = sym_plane_tol(V, verts);
+    int N = V;
+    for (int v = 0; v < V; ++v) {
+        double w = 1.0;
+        if ((mode == 1 || mode == 2) && fabs(verts[3 * v]) <= tol) w *= 2.0;
+        if (mode == 2 && fabs(verts[3 * v + 1]) <= tol) w *= 2.0;
+        if (w == 1.0) continue;
+        for (int c = 0; c < N; ++c) { A[2 * (v + (size_t)c * N)] *= w; A[2 * (v + (size_t)c * N) + 1] *= w; }
+        for (int d = 0; d < R; ++d) { b[2 * (v + (size_t)d * N)] *= w; b[2 * (v + (size_t)d * N) + 1] *= w; }
+    }
+    mesh_free(&m);
+    return BO_OK;
+}
+
+/* Field and far field with the image sources (reflected positions and
+ * normals, the same p and q). */
+int bo_field_sym(int V, const double *verts, int F, const int *faces, int quad_order, double k, int M,
+                 const double *points, int R, const double *p, const double *q, double *out, int nthreads, int mode,
+                 int far)
+{
+    bo_mesh m;
+    int st = mesh_init(&m, V, verts, F, faces, quad_order);
+    if (st != BO_OK) { mesh_free(&m); return st; }
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    bo_xf xf[5];
+    xf[0].s[0] = xf[0].s[1] = xf[0].s[2] = 1.0; xf[0].det = 1.0;
+    int nx = 1 + sym_images(mode, xf + 1);
+    int N = V, Q = m.Q;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int i = 0; i < M; ++i) {
+        v3 xo = v3make(points + 3 * i);
+        if (far) { double nn = v3norm(xo); xo.x /= nn; xo.y /= nn; xo.z /= nn; }
+        for (int d = 0; d < R; ++d) { out[2 * (i + (size_t)d * M)] = 0.0; out[2 * (i + (size_t)d * M) + 1] = 0.0; }
+        for (int ix = 0; ix < nx; ++ix)
+            for (int f = 0; f < F; ++f) {
+                const int *fc = faces + 3 * f;
+                v3 n = reflect(&xf[ix], v3make(m.normals + 3 * f));
+                double jac = 2.0 * m.areas[f];
+                for (int qq = 0; qq < Q; ++qq) {
+                    v3 y = reflect(&xf[ix], v3make(m.qpts + 3 * (f * Q + qq)));
+                    double g_re, g_im, dl_re, dl_im;
+                    if (far) {
+                        double ph_ = -k * v3dot(xo, y);
+                        g_re = cos(ph_) / (4.0 * BO_PI); g_im = sin(ph_) / (4.0 * BO_PI);
+                        double dnrm = v3dot(xo, n);
+                        dl_re = g_im * k * dnrm; dl_im = -g_re * k * dnrm;
+                    } else {
+                        v3 r = v3sub(y, xo);
+                        double radius = v3norm(r);
+                        if (radius == 0.0) continue;
+                        double phase = k * radius, gsc = 1.0 / (4.0 * BO_PI * radius);
+                        g_re = cos(phase) * gsc; g_im = sin(phase) * gsc;
+                        double proj = v3dot(r, n) / radius, fr = -1.0 / radius, fi = k;
+                        dl_re = (g_re * fr - g_im * fi) * proj; dl_im = (g_re * fi + g_im * fr) * proj;
+                    }
+                    double w = m.rw[qq] * jac;
+                    const double *ph = m.basis + 3 * qq;
+                    for (int d = 0; d < R; ++d) {
+                        const double *pd = p + 2 * (size_t)d * N;
+                        double ps_re = (ph[0] * pd[2 * fc[0]] + ph[1] * pd[2 * fc[1]] + ph[2] * pd[2 * fc[2]]) * w;
+                        double ps_im = (ph[0] * pd[2 * fc[0] + 1] + ph[1] * pd[2 * fc[1] + 1] + ph[2] * pd[2 * fc[2] + 1]) * w;
+                        double qs_re = q[2 * (f + (size_t)d * F)] * w, qs_im = q[2 * (f + (size_t)d * F) + 1] * w;
+                        out[2 * (i + (size_t)d * M)] += dl_re * ps_re - dl_im * ps_im - (g_re * qs_re - g_im * qs_im);
+                        out[2 * (i + (size_t)d * M) + 1] += dl_re * ps_im + dl_im * ps_re - (g_re * qs_im + g_im * qs_re);
+                    }
+                }
+            }
+    }
+    mesh_free(&m);
+    return BO_OK;
+}
+
 int bo_version(void) { return 1; }
