@@ -26,7 +26,10 @@ EXPORTS = (
     "beat_b200_field", "beat_b200_farfield", "beat_b200_farfield_device", "beat_b200_assemble",
     "beat_b200_release_workspace", "beat_b200_device_bytes", "beat_b200_stream", "beat_b200_resolve_noalloc",
     "beat_b200_sweep", "beat_b200_sweep_device", "beat_b200_set_admittance", "beat_b200_adjoint",
+    "beat_b200_set_symmetry",
 )
+
+SYMMETRY_MODES = {"off": 0, "x": 1, "xy": 2, "ground": 3}
 
 
 class Opts(ctypes.Structure):
@@ -106,6 +109,8 @@ def load(path: str = LIB_PATH):
     L.beat_b200_sweep_device.argtypes = [vp, i32, dp, dp, i32, vp, ctypes.POINTER(Opts), vp, i32, dp, vp,
                                          ctypes.POINTER(Diag)]
     L.beat_b200_sweep_device.restype = i32
+    L.beat_b200_set_symmetry.argtypes = [vp, i32]
+    L.beat_b200_set_symmetry.restype = i32
     L.beat_b200_set_admittance.argtypes = [vp, dp]
     L.beat_b200_set_admittance.restype = i32
     L.beat_b200_adjoint.argtypes = [vp, f64, i32, dp, i32, dp, dp, ctypes.POINTER(Opts), dp, dp]
@@ -273,6 +278,11 @@ class Context:
             ctypes.byref(opts) if opts is not None else None, ctypes.c_void_p(d_p_ptr), M,
             _dp(dd) if dd is not None else None, ctypes.c_void_p(d_ff_ptr), diags))
         return [diags[i].as_dict() for i in range(nf)]
+
+    def set_symmetry(self, mode):
+        """Symmetry images: "off", "x", "xy" or "ground" (or 0..3)."""
+        m = SYMMETRY_MODES[mode] if isinstance(mode, str) else int(mode)
+        self._check(self.lib.beat_b200_set_symmetry(self.handle, m))
 
     def set_admittance(self, a=None):
         """Per-face admittance coefficients a (F complex): later solves use

@@ -158,6 +158,7 @@ beat_b200_ctx *sweep_lane(beat_b200_ctx *c, int i) {
         const int32_t st = beat_b200_create(c->device, &l);
         BB_REQUIRE(st == BEAT_B200_OK, st, "sweep: could not create a solve lane");
         c->lanes.push_back(l);
+        l->sym_mode = c->sym_mode;
         std::vector<int32_t> faces1(c->faces.size());
         for (size_t j = 0; j < faces1.size(); ++j) faces1[j] = c->faces[j] + 1;
         BB_CUDA(cudaSetDevice(c->device));
@@ -272,7 +273,8 @@ int32_t beat_b200_destroy(beat_b200_ctx *c) {
     for (DevBuf *b : {&c->pos_face, &c->pos_qpts64, &c->pos_qpts32, &c->pos_normal64, &c->pos_normal32,
                       &c->pos_curl64, &c->pos_curl32, &c->pos_area64, &c->pos_area32, &c->pos_gvert, &c->d_verts,
                       &c->d_faces, &c->d_normals, &c->d_areas, &c->d_curls, &c->d_qpts, &c->vf_start, &c->vf_face,
-                      &c->adm, &c->sp_test, &c->sp_trial,
+                      &c->adm, &c->ip_test, &c->ip_trial, &c->ip_rule, &c->ip_img, &c->ip_jac, &c->ip_nn,
+                      &c->rw_vert, &c->rw_weight, &c->sp_test, &c->sp_trial,
                       &c->sp_rule, &c->sp_jac, &c->sp_nn, &c->rule_start, &c->rule_data, &c->status, &c->barrier})
         b->free_();
     for (Tiling *t : {&c->test_tiles, &c->trial_tiles, &c->sym_tiles}) {
@@ -473,6 +475,40 @@ int32_t beat_b200_sweep(beat_b200_ctx *c, int32_t nfreq, const double *k_signed,
                 BB_CUDA(cudaMemcpyAsync(ff_out + f * fs, dff, fs * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
             BB_CUDA(cudaStreamSynchronize(l->stream));
         });
+    });
+}
+
+int32_t beat_b200_set_symmetry(beat_b200_ctx *c, int32_t mode) {
+    return guarded(c, [&] {
+        BB_REQUIRE(mode >= 0 && mode <= 3, BEAT_B200_INVALID_ARG, "symmetry mode must be 0 (off), 1 (x), 2 (xy) or 3 (ground)");
+        BB_CUDA(cudaStreamSynchronize(c->stream));
+        for (beat_b200_ctx *l : c->lanes) beat_b200_destroy(l);  // lanes hold the previous set-up
+        c->lanes.clear();
+        const int old = c->sym_mode;
+        c->sym_mode = mode;
+        if (c->F > 0 && mode != old) {
+            const bool adm = c->adm_set;
+            DevBuf keep;
+            if (adm) {  // set_mesh clears the admittance: carry it over
+                keep.alloc(c->adm.bytes);
+                BB_CUDA(cudaMemcpy(keep.p, c->adm.p, c->adm.bytes, cudaMemcpyDeviceToDevice));
+            }
+            try {
+                set_mesh(c, c->V, c->in_verts.data(), c->F, c->in_faces.data(), c->quad_order, c->sing_order);
+            } catch (...) {
+                c->sym_mode = old;
+                keep.free_();
+                set_mesh(c, c->V, c->in_verts.data(), c->F, c->in_faces.data(), c->quad_order, c->sing_order);
+                throw;
+            }
+            if (adm) {
+                c->adm.alloc(keep.bytes);
+                BB_CUDA(cudaMemcpy(c->adm.p, keep.p, keep.bytes, cudaMemcpyDeviceToDevice));
+                c->adm_set = true;
+                keep.free_();
+            }
+        }
+        c->ws.lu_valid = 0;
     });
 }
 

@@ -134,10 +134,15 @@ __global__ void admittance_gradient_kernel(const int *faces, int F, int N, int R
 // ---------------------------------------------------------------------------
 constexpr int FA_RC = 16, FA_CHUNK = 64, FA_THREADS = 128;
 
+struct AdjImages {
+    int n;           // the mesh itself, then its symmetry images
+    double s[4][3];  // signs per copy
+};
+
 __global__ void __launch_bounds__(FA_THREADS) farfield_adjoint_kernel(
     const double *qpts, const double *normals, const double *areas, const int *faces, int F, int Q,
     const double *rule_w3, int N, const double *dirs, int M, const double2 *g, int R, int r0, double k, double2 *yp,
-    double2 *wq) {
+    double2 *wq, AdjImages images) {
     __shared__ double sd[FA_CHUNK][3];
     __shared__ double2 sg[FA_RC][FA_CHUNK];
     const int S = F * Q;
@@ -175,15 +180,19 @@ __global__ void __launch_bounds__(FA_THREADS) farfield_adjoint_kernel(
         }
         __syncthreads();
         if (s >= S) continue;
-        for (int j = 0; j < mn; ++j) {
+        for (int j = 0; j < mn * images.n; ++j) {
+            // direction j % mn against copy j / mn of the source (reflected y and n)
+            const int jm = j % mn, ix = j / mn;
+            const double d0 = sd[jm][0] * images.s[ix][0], d1 = sd[jm][1] * images.s[ix][1],
+                         d2 = sd[jm][2] * images.s[ix][2];  // d.(S y) = (S d).y
             double sn_, cs_;
-            sincos_cw(-k * (sd[j][0] * y0 + sd[j][1] * y1 + sd[j][2] * y2), &sn_, &cs_);
+            sincos_cw(-k * (d0 * y0 + d1 * y1 + d2 * y2), &sn_, &cs_);
             const double er = cs_ * inv4pi, ei = sn_ * inv4pi;  // E
-            const double dn = sd[j][0] * n0 + sd[j][1] * n1 + sd[j][2] * n2;
+            const double dn = d0 * n0 + d1 * n1 + d2 * n2;
             const double dr = ei * k * dn, di = -er * k * dn;  // D = E (-ik dn)
 #pragma unroll
             for (int r = 0; r < FA_RC; ++r) {
-                const double2 gv = sg[r][j];
+                const double2 gv = sg[r][jm];
                 pr[r] += dr * gv.x + di * gv.y;  // conj(D) g
                 pi[r] += dr * gv.y - di * gv.x;
                 qr[r] += er * gv.x + ei * gv.y;  // conj(E) g
@@ -386,11 +395,16 @@ void adjoint(beat_b200_ctx *c, double k, int M, const double *dirs_host, int R, 
     BB_CUDA(cudaMemsetAsync(y, 0, sizeof(double2) * (size_t)n * R, c->stream));
     BB_CUDA(cudaMemsetAsync(w_dev, 0, sizeof(double2) * (size_t)F * R, c->stream));
     const int S = F * Q;
+    AdjImages images;
+    images.n = 1 + c->nimg;
+    for (int i = 0; i < 3; ++i) images.s[0][i] = 1.0;
+    for (int ix = 0; ix < c->nimg; ++ix)
+        for (int i = 0; i < 3; ++i) images.s[1 + ix][i] = c->img_sign[ix][i];
     for (int r0 = 0; r0 < R; r0 += FA_RC)
         farfield_adjoint_kernel<<<(S + FA_THREADS - 1) / FA_THREADS, FA_THREADS, 0, c->stream>>>(
             c->d_qpts.as<double>(), c->d_normals.as<double>(), c->d_areas.as<double>(), c->d_faces.as<int>(), F, Q,
             d_rw, n, d_dirs, M, reinterpret_cast<const double2 *>(g_dev), R, r0, k, y,
-            reinterpret_cast<double2 *>(w_dev));
+            reinterpret_cast<double2 *>(w_dev), images);
     BB_CUDA(cudaGetLastError());
     // 2. y -= P^T diag(conj a) Fq^H g
     if (c->adm_set) {

@@ -108,6 +108,11 @@ template <typename T> struct RegArgs {
     int64_t ld;         // row stride of A (complex entries)
     int F;
     T k, eta, k2;
+    // image pass: trial elements reflected by these signs (curls also by det),
+    // touching pairs kept (their Duffy delta comes from image_delta_kernel)
+    int image = 0;
+    T xs[3] = {T(1), T(1), T(1)};
+    T xdet = T(1);
 };
 
 // Element-pair kernel.  grid = (trial tiles, test tiles), 256 threads.
@@ -150,17 +155,17 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
     for (int i = tid; i < nt; i += REG_THREADS) ta[i] = g.area[t0 + i];
     for (int i = tid; i < ns * Q * 3; i += REG_THREADS) {
         int s = i / (Q * 3), j = i % (Q * 3);
-        sq[j * TS + s] = g.qpts[(size_t)s0 * Q * 3 + i];
+        sq[j * TS + s] = g.xs[j % 3] * g.qpts[(size_t)s0 * Q * 3 + i];
     }
     for (int i = tid; i < ns * 3; i += REG_THREADS) {
         int s = i / 3, j = i % 3;
-        sn[j * TS + s] = g.normal[(size_t)s0 * 3 + i];
+        sn[j * TS + s] = g.xs[j] * g.normal[(size_t)s0 * 3 + i];
         sgv[j * TS + s] = g.gvert[(size_t)s0 * 3 + i];
         slv[j * TS + s] = g.s_local[(size_t)s0 * 3 + i];
     }
     for (int i = tid; i < ns * 9; i += REG_THREADS) {
         int s = i / 9, j = i % 9;
-        sc[j * TS + s] = g.curl[(size_t)s0 * 9 + i];
+        sc[j * TS + s] = g.xdet * g.xs[j % 3] * g.curl[(size_t)s0 * 9 + i];
     }
     for (int i = tid; i < ns; i += REG_THREADS) sa[i] = g.area[s0 + i];
     __syncthreads();
@@ -179,8 +184,8 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
         if (sl >= ns) continue;
         const int ga = tgv[3 * tl], gb = tgv[3 * tl + 1], gc = tgv[3 * tl + 2];
         const int ha = sgv[sl], hb = sgv[TS + sl], hc = sgv[2 * TS + sl];
-        if (ga == ha || ga == hb || ga == hc || gb == ha || gb == hb || gb == hc || gc == ha || gc == hb ||
-            gc == hc)
+        if (!g.image && (ga == ha || ga == hb || ga == hc || gb == ha || gb == hb || gb == hc || gc == ha ||
+                         gc == hb || gc == hc))
             continue;  // touching pair: the Duffy kernel integrates it
         const T ntx = tn[3 * tl], nty = tn[3 * tl + 1], ntz = tn[3 * tl + 2];
         const T nsx = sn[sl], nsy = sn[TS + sl], nsz = sn[2 * TS + sl];
@@ -354,19 +359,21 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
     }
     for (int i = tid; i < nI * 9; i += REG_THREADS) xc[i] = g.curl[(size_t)t0 * 9 + i];
     for (int i = tid; i < nI; i += REG_THREADS) xa[i] = g.area[t0 + i];
+    // (an image pass reflects tile J: pairs (tau, S sigma) and (sigma, S tau)
+    // have the same distances, |x - Sy| = |Sx - y|, and swap dn_s / dn_t)
     for (int i = tid; i < nJ * Q * 3; i += REG_THREADS) {
         const int s = i / (Q * 3), j = i % (Q * 3);
-        yq[j * SYM_F + s] = g.qpts[(size_t)s0 * Q * 3 + i];
+        yq[j * SYM_F + s] = g.xs[j % 3] * g.qpts[(size_t)s0 * Q * 3 + i];
     }
     for (int i = tid; i < nJ * 3; i += REG_THREADS) {
         const int s = i / 3, j = i % 3;
-        yn[j * SYM_F + s] = g.normal[(size_t)s0 * 3 + i];
+        yn[j * SYM_F + s] = g.xs[j] * g.normal[(size_t)s0 * 3 + i];
         ygv[j * SYM_F + s] = g.gvert[(size_t)s0 * 3 + i];
         ylv[j * SYM_F + s] = g.t_local[(size_t)s0 * 3 + i];
     }
     for (int i = tid; i < nJ * 9; i += REG_THREADS) {
         const int s = i / 9, j = i % 9;
-        yc[j * SYM_F + s] = g.curl[(size_t)s0 * 9 + i];
+        yc[j * SYM_F + s] = g.xdet * g.xs[j % 3] * g.curl[(size_t)s0 * 9 + i];
     }
     for (int i = tid; i < nJ; i += REG_THREADS) ya[i] = g.area[s0 + i];
     __syncthreads();
@@ -380,11 +387,13 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
     const T inv4pi = T(0.07957747154594767);  // 1 / (4 pi)
     for (int p = tid; p < SYM_F * SYM_F; p += REG_THREADS) {
         const int ti = p / SYM_F, sj = p % SYM_F;  // a warp: one tau, every sigma
-        if (ti >= nI || sj >= nJ || (diag && sj <= ti)) continue;
+        // (an image pass keeps tau == sigma: the element and its own image,
+        // whose two orders coincide and are taken at half weight)
+        if (ti >= nI || sj >= nJ || (diag && (g.image ? sj < ti : sj <= ti))) continue;
         const int ga = xgv[3 * ti], gb = xgv[3 * ti + 1], gc = xgv[3 * ti + 2];
         const int ha = ygv[sj], hb = ygv[SYM_F + sj], hc = ygv[2 * SYM_F + sj];
-        if (ga == ha || ga == hb || ga == hc || gb == ha || gb == hb || gb == hc || gc == ha || gc == hb ||
-            gc == hc)
+        if (!g.image && (ga == ha || ga == hb || ga == hc || gb == ha || gb == hb || gb == hc || gc == ha ||
+                         gc == hb || gc == hc))
             continue;  // touching pair: the Duffy kernel integrates both orders
         const T ntx = xn[3 * ti], nty = xn[3 * ti + 1], ntz = xn[3 * ti + 2];
         const T nsx = yn[sj], nsy = yn[SYM_F + sj], nsz = yn[2 * SYM_F + sj];
@@ -471,7 +480,7 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
         }
         // hypersingular curl term: eta * sum(g w) * curl_test . curl_trial (same sum for both orders)
         const T ccr = -eta * ci, cci = eta * cr;
-        const T jac = T(4) * xa[ti] * ya[sj];
+        const T jac = T(4) * xa[ti] * ya[sj] * ((g.image && diag && sj == ti) ? T(0.5) : T(1));
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             const int ra = xlv[3 * ti + a];      // vertex a of tau, tile I local
@@ -640,6 +649,166 @@ __global__ void __launch_bounds__(256) singular_pairs_kernel(SingArgs<T> g) {
 }
 
 // ---------------------------------------------------------------------------
+// touching image pairs (test t, trial s reflected by image x): the remapped
+// Duffy integral minus the regular-rule integral the image pass added
+// (_cuda_image_singular_delta_blocks_kernel!, BeatEngineCudaSingular.jl:590-897).
+// One warp per pair, FP64, lanes over the Duffy points, then over the Q x Q
+// regular points.
+// ---------------------------------------------------------------------------
+struct ImgXf {
+    double s[3][3];  // per image: signs
+    double det[3];
+};
+
+template <typename T> struct ImgArgs {
+    const int *test, *trial, *rule, *img;
+    const double *jac, *nn;
+    const int *rule_start;
+    const double *rule_data;  // 5 per point
+    const double *verts;
+    const int *faces;
+    const double *normals, *curls;
+    int Q, RI;
+    Cx<T> *A, *B;
+    int64_t ld;
+    int F;
+    int64_t npairs;
+    double k, eta;
+    ImgXf xf;
+};
+
+__device__ __forceinline__ void bm_point_d(const double *x, const double *y, const double *bt, const double *bs,
+                                           double w, const double *nt, const double *ns, double k, double eta,
+                                           double k2n, double sign, double *acc) {
+    const double rx = y[0] - x[0], ry = y[1] - x[1], rz = y[2] - x[2];
+    const double r2 = rx * rx + ry * ry + rz * rz;
+    if (r2 == 0.0) return;
+    const double rad = sqrt(r2), ir = 1.0 / rad;
+    double sn_, cs_;
+    sincos_cw(k * rad, &sn_, &cs_);
+    const double scl = sign * ir * (0.07957747154594767 * w);
+    const double gr = cs_ * scl, gi = sn_ * scl;
+    const double gsr = -gr * ir - gi * k, gsi = gr * k - gi * ir;
+    const double dns = (rx * ns[0] + ry * ns[1] + rz * ns[2]) * ir;
+    const double dnt = -(rx * nt[0] + ry * nt[1] + rz * nt[2]) * ir;
+    const double lr = -gsr * dns + k2n * gi, li = -gsi * dns - k2n * gr;
+    const double rr = -gr + eta * (gsi * dnt), ri = -gi - eta * (gsr * dnt);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const double bp = bt[a] * bs[b];
+            acc[2 * (3 * a + b)] += bp * lr;
+            acc[2 * (3 * a + b) + 1] += bp * li;
+        }
+        acc[18 + 2 * a] += bt[a] * rr;
+        acc[18 + 2 * a + 1] += bt[a] * ri;
+    }
+    acc[24] += gr;
+    acc[25] += gi;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) image_delta_kernel(ImgArgs<T> g) {
+    const int lane = threadIdx.x & 31;
+    const int64_t pair = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    if (pair >= g.npairs) return;
+    const int t = g.test[pair], s = g.trial[pair], r = g.rule[pair], ix = g.img[pair];
+    const double *sg = g.xf.s[ix];
+    const int *ft = g.faces + 3 * t, *fs = g.faces + 3 * s;
+    double tv[3][3], sv[3][3], nt[3], ns[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            tv[a][c] = g.verts[3 * ft[a] + c];
+            sv[a][c] = sg[c] * g.verts[3 * fs[a] + c];
+        }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        nt[c] = g.normals[3 * t + c];
+        ns[c] = sg[c] * g.normals[3 * s + c];
+    }
+    const double k = g.k, eta = g.eta;
+    const double k2n = eta * (k * k * g.nn[pair]);
+    double acc[26];
+#pragma unroll
+    for (int i = 0; i < 26; ++i) acc[i] = 0.0;
+    // + Duffy
+    for (int q = g.rule_start[r] + lane; q < g.rule_start[r + 1]; q += 32) {
+        const double *d = g.rule_data + 5 * (size_t)q;
+        const double bt[3] = {1.0 - d[0] - d[1], d[0], d[1]}, bs[3] = {1.0 - d[2] - d[3], d[2], d[3]};
+        double x[3], y[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            x[c] = bt[0] * tv[0][c] + bt[1] * tv[1][c] + bt[2] * tv[2][c];
+            y[c] = bs[0] * sv[0][c] + bs[1] * sv[1][c] + bs[2] * sv[2][c];
+        }
+        bm_point_d(x, y, bt, bs, d[4], nt, ns, k, eta, k2n, 1.0, acc);
+    }
+    // - regular rule
+    for (int pq = lane; pq < g.Q * g.Q; pq += 32) {
+        const int qt = pq / g.Q, qs = pq % g.Q;
+        const double bt[3] = {c_rb64[g.RI][qt][0], c_rb64[g.RI][qt][1], c_rb64[g.RI][qt][2]};
+        const double bs[3] = {c_rb64[g.RI][qs][0], c_rb64[g.RI][qs][1], c_rb64[g.RI][qs][2]};
+        double x[3], y[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            x[c] = bt[0] * tv[0][c] + bt[1] * tv[1][c] + bt[2] * tv[2][c];
+            y[c] = bs[0] * sv[0][c] + bs[1] * sv[1][c] + bs[2] * sv[2][c];
+        }
+        bm_point_d(x, y, bt, bs, c_rw64[g.RI][qt] * c_rw64[g.RI][qs], nt, ns, k, eta, k2n, -1.0, acc);
+    }
+#pragma unroll
+    for (int i = 0; i < 26; ++i) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
+    }
+    const double jac = g.jac[pair];
+    const double ccr = -eta * acc[25], cci = eta * acc[24];
+    const double cdet = g.xf.det[ix];
+    if (lane < 9) {
+        const int a = lane / 3, b = lane % 3;
+        const double *cta = g.curls + 9 * t + 3 * a, *csb = g.curls + 9 * s + 3 * b;
+        const double d = cdet * (cta[0] * sg[0] * csb[0] + cta[1] * sg[1] * csb[1] + cta[2] * sg[2] * csb[2]);
+        double vr = 0, vi = 0;
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+            if (i == lane) {
+                vr = acc[2 * i];
+                vi = acc[2 * i + 1];
+            }
+        red_add_cx(&g.A[(int64_t)ft[a] * g.ld + fs[b]], (T)((vr + d * ccr) * jac), (T)((vi + d * cci) * jac));
+    } else if (lane < 12) {
+        const int a = lane - 9;
+        double vr = 0, vi = 0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            if (i == a) {
+                vr = acc[18 + 2 * i];
+                vi = acc[18 + 2 * i + 1];
+            }
+        red_add_cx(&g.B[(int64_t)ft[a] * g.F + s], (T)(vr * jac), (T)(vi * jac));
+    }
+}
+
+// orbit row weights (p1_symmetry_orbit_weights, BeatEngineCore.jl:563-582):
+// the rows of A and B of vertices on a symmetry plane, times 2 per plane
+template <typename T>
+__global__ void row_weight_kernel(const int *verts, const double *weights, int nw, Cx<T> *A, int64_t ld, int n,
+                                  Cx<T> *B, int F) {
+    const int v = blockIdx.y;
+    if (v >= nw) return;
+    const int row = verts[v];
+    const T w = (T)weights[v];
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n + F; j += gridDim.x * blockDim.x) {
+        Cx<T> &e = j < n ? A[(int64_t)row * ld + j] : B[(int64_t)row * F + (j - n)];
+        e.re *= w;
+        e.im *= w;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // identity terms: A += 0.5 M_p1p1, B += -0.5 eta M_p1dp0
 // ---------------------------------------------------------------------------
 template <typename T>
@@ -668,7 +837,7 @@ __global__ void identity_kernel(const int *faces, const double *areas, int F, in
 // ---------------------------------------------------------------------------
 // host driver
 // ---------------------------------------------------------------------------
-template <typename T, int Q> static void launch_regular(beat_b200_ctx *c, double k, double eta) {
+template <typename T, int Q> static void launch_regular(beat_b200_ctx *c, double k, double eta, int img) {
     RegArgs<T> g;
     const bool d = sizeof(T) == 8;
     g.qpts = (const T *)(d ? c->pos_qpts64.p : c->pos_qpts32.p);
@@ -692,6 +861,11 @@ template <typename T, int Q> static void launch_regular(beat_b200_ctx *c, double
     g.k = (T)k;
     g.eta = (T)eta;
     g.k2 = (T)(k * k);
+    if (img >= 0) {
+        g.image = 1;
+        for (int i = 0; i < 3; ++i) g.xs[i] = (T)c->img_sign[img][i];
+        g.xdet = (T)c->img_det[img];
+    }
     const size_t smem = regular_smem_bytes<T, Q>();
     BB_CUDA(cudaFuncSetAttribute(regular_pairs_kernel<T, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid(c->trial_tiles.ntiles, c->test_tiles.ntiles);
@@ -700,7 +874,7 @@ template <typename T, int Q> static void launch_regular(beat_b200_ctx *c, double
 }
 
 // FP32 form: the symmetric kernel over unordered pairs of square tiles
-template <int Q> static void launch_sym(beat_b200_ctx *c, double k, double eta) {
+template <int Q> static void launch_sym(beat_b200_ctx *c, double k, double eta, int img) {
     RegArgs<float> g;
     g.qpts = c->pos_qpts32.as<float>();
     g.normal = c->pos_normal32.as<float>();
@@ -720,6 +894,11 @@ template <int Q> static void launch_sym(beat_b200_ctx *c, double k, double eta) 
     g.k = (float)k;
     g.eta = (float)eta;
     g.k2 = (float)(k * k);
+    if (img >= 0) {
+        g.image = 1;
+        for (int i = 0; i < 3; ++i) g.xs[i] = c->img_sign[img][i];
+        g.xdet = c->img_det[img];
+    }
     const size_t smem = sym_smem_bytes<Q>();
     BB_CUDA(cudaFuncSetAttribute(sym_pairs_kernel<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int64_t nt = c->sym_tiles.ntiles;
@@ -737,17 +916,19 @@ template <typename T> static void assemble_t(beat_b200_ctx *c, double k, double 
     BB_CUDA(cudaMemsetAsync(w.A.p, 0, (size_t)N * w.ld * sizeof(Cx<T>), c->stream));
     BB_CUDA(cudaMemsetAsync(w.B.p, 0, (size_t)N * F * sizeof(Cx<T>), c->stream));
     BB_CUDA(cudaEventRecord(c->ev[8], c->stream));
-    if (sizeof(T) == 4) {
-        switch (c->Q) {
-            case 1: launch_sym<1>(c, k, eta); break;
-            case 3: launch_sym<3>(c, k, eta); break;
-            default: launch_sym<6>(c, k, eta); break;
-        }
-    } else {
-        switch (c->Q) {
-            case 1: launch_regular<T, 1>(c, k, eta); break;
-            case 3: launch_regular<T, 3>(c, k, eta); break;
-            default: launch_regular<T, 6>(c, k, eta); break;
+    for (int img = -1; img < c->nimg; ++img) {  // the mesh itself, then one pass per symmetry image
+        if (sizeof(T) == 4) {
+            switch (c->Q) {
+                case 1: launch_sym<1>(c, k, eta, img); break;
+                case 3: launch_sym<3>(c, k, eta, img); break;
+                default: launch_sym<6>(c, k, eta, img); break;
+            }
+        } else {
+            switch (c->Q) {
+                case 1: launch_regular<T, 1>(c, k, eta, img); break;
+                case 3: launch_regular<T, 3>(c, k, eta, img); break;
+                default: launch_regular<T, 6>(c, k, eta, img); break;
+            }
         }
     }
     BB_CUDA(cudaEventRecord(c->ev[1], c->stream));
@@ -775,10 +956,46 @@ template <typename T> static void assemble_t(beat_b200_ctx *c, double k, double 
         singular_pairs_kernel<T><<<(unsigned)((c->npairs + wpb - 1) / wpb), 32 * wpb, 0, c->stream>>>(s);
         BB_CUDA(cudaGetLastError());
     }
+    if (c->nimg_pairs > 0) {
+        ImgArgs<T> d;
+        d.test = c->ip_test.as<int>();
+        d.trial = c->ip_trial.as<int>();
+        d.rule = c->ip_rule.as<int>();
+        d.img = c->ip_img.as<int>();
+        d.jac = c->ip_jac.as<double>();
+        d.nn = c->ip_nn.as<double>();
+        d.rule_start = c->rule_start.as<int>();
+        d.rule_data = c->rule_data.as<double>();
+        d.verts = c->d_verts.as<double>();
+        d.faces = c->d_faces.as<int>();
+        d.normals = c->d_normals.as<double>();
+        d.curls = c->d_curls.as<double>();
+        d.Q = c->Q;
+        d.RI = c->Q == 1 ? 0 : c->Q == 3 ? 1 : 2;
+        d.A = w.A.as<Cx<T>>();
+        d.B = w.B.as<Cx<T>>();
+        d.ld = w.ld;
+        d.F = F;
+        d.npairs = c->nimg_pairs;
+        d.k = k;
+        d.eta = eta;
+        for (int i = 0; i < 3; ++i) {
+            for (int j = 0; j < 3; ++j) d.xf.s[i][j] = c->img_sign[i][j];
+            d.xf.det[i] = c->img_det[i];
+        }
+        image_delta_kernel<T><<<(unsigned)((c->nimg_pairs + 7) / 8), 256, 0, c->stream>>>(d);
+        BB_CUDA(cudaGetLastError());
+    }
     BB_CUDA(cudaEventRecord(c->ev[2], c->stream));
     identity_kernel<T><<<(F + 255) / 256, 256, 0, c->stream>>>(c->d_faces.as<int>(), c->d_areas.as<double>(), F,
                                                                c->Q, eta, w.A.as<Cx<T>>(), w.ld, w.B.as<Cx<T>>());
     BB_CUDA(cudaGetLastError());
+    if (c->nweighted > 0) {
+        row_weight_kernel<T><<<dim3(32, c->nweighted), 256, 0, c->stream>>>(
+            c->rw_vert.as<int>(), c->rw_weight.as<double>(), c->nweighted, w.A.as<Cx<T>>(), w.ld, N,
+            w.B.as<Cx<T>>(), F);
+        BB_CUDA(cudaGetLastError());
+    }
     BB_CUDA(cudaMemsetAsync(w.b.p, 0, sizeof(Cx<double>) * (size_t)N * R, c->stream));
     tall_gemm<T>(c->stream, c->sm_count, w.B.as<Cx<T>>(), F, N, F, reinterpret_cast<const double *>(q), w.b.as<double>(),
                  R, 1.0);

@@ -266,11 +266,66 @@ void set_mesh(beat_b200_ctx *c, int V, const double *verts, int F, const int32_t
                "set_mesh: singular order must be in 1..8");
     BB_REQUIRE(F <= (1 << 24) && V <= (1 << 24), BEAT_B200_INVALID_ARG, "set_mesh: mesh too large");
     release_workspace(c);
+    if (c->in_verts.data() != verts) c->in_verts.assign(verts, verts + 3 * (size_t)V);
+    if (c->in_faces.data() != faces) c->in_faces.assign(faces, faces + 3 * (size_t)F);
     c->V = V;
     c->F = F;
     c->quad_order = quad_order;
     c->sing_order = sing_order;
     c->verts.assign(verts, verts + 3 * (size_t)V);
+    // symmetry: images, plane snapping, fundamental-domain check
+    // (symmetry_transforms, snap_symmetry_plane_vertices,
+    // validate_symmetry_fundamental_domain!, BeatEngineCore.jl:463-548)
+    c->nimg = 0;
+    {
+        auto add = [&](float sx, float sy, float sz, float det) {
+            c->img_sign[c->nimg][0] = sx;
+            c->img_sign[c->nimg][1] = sy;
+            c->img_sign[c->nimg][2] = sz;
+            c->img_det[c->nimg] = det;
+            ++c->nimg;
+        };
+        if (c->sym_mode == 1 || c->sym_mode == 2) add(-1, 1, 1, -1);
+        if (c->sym_mode == 2) {
+            add(1, -1, 1, -1);
+            add(-1, -1, 1, 1);
+        }
+        if (c->sym_mode == 3) add(1, -1, 1, -1);
+    }
+    std::vector<int> rw_v;
+    std::vector<double> rw_w;
+    if (c->sym_mode == 1 || c->sym_mode == 2) {
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int v = 0; v < V; ++v)
+            for (int i = 0; i < 3; ++i) {
+                lo[i] = std::min(lo[i], verts[3 * v + i]);
+                hi[i] = std::max(hi[i], verts[3 * v + i]);
+            }
+        const double diag = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
+                                      (hi[2] - lo[2]) * (hi[2] - lo[2]));
+        const double tol = std::max(1e-9, diag * 1e-6);
+        const int naxes = c->sym_mode == 2 ? 2 : 1;
+        for (int v = 0; v < V; ++v) {
+            double w = 1.0;
+            for (int ax = 0; ax < naxes; ++ax) {
+                double &x = c->verts[3 * v + ax];
+                BB_REQUIRE(x >= -tol, BEAT_B200_INVALID_ARG,
+                           std::string("set_mesh: vertex ") + std::to_string(v + 1) +
+                               " lies outside the positive fundamental domain of the symmetry");
+                if (std::fabs(x) <= tol) {
+                    x = 0.0;
+                    w *= 2.0;
+                }
+            }
+            if (w != 1.0) {
+                rw_v.push_back(v);
+                rw_w.push_back(w);
+            }
+        }
+    }
+    c->nweighted = (int)rw_v.size();
+    upload(c->rw_vert, rw_v);
+    upload(c->rw_weight, rw_w);
     c->faces.resize(3 * (size_t)F);
     for (size_t i = 0; i < 3 * (size_t)F; ++i) {
         BB_REQUIRE(faces[i] >= 1 && faces[i] <= V, BEAT_B200_INVALID_ARG,
@@ -468,7 +523,92 @@ void set_mesh(beat_b200_ctx *c, int V, const double *verts, int F, const int32_t
         }
     }
     c->npairs = (int64_t)sp_t.size();
-    c->regular_pairs = (int64_t)F * F - c->npairs;
+    c->regular_pairs = (int64_t)F * F * (1 + c->nimg) - c->npairs;
+
+    // touching image pairs: test element t and reflected trial element s
+    // sharing vertex positions (image_singular_candidates and
+    // geometric_adjacency_info, BeatEngineCore.jl:624-650,1152-1180; tolerance
+    // 1e-8 as there); their rules join the same remapped-rule table
+    std::vector<int> ip_t, ip_s, ip_r, ip_x;
+    std::vector<double> ip_j, ip_n;
+    if (c->nimg > 0) {
+        const double tol = 1e-8;
+        auto key_of = [&](double x, double y, double z) {
+            return std::array<long long, 3>{(long long)std::llround(x / tol), (long long)std::llround(y / tol),
+                                            (long long)std::llround(z / tol)};
+        };
+        std::map<std::array<long long, 3>, std::vector<int>> by_key;
+        for (int t = 0; t < F; ++t)
+            for (int a = 0; a < 3; ++a) {
+                const double *p = &c->verts[3 * c->faces[3 * t + a]];
+                by_key[key_of(p[0], p[1], p[2])].push_back(t);
+            }
+        for (int ix = 0; ix < c->nimg; ++ix) {
+            const float *sg = c->img_sign[ix];
+            std::map<std::pair<int, int>, int> seen_pair;
+            for (int s = 0; s < F; ++s) {
+                double sv[3][3];
+                for (int b = 0; b < 3; ++b)
+                    for (int i = 0; i < 3; ++i) sv[b][i] = sg[i] * c->verts[3 * c->faces[3 * s + b] + i];
+                for (int b = 0; b < 3; ++b) {
+                    auto it = by_key.find(key_of(sv[b][0], sv[b][1], sv[b][2]));
+                    if (it == by_key.end()) continue;
+                    for (int t : it->second) {
+                        if (seen_pair.count({t, s})) continue;
+                        seen_pair[{t, s}] = 1;
+                        int sa[3], sb[3], n = 0;
+                        for (int i = 0; i < 3; ++i)
+                            for (int j = 0; j < 3; ++j) {
+                                const double *tp = &c->verts[3 * c->faces[3 * t + i]];
+                                const double d0 = tp[0] - sv[j][0], d1 = tp[1] - sv[j][1], d2 = tp[2] - sv[j][2];
+                                if (std::sqrt(d0 * d0 + d1 * d1 + d2 * d2) <= tol && n < 3) {
+                                    sa[n] = i + 1;
+                                    sb[n] = j + 1;
+                                    ++n;
+                                }
+                            }
+                        if (n == 0) continue;
+                        int kind = n == 3 ? COINCIDENT : n == 2 ? EDGE : VERTEX;
+                        std::array<int, 5> key{kind, 0, 0, 0, 0};
+                        if (kind == EDGE) {
+                            if (sb[1] < sb[0]) {
+                                std::swap(sa[0], sa[1]);
+                                std::swap(sb[0], sb[1]);
+                            }
+                            key = {kind, sa[0], sa[1], sb[0], sb[1]};
+                        } else if (kind == VERTEX) {
+                            key = {kind, sa[0], 0, sb[0], 0};
+                        }
+                        int kc = (((key[0] * 4 + key[1]) * 4 + key[2]) * 4 + key[3]) * 4 + key[4];
+                        auto kr = key_rule.find(kc);
+                        int r;
+                        if (kr == key_rule.end()) {
+                            r = (int)keys.size();
+                            key_rule[kc] = r;
+                            keys.push_back(key);
+                        } else {
+                            r = kr->second;
+                        }
+                        ip_t.push_back(t);
+                        ip_s.push_back(s);
+                        ip_r.push_back(r);
+                        ip_x.push_back(ix);
+                        ip_j.push_back((2.0 * c->areas[t]) * (2.0 * c->areas[s]));
+                        double nn = 0;
+                        for (int i = 0; i < 3; ++i) nn += c->normals[3 * t + i] * sg[i] * c->normals[3 * s + i];
+                        ip_n.push_back(nn);
+                    }
+                }
+            }
+        }
+    }
+    c->nimg_pairs = (int64_t)ip_t.size();
+    upload(c->ip_test, ip_t);
+    upload(c->ip_trial, ip_s);
+    upload(c->ip_rule, ip_r);
+    upload(c->ip_img, ip_x);
+    upload(c->ip_jac, ip_j);
+    upload(c->ip_nn, ip_n);
     c->nrules = (int)keys.size();
     std::vector<DuffyPt> base[4];
     for (int k = 1; k <= 3; ++k) base[k] = duffy(sing_order, k);
@@ -549,7 +689,8 @@ int64_t device_bytes(const beat_b200_ctx *c) {
     for (const DevBuf *b : {&c->pos_face, &c->pos_qpts64, &c->pos_qpts32, &c->pos_normal64, &c->pos_normal32,
                             &c->pos_curl64, &c->pos_curl32, &c->pos_area64, &c->pos_area32, &c->pos_gvert,
                             &c->d_verts, &c->d_faces, &c->d_normals, &c->d_areas, &c->d_curls, &c->d_qpts,
-                            &c->vf_start, &c->vf_face, &c->adm,
+                            &c->vf_start, &c->vf_face, &c->adm, &c->ip_test, &c->ip_trial, &c->ip_rule,
+                            &c->ip_img, &c->ip_jac, &c->ip_nn, &c->rw_vert, &c->rw_weight,
                             &c->sp_test, &c->sp_trial, &c->sp_rule, &c->sp_jac, &c->sp_nn, &c->rule_start,
                             &c->rule_data, &c->status, &c->barrier})
         s += (int64_t)b->bytes;

@@ -28,27 +28,40 @@ constexpr int FLD_RC = 16;      // right-hand sides per pass
 constexpr int FLD_CHUNK = 32;   // sources per shared-memory chunk
 constexpr int FLD_THREADS = 128;
 
-// per source: position, normal, p-density and q-density for R columns
+struct FieldImages {
+    int n;            // copies: the mesh itself, then its symmetry images
+    double s[4][3];   // per copy: signs of x, y, z
+};
+
+// per source: position, normal, p-density and q-density for R columns, for
+// the mesh and each symmetry image (reflected position and normal, the same
+// densities); copy ix of source s is entry ix * F Q + s of arrays of stride
+// ST = images.n F Q
 __global__ void field_sources_kernel(const double *qpts, const double *normals, const double *areas,
                                      const int *faces, int F, int Q, const double *rule_w3, int N,
                                      const double2 *p, const double2 *q, int R, double *ys, double *ns,
-                                     double2 *ps, double2 *qs) {
+                                     double2 *ps, double2 *qs, FieldImages images) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    const int S = F * Q;
+    const int S = F * Q, ST = S * images.n;
     if (s >= S) return;
     const int f = s / Q, qi = s % Q;
     const double w = rule_w3[4 * qi] * 2.0 * areas[f];
     const double b0 = rule_w3[4 * qi + 1], b1 = rule_w3[4 * qi + 2], b2 = rule_w3[4 * qi + 3];
-    for (int c = 0; c < 3; ++c) {
-        ys[3 * (size_t)s + c] = qpts[3 * (size_t)s + c];
-        ns[3 * (size_t)s + c] = normals[3 * f + c];
-    }
+    for (int ix = 0; ix < images.n; ++ix)
+        for (int c = 0; c < 3; ++c) {
+            ys[3 * ((size_t)ix * S + s) + c] = images.s[ix][c] * qpts[3 * (size_t)s + c];
+            ns[3 * ((size_t)ix * S + s) + c] = images.s[ix][c] * normals[3 * f + c];
+        }
     const int v0 = faces[3 * f], v1 = faces[3 * f + 1], v2 = faces[3 * f + 2];
     for (int r = 0; r < R; ++r) {
         const double2 a = p[(size_t)r * N + v0], b = p[(size_t)r * N + v1], c = p[(size_t)r * N + v2];
-        ps[(size_t)r * S + s] = make_double2((b0 * a.x + b1 * b.x + b2 * c.x) * w, (b0 * a.y + b1 * b.y + b2 * c.y) * w);
+        const double2 pv = make_double2((b0 * a.x + b1 * b.x + b2 * c.x) * w, (b0 * a.y + b1 * b.y + b2 * c.y) * w);
         const double2 qq = q[(size_t)r * F + f];
-        qs[(size_t)r * S + s] = make_double2(qq.x * w, qq.y * w);
+        const double2 qv = make_double2(qq.x * w, qq.y * w);
+        for (int ix = 0; ix < images.n; ++ix) {
+            ps[(size_t)r * ST + (size_t)ix * S + s] = pv;
+            qs[(size_t)r * ST + (size_t)ix * S + s] = qv;
+        }
     }
 }
 
@@ -142,7 +155,13 @@ void farfield(beat_b200_ctx *c, double k, int M, const double *pts_host, int R, 
     BB_REQUIRE(c->F > 0, BEAT_B200_STATE, "no mesh: call beat_b200_set_mesh first");
     BB_REQUIRE(M >= 0 && R >= 1, BEAT_B200_INVALID_ARG, "field: M must be >= 0 and R >= 1");
     if (M == 0) return;
-    const int F = c->F, Q = c->Q, S = F * Q, N = c->V;
+    const int F = c->F, Q = c->Q, N = c->V;
+    FieldImages images;
+    images.n = 1 + c->nimg;
+    for (int i = 0; i < 3; ++i) images.s[0][i] = 1.0;
+    for (int ix = 0; ix < c->nimg; ++ix)
+        for (int i = 0; i < 3; ++i) images.s[1 + ix][i] = c->img_sign[ix][i];
+    const int S = F * Q * images.n;  // sources of the mesh and its images
     if (c->adm_set) {  // the boundary's Neumann data include the admittance term
         c->ws.qeff.alloc(sizeof(double2) * (size_t)F * R);
         effective_neumann(c, R, p_dev, q_dev, c->ws.qeff.as<double>());
@@ -169,10 +188,10 @@ void farfield(beat_b200_ctx *c, double k, int M, const double *pts_host, int R, 
         BB_CUDA(cudaMemcpyAsync(d_rw, rw3.data(), sizeof(double) * 4 * Q, cudaMemcpyHostToDevice, c->stream));
         BB_CUDA(cudaMemcpyAsync(d_pts, pts_host, sizeof(double) * 3 * M, cudaMemcpyHostToDevice, c->stream));
         BB_CUDA(cudaMemsetAsync(out_dev, 0, sizeof(double2) * (size_t)M * R, c->stream));
-        field_sources_kernel<<<(S + 255) / 256, 256, 0, c->stream>>>(
+        field_sources_kernel<<<(F * Q + 255) / 256, 256, 0, c->stream>>>(
             c->d_qpts.as<double>(), c->d_normals.as<double>(), c->d_areas.as<double>(), c->d_faces.as<int>(), F, Q,
             d_rw, N, reinterpret_cast<const double2 *>(p_dev), reinterpret_cast<const double2 *>(q_dev), R, ys, ns, ps,
-            qs);
+            qs, images);
         BB_CUDA(cudaGetLastError());
         const int mt = (M + FLD_THREADS - 1) / FLD_THREADS;
         const int want = std::max(1, (4 * c->sm_count) / mt);

@@ -168,6 +168,20 @@ struct beat_b200_ctx {
     bb::DevBuf d_qpts;            // F x Q x 3 double (field sources)
     bb::DevBuf vf_start, vf_face; // vertex -> incident faces (CSR: V + 1 offsets, 3F face ids)
 
+    // symmetry images (0 off, 1 x, 2 xy, 3 ground): the mesh is the
+    // fundamental domain, every image reflects the trial elements
+    int sym_mode = 0;
+    int nimg = 0;
+    float img_sign[3][3] = {};    // per image: sign of x, y, z
+    float img_det[3] = {};        // per image: determinant (curl factor)
+    std::vector<double> in_verts; // set_mesh input as given (re-run on a symmetry change)
+    std::vector<int32_t> in_faces;
+    int64_t nimg_pairs = 0;       // touching (test, reflected trial) pairs
+    bb::DevBuf ip_test, ip_trial, ip_rule, ip_img;   // int per pair
+    bb::DevBuf ip_jac, ip_nn;                        // double per pair
+    int nweighted = 0;            // vertices on a symmetry plane
+    bb::DevBuf rw_vert, rw_weight;  // their ids and orbit weights (2 or 4)
+
     // admittance boundary condition q = q0 - a (P p), P = face average of P1 p
     bb::DevBuf adm;               // F complex FP64 coefficients a_f
     bool adm_set = false;

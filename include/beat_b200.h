@@ -187,6 +187,19 @@ int32_t beat_b200_sweep_device(beat_b200_ctx *ctx, int32_t nfreq, const double *
                                const beat_b200_opts *opts, void *d_p, int32_t M,
                                const double *dirs, void *d_ff, beat_b200_diag *diags);
 
+/* Symmetry images (the reference's symmetry_mode: normalized_symmetry_mode,
+ * symmetry_transforms, BeatEngineCore.jl:448-482; image passes and
+ * image-singular deltas, src/BeatEngineCudaBurtonMiller.jl:475-493,
+ * src/BeatEngineCudaSingular.jl:140-278,590-897; orbit row weights,
+ * BeatEngineCore.jl:563-582): 0 off, 1 x (mesh in x >= 0, mirror x), 2 xy
+ * (mesh in x, y >= 0), 3 ground (rigid ground plane y = 0).  The mesh is the
+ * fundamental domain: vertices within max(1e-9, 1e-6 x bounding-box
+ * diagonal) of an active plane are snapped onto it, a vertex on the negative
+ * side is an error.  Solves, fields, sweeps and the adjoint include the
+ * images.  May be called before or after beat_b200_set_mesh (after: the mesh
+ * set-up is rebuilt). */
+int32_t beat_b200_set_symmetry(beat_b200_ctx *ctx, int32_t mode);
+
 /* Admittance boundary condition (row a19 of the path; the reference's
  * exterior solve has none, its admittance is a coupled-FEM wall model,
  * BeatEngineCoupled.jl:594-623).  With coefficients a (F complex, one per
