@@ -26,7 +26,7 @@ EXPORTS = (
     "beat_b200_field", "beat_b200_farfield", "beat_b200_farfield_device", "beat_b200_assemble",
     "beat_b200_release_workspace", "beat_b200_device_bytes", "beat_b200_stream", "beat_b200_resolve_noalloc",
     "beat_b200_sweep", "beat_b200_sweep_device", "beat_b200_set_admittance", "beat_b200_adjoint",
-    "beat_b200_set_symmetry",
+    "beat_b200_set_symmetry", "beat_b200_field_gradient", "beat_b200_field_gradient_device",
 )
 
 SYMMETRY_MODES = {"off": 0, "x": 1, "xy": 2, "ground": 3}
@@ -93,6 +93,10 @@ def load(path: str = LIB_PATH):
     L.beat_b200_farfield.restype = i32
     L.beat_b200_farfield_device.argtypes = [vp, f64, i32, dp, i32, vp, vp, vp]
     L.beat_b200_farfield_device.restype = i32
+    L.beat_b200_field_gradient.argtypes = [vp, f64, i32, dp, i32, dp, dp, dp]
+    L.beat_b200_field_gradient.restype = i32
+    L.beat_b200_field_gradient_device.argtypes = [vp, f64, i32, dp, i32, vp, vp, vp]
+    L.beat_b200_field_gradient_device.restype = i32
     L.beat_b200_assemble.argtypes = [vp, f64, f64, i32, dp, i32, dp, dp]
     L.beat_b200_assemble.restype = i32
     L.beat_b200_release_workspace.argtypes = [vp]
@@ -228,6 +232,18 @@ class Context:
 
     def field(self, k_signed, points, p, q):
         return self._eval(self.lib.beat_b200_field, k_signed, points, p, q)
+
+    def field_gradient(self, k_signed, points, p, q):
+        """Pressure and gradient at points: M x 4 x R complex128 (value, d/dx,
+        d/dy, d/dz per column)."""
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+        pf, qf = _c128_f(p, self.V), _c128_f(q, self.F)
+        if pf.shape[1] != qf.shape[1]:
+            raise ValueError("p and q need the same number of columns")
+        out = np.zeros((pts.shape[0], 4, pf.shape[1]), dtype=np.complex128, order="F")
+        self._check(self.lib.beat_b200_field_gradient(self.handle, float(k_signed), pts.shape[0], _dp(pts),
+                                                      pf.shape[1], _dp(pf), _dp(qf), _dp(out)))
+        return out
 
     def farfield(self, k_signed, dirs, p, q):
         return self._eval(self.lib.beat_b200_farfield, k_signed, dirs, p, q)

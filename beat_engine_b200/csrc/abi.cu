@@ -366,6 +366,37 @@ int32_t beat_b200_farfield(beat_b200_ctx *c, double k, int32_t M, const double *
     return field_common(c, k, M, dirs, R, p, q, out, true);
 }
 
+int32_t beat_b200_field_gradient(beat_b200_ctx *c, double k, int32_t M, const double *points, int32_t R,
+                                 const double *p, const double *q, double *out) {
+    return guarded(c, [&] {
+        BB_REQUIRE(c->F > 0, BEAT_B200_STATE, "no mesh: call beat_b200_set_mesh first");
+        BB_REQUIRE(M >= 0 && R >= 1 && (M == 0 || (points && p && q && out)), BEAT_B200_INVALID_ARG,
+                   "field gradient: bad arguments");
+        if (M == 0) return;
+        DevBuf &buf = c->ws.io;
+        buf.alloc(16 * ((size_t)c->V * R + (size_t)c->F * R + 4 * (size_t)M * R));
+        try {
+            double *dp = buf.as<double>(), *dq = dp + 2 * (size_t)c->V * R, *dout = dq + 2 * (size_t)c->F * R;
+            BB_CUDA(cudaMemcpyAsync(dp, p, (size_t)c->V * R * 16, cudaMemcpyHostToDevice, c->stream));
+            BB_CUDA(cudaMemcpyAsync(dq, q, (size_t)c->F * R * 16, cudaMemcpyHostToDevice, c->stream));
+            field_gradient(c, k, M, points, R, dp, dq, dout);
+            BB_CUDA(cudaMemcpyAsync(out, dout, 4 * (size_t)M * R * 16, cudaMemcpyDeviceToHost, c->stream));
+            BB_CUDA(cudaStreamSynchronize(c->stream));
+        } catch (...) {
+            if (c->stream) cudaStreamSynchronize(c->stream);
+            throw;
+        }
+    });
+}
+
+int32_t beat_b200_field_gradient_device(beat_b200_ctx *c, double k, int32_t M, const double *points, int32_t R,
+                                        const void *d_p, const void *d_q, void *d_out) {
+    return guarded(c, [&] {
+        BB_REQUIRE(M == 0 || (points && d_p && d_q && d_out), BEAT_B200_INVALID_ARG, "null pointer");
+        field_gradient(c, k, M, points, R, (const double *)d_p, (const double *)d_q, (double *)d_out);
+    });
+}
+
 int32_t beat_b200_farfield_device(beat_b200_ctx *c, double k, int32_t M, const double *dirs, int32_t R,
                                   const void *d_p, const void *d_q, void *d_out) {
     return guarded(c, [&] {

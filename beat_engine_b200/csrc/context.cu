@@ -54,7 +54,7 @@ template <typename T> static void upload(DevBuf &d, const std::vector<T> &h) {
 // ---------------------------------------------------------------------------
 // rules
 // ---------------------------------------------------------------------------
-static int triangle_rule(int order, std::vector<double> &pts, std::vector<double> &w) {
+int triangle_rule(int order, std::vector<double> &pts, std::vector<double> &w) {
     if (order <= 1) {
         pts = {1.0 / 3.0, 1.0 / 3.0};
         w = {0.5};
@@ -672,7 +672,7 @@ void ensure_workspace(beat_b200_ctx *c, int precision, int R) {
 void release_workspace(beat_b200_ctx *c) {
     Workspace &w = c->ws;
     for (DevBuf *b : {&w.A, &w.Aop, &w.B, &w.b, &w.x, &w.ipiv, &w.perm, &w.panel_scratch, &w.stage, &w.krylov,
-                      &w.small, &w.q, &w.small_solve, &w.dinv, &w.field, &w.io, &w.qeff})
+                      &w.small, &w.q, &w.small_solve, &w.dinv, &w.field, &w.io, &w.qeff, &w.grad})
         b->free_();
     w.precision = -1;
     w.N = w.F = w.R = 0;
@@ -684,7 +684,7 @@ int64_t device_bytes(const beat_b200_ctx *c) {
     int64_t s = 0;
     const Workspace &w = c->ws;
     for (const DevBuf *b : {&w.A, &w.Aop, &w.B, &w.b, &w.x, &w.ipiv, &w.perm, &w.panel_scratch, &w.stage, &w.krylov,
-                            &w.small, &w.q, &w.small_solve, &w.dinv, &w.field, &w.io, &w.qeff})
+                            &w.small, &w.q, &w.small_solve, &w.dinv, &w.field, &w.io, &w.qeff, &w.grad})
         s += (int64_t)b->bytes;
     for (const DevBuf *b : {&c->pos_face, &c->pos_qpts64, &c->pos_qpts32, &c->pos_normal64, &c->pos_normal32,
                             &c->pos_curl64, &c->pos_curl32, &c->pos_area64, &c->pos_area32, &c->pos_gvert,

@@ -121,6 +121,7 @@ struct Workspace {
     DevBuf field;         // field sources and evaluation points (grow-only)
     DevBuf io;            // device staging of the host-buffer entry points (grow-only)
     DevBuf qeff;          // Neumann data with the admittance term, for the field (grow-only)
+    DevBuf grad;          // field gradient: near (point, face) pairs and error word (grow-only)
     int solve_epoch = 0;  // flag value of the latest substitution launch
     int lu_valid = 0;     // factors match the current operator
 };
@@ -222,6 +223,8 @@ int read_status(beat_b200_ctx *c);
 
 // assembly.cu: rule tables in constant memory (fixed per rule size)
 void upload_rule_tables(const std::vector<double> &pts, const std::vector<double> &w, int Q);
+// context.cu: triangle_rule(T, order) of the reference (weights sum to 1/2)
+int triangle_rule(int order, std::vector<double> &pts, std::vector<double> &w);
 // assembly.cu: A (row-major N x ld) and B (N x F) in the workspace precision,
 // then b = B q (FP64, N x R column-major).  q_dev is F x R FP64 complex.
 void assemble(beat_b200_ctx *c, double k, double eta, int precision, int R, const void *q_dev,
@@ -261,5 +264,8 @@ IrResult gmres_refine_adjoint(beat_b200_ctx *c, int R, double *x_dev, const doub
 // field.cu
 void farfield(beat_b200_ctx *c, double k, int M, const double *dirs_host, int R, const double *p_dev,
               const double *q_dev, double *out_dev, bool far);
+// pressure and its gradient, M x 4 x R complex (value, d/dx, d/dy, d/dz)
+void field_gradient(beat_b200_ctx *c, double k, int M, const double *pts_host, int R, const double *p_dev,
+                    const double *q_dev, double *out_dev);
 
 }  // namespace bb

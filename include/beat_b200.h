@@ -130,6 +130,26 @@ int32_t beat_b200_field(beat_b200_ctx *ctx, double k_signed, int32_t M, const do
 int32_t beat_b200_farfield(beat_b200_ctx *ctx, double k_signed, int32_t M, const double *dirs,
                            int32_t R, const double *p, const double *q, double *out);
 
+/* Pressure and its gradient at M observation points (pressure_gradient_v1):
+ * out is M x 4 x R complex, column-major, component d (0 = value, 1..3 =
+ * d/dx, d/dy, d/dz) of column r at out[m + M (d + 4 r)].  The regular
+ * quadrature sum is corrected, for every face (and symmetry image) whose
+ * centroid lies within 3 face diameters of a point, by adaptive subdivision
+ * with the fourth-order rule down to depth 12; a point closer to the boundary
+ * than that resolves gives BEAT_B200_INVALID_ARG.  Replaces
+ * evaluate_galerkin_field_gradient_cuda (src/BeatEngineCudaFieldGradient.jl:
+ * 20-38) with correct_field_gradient! (src/BeatEngineFieldGradient.jl:45-71),
+ * which the reference runs on host threads; here both parts run on the GPU.
+ * The reference requires the fourth-order rule for gradients
+ * (BeatEngineCompiledDriver.jl:4169-4170): set_mesh with quad_order 4. */
+int32_t beat_b200_field_gradient(beat_b200_ctx *ctx, double k_signed, int32_t M, const double *points,
+                                 int32_t R, const double *p, const double *q, double *out);
+
+/* As beat_b200_field_gradient with p, q and out in device memory. */
+int32_t beat_b200_field_gradient_device(beat_b200_ctx *ctx, double k_signed, int32_t M,
+                                        const double *points, int32_t R, const void *d_p,
+                                        const void *d_q, void *d_out);
+
 /* Device-pointer variants of the two evaluators (points/dirs stay host). */
 int32_t beat_b200_farfield_device(beat_b200_ctx *ctx, double k_signed, int32_t M,
                                   const double *dirs, int32_t R, const void *d_p,

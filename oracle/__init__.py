@@ -54,6 +54,8 @@ def lib():
                                       c_int, dp, dp, dp, c_int, c_int]
         L.bo_field_sym.argtypes = [c_int, dp, c_int, ip, c_int, c_double, c_int, dp, c_int, dp, dp, dp, c_int,
                                    c_int, c_int]
+        L.bo_field_gradient.argtypes = [c_int, dp, c_int, ip, c_int, c_double, c_int, dp, c_int, dp, dp, dp,
+                                        c_int, c_int]
         _lib = L
     return _lib
 
@@ -233,4 +235,28 @@ def field_sym(mesh, k_signed, pts, p, q, mode, far=False, quad_order=4, threads=
                             1 if far else 0)
     if st != 0:
         raise RuntimeError(f"oracle field failed with status {st}")
+    return out
+
+
+def field_gradient(mesh, k_signed, points, p, q, mode="off", quad_order=4, threads=0):
+    """Pressure and its gradient at observation points (pressure_gradient_v1):
+    ``M x 4 x R`` complex (value, d/dx, d/dy, d/dz), with the reference's
+    adaptive near-panel correction."""
+    v = symmetry_snap(mesh.vertices, mode) if mode != "off" else np.ascontiguousarray(mesh.vertices, np.float64)
+    f = np.ascontiguousarray(mesh.faces, dtype=np.int32)
+    pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+    p = np.asarray(p, dtype=np.complex128)
+    q = np.asarray(q, dtype=np.complex128)
+    if p.ndim == 1:
+        p, q = p[:, None], q[:, None]
+    R, M = p.shape[1], pts.shape[0]
+    pf, qf = np.asfortranarray(p), np.asfortranarray(q)
+    out = np.zeros((M, 4, R), dtype=np.complex128, order="F")
+    st = lib().bo_field_gradient(mesh.num_vertices, _dp(v), mesh.num_faces, _ip(f), quad_order, float(k_signed), M,
+                                 _dp(pts), R, pf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                 qf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                 out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), threads, SYMMETRY_MODES[mode])
+    if st != 0:
+        raise RuntimeError("oracle field gradient failed: a point is too close to the boundary"
+                           if st == 4 else f"oracle field gradient failed with status {st}")
     return out

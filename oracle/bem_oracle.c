@@ -38,6 +38,7 @@
 #define BO_EINVAL 1
 #define BO_ENOMEM 2
 #define BO_ESINGULAR 3
+#define BO_ETOOCLOSE 4 /* a field point too close to the boundary for the adaptive correction */
 
 #define BO_SKIP_REGULAR 1
 #define BO_SKIP_SINGULAR 2
@@ -1161,6 +1162,158 @@ int bo_field_sym(int V, const double *verts, int F, const int *faces, int quad_o
     }
     mesh_free(&m);
     return BO_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* pressure and its gradient at observation points (pressure_gradient_v1):   */
+/* field_value_gradient, _gradient_triangle, _adaptive_gradient_triangle,    */
+/* correct_field_gradient!, evaluate_galerkin_field_gradient_cpu,            */
+/* BeatEngineFieldGradient.jl:1-88.  out is M x 4 x R complex, column-major: */
+/* (value, d/dx, d/dy, d/dz) of column r at out[i + M (d + 4 r)].            */
+/* ------------------------------------------------------------------------ */
+static void fvg(v3 x, v3 y, v3 n, const double *p, const double *q, int R, double k, double w, double *acc)
+{
+    v3 r = v3sub(y, x);
+    double rad = v3norm(r);
+    if (rad == 0.0) return;
+    v3 u = {r.x / rad, r.y / rad, r.z / rad};
+    double gsc = w / (4.0 * BO_PI * rad);
+    double g_re = cos(k * rad) * gsc, g_im = sin(k * rad) * gsc;
+    double a_re = -1.0 / rad, a_im = k;
+    double b_re = 3.0 / (rad * rad) - k * k, b_im = -3.0 * k / rad;
+    double proj = v3dot(u, n);
+    double ua[3] = {u.x, u.y, u.z}, na[3] = {n.x, n.y, n.z};
+    for (int c = 0; c < R; ++c) {
+        double pr = p[2 * c], pi = p[2 * c + 1], qr = q[2 * c], qi = q[2 * c + 1];
+        /* value = G (a proj p - q) */
+        double t_re = (a_re * pr - a_im * pi) * proj - qr, t_im = (a_re * pi + a_im * pr) * proj - qi;
+        acc[8 * c] += g_re * t_re - g_im * t_im;
+        acc[8 * c + 1] += g_re * t_im + g_im * t_re;
+        /* gradient = G (a q u - p (b proj u + (a / r) n)) */
+        double aq_re = a_re * qr - a_im * qi, aq_im = a_re * qi + a_im * qr;
+        double bp_re = (b_re * pr - b_im * pi) * proj, bp_im = (b_re * pi + b_im * pr) * proj;
+        double ap_re = (a_re * pr - a_im * pi) / rad, ap_im = (a_re * pi + a_im * pr) / rad;
+        for (int d = 0; d < 3; ++d) {
+            double v_re = aq_re * ua[d] - (bp_re * ua[d] + ap_re * na[d]);
+            double v_im = aq_im * ua[d] - (bp_im * ua[d] + ap_im * na[d]);
+            acc[8 * c + 2 + 2 * d] += g_re * v_re - g_im * v_im;
+            acc[8 * c + 3 + 2 * d] += g_re * v_im + g_im * v_re;
+        }
+    }
+}
+
+/* one triangle with the rule (rpts, rw, nq); pv: 3 x R complex vertex values */
+static void grad_triangle(v3 x, const v3 *v, v3 n, const double *pv, const double *q, int R, double k,
+                          const double *rpts, const double *rw, int nq, double *acc)
+{
+    double jac = v3norm(v3cross(v3sub(v[1], v[0]), v3sub(v[2], v[0])));
+    double *ps = malloc(sizeof(double) * 2 * R);
+    for (int j = 0; j < nq; ++j) {
+        double xi = rpts[2 * j], et = rpts[2 * j + 1], b[3] = {1.0 - xi - et, xi, et};
+        v3 y = {b[0] * v[0].x + b[1] * v[1].x + b[2] * v[2].x, b[0] * v[0].y + b[1] * v[1].y + b[2] * v[2].y,
+                b[0] * v[0].z + b[1] * v[1].z + b[2] * v[2].z};
+        for (int c = 0; c < R; ++c) {
+            ps[2 * c] = b[0] * pv[2 * c] + b[1] * pv[2 * (R + c)] + b[2] * pv[2 * (2 * R + c)];
+            ps[2 * c + 1] = b[0] * pv[2 * c + 1] + b[1] * pv[2 * (R + c) + 1] + b[2] * pv[2 * (2 * R + c) + 1];
+        }
+        fvg(x, y, n, ps, q, R, k, jac * rw[j], acc);
+    }
+    free(ps);
+}
+
+static int grad_adaptive(v3 x, const v3 *v, v3 n, const double *pv, const double *q, int R, double k,
+                         const double *rpts, const double *rw, int nq, int depth, double *acc)
+{
+    v3 c = {(v[0].x + v[1].x + v[2].x) / 3, (v[0].y + v[1].y + v[2].y) / 3, (v[0].z + v[1].z + v[2].z) / 3};
+    double d01 = v3norm(v3sub(v[0], v[1])), d12 = v3norm(v3sub(v[1], v[2])), d20 = v3norm(v3sub(v[2], v[0]));
+    double diam = d01 > d12 ? (d01 > d20 ? d01 : d20) : (d12 > d20 ? d12 : d20);
+    double dist = v3norm(v3sub(x, c));
+    if (diam <= 0.4 * dist && fabs(k) * diam <= 0.7) {
+        grad_triangle(x, v, n, pv, q, R, k, rpts, rw, nq, acc);
+        return BO_OK;
+    }
+    if (depth >= 12) return BO_ETOOCLOSE;
+    v3 ab = {(v[0].x + v[1].x) / 2, (v[0].y + v[1].y) / 2, (v[0].z + v[1].z) / 2};
+    v3 bc = {(v[1].x + v[2].x) / 2, (v[1].y + v[2].y) / 2, (v[1].z + v[2].z) / 2};
+    v3 ca = {(v[2].x + v[0].x) / 2, (v[2].y + v[0].y) / 2, (v[2].z + v[0].z) / 2};
+    double *mid = malloc(sizeof(double) * 6 * R), *sub = malloc(sizeof(double) * 6 * R);
+    /* midpoint values pab, pbc, pca */
+    for (int c2 = 0; c2 < 2 * R; ++c2) {
+        mid[c2] = (pv[c2] + pv[2 * R + c2]) / 2;              /* ab */
+        mid[2 * R + c2] = (pv[2 * R + c2] + pv[4 * R + c2]) / 2;  /* bc */
+        mid[4 * R + c2] = (pv[4 * R + c2] + pv[c2]) / 2;      /* ca */
+    }
+    const v3 tri[4][3] = {{v[0], ab, ca}, {ab, v[1], bc}, {ca, bc, v[2]}, {ab, bc, ca}};
+    const double *src[4][3] = {{pv, mid, mid + 4 * R}, {mid, pv + 2 * R, mid + 2 * R},
+                               {mid + 4 * R, mid + 2 * R, pv + 4 * R}, {mid, mid + 2 * R, mid + 4 * R}};
+    int st = BO_OK;
+    for (int t = 0; t < 4 && st == BO_OK; ++t) {
+        for (int a = 0; a < 3; ++a) memcpy(sub + 2 * R * a, src[t][a], sizeof(double) * 2 * R);
+        st = grad_adaptive(x, tri[t], n, sub, q, R, k, rpts, rw, nq, depth + 1, acc);
+    }
+    free(mid); free(sub);
+    return st;
+}
+
+int bo_field_gradient(int V, const double *verts, int F, const int *faces, int quad_order, double k, int M,
+                      const double *points, int R, const double *p, const double *q, double *out, int nthreads,
+                      int mode)
+{
+    bo_mesh m;
+    int st = mesh_init(&m, V, verts, F, faces, quad_order);
+    if (st != BO_OK) { mesh_free(&m); return st; }
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    bo_xf xf[5];
+    xf[0].s[0] = xf[0].s[1] = xf[0].s[2] = 1.0; xf[0].det = 1.0;
+    int nx = 1 + sym_images(mode, xf + 1);
+    double fine_pts[2 * BO_MAXQ], fine_w[BO_MAXQ];
+    int nfine = bo_triangle_rule(4, fine_pts, fine_w);
+    int N = V, Q = m.Q, status = BO_OK;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int i = 0; i < M; ++i) {
+        v3 x = v3make(points + 3 * i);
+        double *acc = calloc(8 * (size_t)R, sizeof(double));
+        double *pv = malloc(sizeof(double) * 6 * R), *qf = malloc(sizeof(double) * 2 * R);
+        for (int ix = 0; ix < nx; ++ix)
+            for (int f = 0; f < F; ++f) {
+                const int *fc = faces + 3 * f;
+                v3 v[3];
+                for (int a = 0; a < 3; ++a) v[a] = reflect(&xf[ix], v3make(verts + 3 * fc[a]));
+                v3 n = reflect(&xf[ix], v3make(m.normals + 3 * f));
+                for (int a = 0; a < 3; ++a)
+                    for (int c = 0; c < R; ++c) {
+                        pv[2 * (a * R + c)] = p[2 * (fc[a] + (size_t)c * N)];
+                        pv[2 * (a * R + c) + 1] = p[2 * (fc[a] + (size_t)c * N) + 1];
+                    }
+                for (int c = 0; c < R; ++c) { qf[2 * c] = q[2 * (f + (size_t)c * F)]; qf[2 * c + 1] = q[2 * (f + (size_t)c * F) + 1]; }
+                /* regular sum (evaluate_galerkin_field_gradient_cpu) */
+                grad_triangle(x, v, n, pv, qf, R, k, m.rpts, m.rw, Q, acc);
+                /* near-panel correction: adaptive - regular (correct_field_gradient!) */
+                v3 cen = {(v[0].x + v[1].x + v[2].x) / 3, (v[0].y + v[1].y + v[2].y) / 3, (v[0].z + v[1].z + v[2].z) / 3};
+                double d01 = v3norm(v3sub(v[0], v[1])), d12 = v3norm(v3sub(v[1], v[2])), d20 = v3norm(v3sub(v[2], v[0]));
+                double diam = d01 > d12 ? (d01 > d20 ? d01 : d20) : (d12 > d20 ? d12 : d20);
+                if (v3norm(v3sub(x, cen)) > 3.0 * diam) continue;
+                double *fine = calloc(8 * (size_t)R, sizeof(double)), *coarse = calloc(8 * (size_t)R, sizeof(double));
+                int s2 = grad_adaptive(x, v, n, pv, qf, R, k, fine_pts, fine_w, nfine, 0, fine);
+                if (s2 != BO_OK) {
+#pragma omp critical
+                    status = s2;
+                }
+                grad_triangle(x, v, n, pv, qf, R, k, m.rpts, m.rw, Q, coarse);
+                for (size_t e = 0; e < 8 * (size_t)R; ++e) acc[e] += fine[e] - coarse[e];
+                free(fine); free(coarse);
+            }
+        for (int c = 0; c < R; ++c)
+            for (int d = 0; d < 4; ++d) {
+                out[2 * (i + (size_t)M * (d + 4 * c))] = acc[8 * c + 2 * d];
+                out[2 * (i + (size_t)M * (d + 4 * c)) + 1] = acc[8 * c + 2 * d + 1];
+            }
+        free(acc); free(pv); free(qf);
+    }
+    mesh_free(&m);
+    return status;
 }
 
 int bo_version(void) { return 1; }
