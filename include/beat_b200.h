@@ -141,7 +141,7 @@ int32_t beat_b200_farfield(beat_b200_ctx *ctx, double k_signed, int32_t M, const
  * 20-38) with correct_field_gradient! (src/BeatEngineFieldGradient.jl:45-71),
  * which the reference runs on host threads; here both parts run on the GPU.
  * The reference requires the fourth-order rule for gradients
- * (BeatEngineCompiledDriver.jl:4169-4170): set_mesh with quad_order 4. */
+ * (BeatEngineCompiledDriver.jl:4168-4170): set_mesh with quad_order 4. */
 int32_t beat_b200_field_gradient(beat_b200_ctx *ctx, double k_signed, int32_t M, const double *points,
                                  int32_t R, const double *p, const double *q, double *out);
 
