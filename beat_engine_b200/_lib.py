@@ -15,6 +15,9 @@ LIB_PATH = os.path.join(HERE, "libbeatb200.so")
 
 OK, INVALID_ARG, OOM, CUDA_ERROR, NOT_CONVERGED, TIMEOUT, NO_DEVICE, STATE, SINGULAR = range(9)
 FP64, MIXED_FP32_IR = 0, 1
+FLAG_NO_REFINE, FLAG_RHS_MATRIX_FREE, FLAG_RHS_CACHED = 1, 2, 4
+RHS_AUTO, RHS_MATRIX_FREE, RHS_CACHED = 0, 1, 2
+RHS_MODES = {"auto": RHS_AUTO, "matrix_free": RHS_MATRIX_FREE, "cached_operator": RHS_CACHED}
 STATUS_NAMES = {OK: "OK", INVALID_ARG: "INVALID_ARG", OOM: "OOM", CUDA_ERROR: "CUDA_ERROR",
                 NOT_CONVERGED: "NOT_CONVERGED", TIMEOUT: "TIMEOUT", NO_DEVICE: "NO_DEVICE", STATE: "STATE",
                 SINGULAR: "SINGULAR"}
@@ -27,6 +30,7 @@ EXPORTS = (
     "beat_b200_release_workspace", "beat_b200_device_bytes", "beat_b200_stream", "beat_b200_resolve_noalloc",
     "beat_b200_sweep", "beat_b200_sweep_device", "beat_b200_set_admittance", "beat_b200_adjoint",
     "beat_b200_set_symmetry", "beat_b200_field_gradient", "beat_b200_field_gradient_device",
+    "beat_b200_rhs_use_operator",
 )
 
 SYMMETRY_MODES = {"off": 0, "x": 1, "xy": 2, "ground": 3}
@@ -45,10 +49,10 @@ class Diag(ctypes.Structure):
                 ("ir_iterations", ctypes.c_int32), ("ir_converged", ctypes.c_int32),
                 ("ir_residual", ctypes.c_double), ("regular_pairs", ctypes.c_int64),
                 ("singular_pairs", ctypes.c_int64), ("precision", ctypes.c_int32), ("lu_block", ctypes.c_int32),
-                ("lu_split_terms", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("lu_split_terms", ctypes.c_int32), ("rhs_mode", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
-        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 class BeatB200Error(RuntimeError):
@@ -58,6 +62,28 @@ class BeatB200Error(RuntimeError):
 
 
 _lib = None
+
+
+def rhs_mode(value) -> str:
+    """exterior_rhs_mode (exterior_rhs_policy.jl:17-23): the normalised mode name."""
+    mode = str(value).strip().lower()
+    if mode not in RHS_MODES:
+        raise ValueError(f"Unknown exterior right-hand-side mode: {value}. "
+                         "Expected auto, matrix_free or cached_operator.")
+    return mode
+
+
+def use_rhs_operator(mode, excitations: int, matrix_bytes: int, operator_bytes: int, available_bytes: int) -> bool:
+    """exterior_use_rhs_operator (exterior_rhs_policy.jl:38-44), evaluated by
+    the library's own policy (beat_b200_rhs_use_operator)."""
+    r = load().beat_b200_rhs_use_operator(RHS_MODES[rhs_mode(mode)], int(excitations), int(matrix_bytes),
+                                          int(operator_bytes), int(available_bytes))
+    return r == 1
+
+
+def rhs_flags(mode) -> int:
+    """opts.flags bits requesting a right-hand-side mode."""
+    return {RHS_AUTO: 0, RHS_MATRIX_FREE: FLAG_RHS_MATRIX_FREE, RHS_CACHED: FLAG_RHS_CACHED}[RHS_MODES[rhs_mode(mode)]]
 
 
 def load(path: str = LIB_PATH):
@@ -93,6 +119,8 @@ def load(path: str = LIB_PATH):
     L.beat_b200_farfield.restype = i32
     L.beat_b200_farfield_device.argtypes = [vp, f64, i32, dp, i32, vp, vp, vp]
     L.beat_b200_farfield_device.restype = i32
+    L.beat_b200_rhs_use_operator.argtypes = [i32, i32, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64]
+    L.beat_b200_rhs_use_operator.restype = i32
     L.beat_b200_field_gradient.argtypes = [vp, f64, i32, dp, i32, dp, dp, dp]
     L.beat_b200_field_gradient.restype = i32
     L.beat_b200_field_gradient_device.argtypes = [vp, f64, i32, dp, i32, vp, vp, vp]

@@ -52,7 +52,17 @@ beat_b200_opts resolve_opts(const beat_b200_opts *o) {
     if (r.lu_block <= 0) r.lu_block = r.precision == BEAT_B200_FP64 ? 64 : 128;
     BB_REQUIRE(r.lu_block == 32 || r.lu_block == 64 || r.lu_block == 128, BEAT_B200_INVALID_ARG,
                "lu_block must be 32, 64 or 128");
+    BB_REQUIRE((r.flags & (BEAT_B200_FLAG_RHS_MATRIX_FREE | BEAT_B200_FLAG_RHS_CACHED)) !=
+                   (BEAT_B200_FLAG_RHS_MATRIX_FREE | BEAT_B200_FLAG_RHS_CACHED),
+               BEAT_B200_INVALID_ARG, "flags request both right-hand-side modes");
     return r;
+}
+
+// the right-hand-side mode the flags request (BEAT_B200_RHS_*)
+static int rhs_request(const beat_b200_opts &o) {
+    if (o.flags & BEAT_B200_FLAG_RHS_MATRIX_FREE) return BEAT_B200_RHS_MATRIX_FREE;
+    if (o.flags & BEAT_B200_FLAG_RHS_CACHED) return BEAT_B200_RHS_CACHED;
+    return BEAT_B200_RHS_AUTO;
 }
 
 __global__ void f32_to_f64_copy(const float2 *src, double2 *dst, size_t n) {
@@ -85,7 +95,7 @@ void solve_core(beat_b200_ctx *c, double k, double eta, int R, const double *d_q
     BB_REQUIRE(R >= 1, BEAT_B200_INVALID_ARG, "R must be >= 1");
     BB_REQUIRE(std::isfinite(k) && k != 0.0 && std::isfinite(eta), BEAT_B200_INVALID_ARG,
                "wavenumber must be finite and nonzero");
-    ensure_workspace(c, o.precision, R);
+    ensure_workspace(c, o.precision, R, rhs_request(o));
     Workspace &w = c->ws;
     const int n = c->V;
     float ms_asm = 0, ms_sing = 0, ms_lu = 0, ms_solve = 0, ms_ir = 0;
@@ -138,7 +148,7 @@ void solve_core(beat_b200_ctx *c, double k, double eta, int R, const double *d_q
         diag->precision = o.precision;
         diag->lu_block = o.lu_block;
         diag->lu_split_terms = o.lu_split_terms;
-        diag->reserved = 0;
+        diag->rhs_mode = w.rhs_cached ? BEAT_B200_RHS_CACHED : BEAT_B200_RHS_MATRIX_FREE;
     }
     BB_REQUIRE(ir.converged || o.precision == BEAT_B200_FP64 || (o.flags & BEAT_B200_FLAG_NO_REFINE),
                BEAT_B200_NOT_CONVERGED,
@@ -317,7 +327,7 @@ int32_t beat_b200_solve(beat_b200_ctx *c, double k, double eta, int32_t R, const
         BB_REQUIRE(q && p_out && R >= 1, BEAT_B200_INVALID_ARG, "null pointer or R < 1");
         BB_REQUIRE(c->F > 0, BEAT_B200_STATE, "no mesh: call beat_b200_set_mesh first");
         const beat_b200_opts o = resolve_opts(opts);
-        ensure_workspace(c, o.precision, R);
+        ensure_workspace(c, o.precision, R, rhs_request(o));
         Workspace &w = c->ws;
         BB_CUDA(cudaMemcpyAsync(w.q.p, q, (size_t)c->F * R * 16, cudaMemcpyHostToDevice, c->stream));
         DevBuf &out = w.io;
@@ -395,6 +405,11 @@ int32_t beat_b200_field_gradient_device(beat_b200_ctx *c, double k, int32_t M, c
         BB_REQUIRE(M == 0 || (points && d_p && d_q && d_out), BEAT_B200_INVALID_ARG, "null pointer");
         field_gradient(c, k, M, points, R, (const double *)d_p, (const double *)d_q, (double *)d_out);
     });
+}
+
+int32_t beat_b200_rhs_use_operator(int32_t mode, int32_t excitations, int64_t matrix_bytes, int64_t operator_bytes,
+                                   int64_t available_bytes) {
+    return rhs_use_operator(mode, excitations, matrix_bytes, operator_bytes, available_bytes);
 }
 
 int32_t beat_b200_farfield_device(beat_b200_ctx *c, double k, int32_t M, const double *dirs, int32_t R,
@@ -494,7 +509,7 @@ int32_t beat_b200_sweep(beat_b200_ctx *c, int32_t nfreq, const double *k_signed,
         const beat_b200_opts o = resolve_opts(opts);
         const size_t qs = (size_t)c->F * R * 2, ps = (size_t)c->V * R * 2, fs = (size_t)M * R * 2;
         run_sweep(c, nfreq, [&](beat_b200_ctx *l, int f) {
-            ensure_workspace(l, o.precision, R);
+            ensure_workspace(l, o.precision, R, rhs_request(o));
             Workspace &w = l->ws;
             BB_CUDA(cudaMemcpyAsync(w.q.p, q + f * qs, qs * sizeof(double), cudaMemcpyHostToDevice, l->stream));
             w.io.alloc((ps + fs) * sizeof(double));

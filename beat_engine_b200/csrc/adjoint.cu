@@ -374,6 +374,9 @@ void adjoint(beat_b200_ctx *c, double k, int M, const double *dirs_host, int R, 
              const double *g_dev, double *w_dev, double *ga_dev, const beat_b200_opts &o, IrResult *ir) {
     Workspace &w = c->ws;
     BB_REQUIRE(w.lu_valid, BEAT_B200_STATE, "adjoint: no factorisation on this context (solve first)");
+    BB_REQUIRE(w.rhs_cached, BEAT_B200_STATE,
+               "adjoint: the last solve formed its right-hand sides matrix-free, so the mapping B is not "
+               "resident; solve with the cached right-hand-side mapping (BEAT_B200_FLAG_RHS_CACHED)");
     BB_REQUIRE(k == c->last_k, BEAT_B200_STATE, "adjoint: the wavenumber differs from the last solve's");
     BB_REQUIRE(M >= 1 && R >= 1, BEAT_B200_INVALID_ARG, "adjoint: M and R must be >= 1");
     const int n = c->V, F = c->F, Q = c->Q;

@@ -94,6 +94,34 @@ __device__ __forceinline__ void red_add_cx(Cx<float> *p, float re, float im) {
     atomicAdd(reinterpret_cast<float2 *>(p), make_float2(re, im));
 }
 
+// Where the right-hand-side operator goes.  Cached (B set): the N x F
+// mapping B, b = B q formed afterwards by one tall product.  Matrix-free (B
+// null): b = B q directly for the R columns of q, so no N x F array exists
+// (exterior_rhs_policy.jl restated, one pass for every column where the
+// reference's matrix_free path integrates once per column).
+template <typename T> struct RhsOut {
+    Cx<T> *B = nullptr;             // N x F, row-major
+    const Cx<double> *q = nullptr;  // F x R, column-major (matrix-free)
+    Cx<double> *b = nullptr;        // N x R, column-major (matrix-free)
+    int F = 0, N = 0, R = 0;
+};
+
+template <typename T>
+__device__ __forceinline__ void rhs_add(const RhsOut<T> &o, int row, int face, T re, T im) {
+    if (o.B) {
+        red_add_cx(&o.B[(int64_t)row * o.F + face], re, im);
+        return;
+    }
+    for (int r = 0; r < o.R; ++r) {
+        const Cx<double> qq = o.q[(size_t)r * o.F + face];
+        red_add_cx(&o.b[(size_t)r * o.N + row], (double)re * qq.re - (double)im * qq.im,
+                   (double)re * qq.im + (double)im * qq.re);
+    }
+}
+
+// columns of q per staged chunk in the matrix-free tile epilogues
+constexpr int MF_RC = 8;
+
 template <typename T> struct RegArgs {
     const T *qpts;      // by position: F x Q x 3
     const T *normal;    // F x 3
@@ -113,6 +141,10 @@ template <typename T> struct RegArgs {
     int image = 0;
     T xs[3] = {T(1), T(1), T(1)};
     T xdet = T(1);
+    // matrix-free right-hand sides (B null): b (N x R) += B-tile x q (F x R)
+    const Cx<double> *q = nullptr;
+    Cx<double> *b = nullptr;
+    int N = 0, R = 0;
 };
 
 // Element-pair kernel.  grid = (trial tiles, test tiles), 256 threads.
@@ -275,11 +307,42 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
         if (v.re != T(0) || v.im != T(0))
             red_add_cx(&g.A[(int64_t)g.t_verts[tv0 + lt] * g.ld + g.s_verts[sv0 + ls]], v.re, v.im);
     }
-    for (int i = tid; i < nvt * ns; i += REG_THREADS) {
-        const int lt = i / ns, sl = i % ns;
-        const Cx<T> v = sB[lt * TS + sl];
-        if (v.re != T(0) || v.im != T(0))
-            red_add_cx(&g.B[(int64_t)g.t_verts[tv0 + lt] * g.F + g.face_id[s0 + sl]], v.re, v.im);
+    if (g.B) {
+        for (int i = tid; i < nvt * ns; i += REG_THREADS) {
+            const int lt = i / ns, sl = i % ns;
+            const Cx<T> v = sB[lt * TS + sl];
+            if (v.re != T(0) || v.im != T(0))
+                red_add_cx(&g.B[(int64_t)g.t_verts[tv0 + lt] * g.F + g.face_id[s0 + sl]], v.re, v.im);
+        }
+        return;
+    }
+    // matrix-free: the tile's rows of b += sB (test vertices x trial faces) q,
+    // q staged MF_RC columns at a time over the (now unused) geometry region
+    Cx<T> *qs = reinterpret_cast<Cx<T> *>(tq);  // [TS][MF_RC]
+    for (int r0 = 0; r0 < g.R; r0 += MF_RC) {
+        const int rc = min(MF_RC, g.R - r0);
+        __syncthreads();
+        for (int i = tid; i < TS * MF_RC; i += REG_THREADS) {
+            const int f = i / MF_RC, r = i % MF_RC;
+            Cx<T> v{T(0), T(0)};
+            if (f < ns && r < rc) {
+                const Cx<double> qq = g.q[(size_t)(r0 + r) * g.F + g.face_id[s0 + f]];
+                v = Cx<T>{(T)qq.re, (T)qq.im};
+            }
+            qs[i] = v;
+        }
+        __syncthreads();
+        for (int i = tid; i < nvt * rc; i += REG_THREADS) {
+            const int lt = i / rc, r = i % rc;
+            T sr = T(0), si = T(0);
+            for (int f = 0; f < ns; ++f) {
+                const Cx<T> bv = sB[lt * TS + f], qv = qs[f * MF_RC + r];
+                sr += bv.re * qv.re - bv.im * qv.im;
+                si += bv.re * qv.im + bv.im * qv.re;
+            }
+            if (sr != T(0) || si != T(0))
+                red_add_cx(&g.b[(size_t)(r0 + r) * g.N + g.t_verts[tv0 + lt]], (double)sr, (double)si);
+        }
     }
 }
 
@@ -522,17 +585,54 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
         if (v.re != T(0) || v.im != T(0)) red_add_cx(&g.A[(int64_t)gi_ * g.ld + gj_], v.re, v.im);
         if (u.re != T(0) || u.im != T(0)) red_add_cx(&g.A[(int64_t)gj_ * g.ld + gi_], u.re, u.im);
     }
-    for (int i = tid; i < nvI * nJ; i += REG_THREADS) {
-        const int li = i / nJ, sj = i % nJ;
-        const Cx<T> v{acc_re[B1 + li * SYM_BS + sj], acc_im[B1 + li * SYM_BS + sj]};
-        if (v.re != T(0) || v.im != T(0))
-            red_add_cx(&g.B[(int64_t)g.t_verts[tv0 + li] * g.F + g.face_id[s0 + sj]], v.re, v.im);
+    if (g.B) {
+        for (int i = tid; i < nvI * nJ; i += REG_THREADS) {
+            const int li = i / nJ, sj = i % nJ;
+            const Cx<T> v{acc_re[B1 + li * SYM_BS + sj], acc_im[B1 + li * SYM_BS + sj]};
+            if (v.re != T(0) || v.im != T(0))
+                red_add_cx(&g.B[(int64_t)g.t_verts[tv0 + li] * g.F + g.face_id[s0 + sj]], v.re, v.im);
+        }
+        for (int i = tid; i < nvJ * nI; i += REG_THREADS) {
+            const int lj = i / nI, ti = i % nI;
+            const Cx<T> v{acc_re[B2 + lj * SYM_BS + ti], acc_im[B2 + lj * SYM_BS + ti]};
+            if (v.re != T(0) || v.im != T(0))
+                red_add_cx(&g.B[(int64_t)g.t_verts[sv0 + lj] * g.F + g.face_id[t0 + ti]], v.re, v.im);
+        }
+        return;
     }
-    for (int i = tid; i < nvJ * nI; i += REG_THREADS) {
-        const int lj = i / nI, ti = i % nI;
-        const Cx<T> v{acc_re[B2 + lj * SYM_BS + ti], acc_im[B2 + lj * SYM_BS + ti]};
-        if (v.re != T(0) || v.im != T(0))
-            red_add_cx(&g.B[(int64_t)g.t_verts[sv0 + lj] * g.F + g.face_id[t0 + ti]], v.re, v.im);
+    // matrix-free: rows of b += B1 q (tile I vertices x tile J faces) and
+    // B2 q (tile J vertices x tile I faces); q of both tiles' faces staged
+    // MF_RC columns at a time over the (now unused) geometry region
+    float2 *qs = reinterpret_cast<float2 *>(xq);  // [2][SYM_F][MF_RC]: tile I faces, then tile J faces
+    for (int r0 = 0; r0 < g.R; r0 += MF_RC) {
+        const int rc = min(MF_RC, g.R - r0);
+        __syncthreads();
+        for (int i = tid; i < 2 * SYM_F * MF_RC; i += REG_THREADS) {
+            const int h = i / (SYM_F * MF_RC), f = (i / MF_RC) % SYM_F, r = i % MF_RC;
+            float2 v = make_float2(0.f, 0.f);
+            if (f < (h ? nJ : nI) && r < rc) {
+                const Cx<double> qq = g.q[(size_t)(r0 + r) * g.F + g.face_id[(h ? s0 : t0) + f]];
+                v = make_float2((float)qq.re, (float)qq.im);
+            }
+            qs[i] = v;
+        }
+        __syncthreads();
+        for (int i = tid; i < (nvI + nvJ) * rc; i += REG_THREADS) {
+            const int row = i / rc, r = i % rc;
+            const bool first = row < nvI;
+            const int base = first ? B1 + row * SYM_BS : B2 + (row - nvI) * SYM_BS;
+            const int nf = first ? nJ : nI;
+            const float2 *qh = qs + (first ? SYM_F * MF_RC : 0);
+            T sr = T(0), si = T(0);
+            for (int f = 0; f < nf; ++f) {
+                const T br = acc_re[base + f], bi = acc_im[base + f];
+                const float2 qv = qh[f * MF_RC + r];
+                sr += br * qv.x - bi * qv.y;
+                si += br * qv.y + bi * qv.x;
+            }
+            const int gv = first ? g.t_verts[tv0 + row] : g.t_verts[sv0 + row - nvI];
+            if (sr != T(0) || si != T(0)) red_add_cx(&g.b[(size_t)(r0 + r) * g.N + gv], (double)sr, (double)si);
+        }
     }
 }
 
@@ -549,9 +649,8 @@ template <typename T> struct SingArgs {
     const double *normals;    // F x 3
     const double *curls;      // F x 9
     Cx<T> *A;
-    Cx<T> *B;
+    RhsOut<T> rhs;
     int64_t ld;
-    int F;
     int64_t npairs;
     double k, eta;
 };
@@ -644,7 +743,7 @@ __global__ void __launch_bounds__(256) singular_pairs_kernel(SingArgs<T> g) {
                 vr = acc[18 + 2 * i];
                 vi = acc[18 + 2 * i + 1];
             }
-        red_add_cx(&g.B[(int64_t)ft[a] * g.F + s], (T)(vr * jac), (T)(vi * jac));
+        rhs_add(g.rhs, ft[a], s, (T)(vr * jac), (T)(vi * jac));
     }
 }
 
@@ -669,9 +768,9 @@ template <typename T> struct ImgArgs {
     const int *faces;
     const double *normals, *curls;
     int Q, RI;
-    Cx<T> *A, *B;
+    Cx<T> *A;
+    RhsOut<T> rhs;
     int64_t ld;
-    int F;
     int64_t npairs;
     double k, eta;
     ImgXf xf;
@@ -788,23 +887,31 @@ __global__ void __launch_bounds__(256) image_delta_kernel(ImgArgs<T> g) {
                 vr = acc[18 + 2 * i];
                 vi = acc[18 + 2 * i + 1];
             }
-        red_add_cx(&g.B[(int64_t)ft[a] * g.F + s], (T)(vr * jac), (T)(vi * jac));
+        rhs_add(g.rhs, ft[a], s, (T)(vr * jac), (T)(vi * jac));
     }
 }
 
 // orbit row weights (p1_symmetry_orbit_weights, BeatEngineCore.jl:563-582):
 // the rows of A and B of vertices on a symmetry plane, times 2 per plane
+// (the rows of b instead of B in the matrix-free mode: b = B q is linear in B)
 template <typename T>
 __global__ void row_weight_kernel(const int *verts, const double *weights, int nw, Cx<T> *A, int64_t ld, int n,
-                                  Cx<T> *B, int F) {
+                                  RhsOut<T> rhs) {
     const int v = blockIdx.y;
     if (v >= nw) return;
     const int row = verts[v];
-    const T w = (T)weights[v];
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n + F; j += gridDim.x * blockDim.x) {
-        Cx<T> &e = j < n ? A[(int64_t)row * ld + j] : B[(int64_t)row * F + (j - n)];
-        e.re *= w;
-        e.im *= w;
+    const double w = weights[v];
+    const int cols = rhs.B ? rhs.F : rhs.R;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n + cols; j += gridDim.x * blockDim.x) {
+        if (j < n || rhs.B) {
+            Cx<T> &e = j < n ? A[(int64_t)row * ld + j] : rhs.B[(int64_t)row * rhs.F + (j - n)];
+            e.re *= (T)w;
+            e.im *= (T)w;
+        } else {
+            Cx<double> &e = rhs.b[(size_t)(j - n) * rhs.N + row];
+            e.re *= w;
+            e.im *= w;
+        }
     }
 }
 
@@ -813,7 +920,7 @@ __global__ void row_weight_kernel(const int *verts, const double *weights, int n
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void identity_kernel(const int *faces, const double *areas, int F, int Q, double eta, Cx<T> *A,
-                                int64_t ld, Cx<T> *B) {
+                                int64_t ld, RhsOut<T> rhs) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= F) return;
     const int ri = Q == 1 ? 0 : Q == 3 ? 1 : 2;
@@ -830,14 +937,26 @@ __global__ void identity_kernel(const int *faces, const double *areas, int F, in
     const int *fc = faces + 3 * f;
     for (int a = 0; a < 3; ++a) {
         for (int b = 0; b < 3; ++b) red_add(&A[(int64_t)fc[a] * ld + fc[b]].re, (T)(0.5 * blk[3 * a + b]));
-        red_add(&B[(int64_t)fc[a] * F + f].im, (T)(-0.5 * eta * col[a]));
+        rhs_add(rhs, fc[a], f, T(0), (T)(-0.5 * eta * col[a]));
     }
 }
 
 // ---------------------------------------------------------------------------
 // host driver
 // ---------------------------------------------------------------------------
-template <typename T, int Q> static void launch_regular(beat_b200_ctx *c, double k, double eta, int img) {
+template <typename T> static RhsOut<T> rhs_out(beat_b200_ctx *c, int R, const Cx<double> *q) {
+    RhsOut<T> o;
+    o.B = c->ws.rhs_cached ? c->ws.B.as<Cx<T>>() : nullptr;
+    o.q = q;
+    o.b = c->ws.b.as<Cx<double>>();
+    o.F = c->F;
+    o.N = c->V;
+    o.R = R;
+    return o;
+}
+
+template <typename T, int Q>
+static void launch_regular(beat_b200_ctx *c, double k, double eta, int img, int R, const Cx<double> *q) {
     RegArgs<T> g;
     const bool d = sizeof(T) == 8;
     g.qpts = (const T *)(d ? c->pos_qpts64.p : c->pos_qpts32.p);
@@ -855,7 +974,11 @@ template <typename T, int Q> static void launch_regular(beat_b200_ctx *c, double
     g.s_verts = c->trial_tiles.verts.as<int>();
     g.s_local = c->trial_tiles.local_vert.as<int>();
     g.A = c->ws.A.as<Cx<T>>();
-    g.B = c->ws.B.as<Cx<T>>();
+    g.B = c->ws.rhs_cached ? c->ws.B.as<Cx<T>>() : nullptr;
+    g.q = q;
+    g.b = c->ws.b.as<Cx<double>>();
+    g.N = c->V;
+    g.R = R;
     g.ld = c->ws.ld;
     g.F = c->F;
     g.k = (T)k;
@@ -874,7 +997,8 @@ template <typename T, int Q> static void launch_regular(beat_b200_ctx *c, double
 }
 
 // FP32 form: the symmetric kernel over unordered pairs of square tiles
-template <int Q> static void launch_sym(beat_b200_ctx *c, double k, double eta, int img) {
+template <int Q>
+static void launch_sym(beat_b200_ctx *c, double k, double eta, int img, int R, const Cx<double> *q) {
     RegArgs<float> g;
     g.qpts = c->pos_qpts32.as<float>();
     g.normal = c->pos_normal32.as<float>();
@@ -888,7 +1012,11 @@ template <int Q> static void launch_sym(beat_b200_ctx *c, double k, double eta, 
     g.t_local = c->sym_tiles.local_vert.as<int>();
     g.s_fstart = g.s_vstart = g.s_verts = g.s_local = nullptr;
     g.A = c->ws.A.as<Cx<float>>();
-    g.B = c->ws.B.as<Cx<float>>();
+    g.B = c->ws.rhs_cached ? c->ws.B.as<Cx<float>>() : nullptr;
+    g.q = q;
+    g.b = c->ws.b.as<Cx<double>>();
+    g.N = c->V;
+    g.R = R;
     g.ld = c->ws.ld;
     g.F = c->F;
     g.k = (float)k;
@@ -914,20 +1042,23 @@ template <typename T> static void assemble_t(beat_b200_ctx *c, double k, double 
     const int N = c->V, F = c->F;
     BB_CUDA(cudaEventRecord(c->ev[0], c->stream));
     BB_CUDA(cudaMemsetAsync(w.A.p, 0, (size_t)N * w.ld * sizeof(Cx<T>), c->stream));
-    BB_CUDA(cudaMemsetAsync(w.B.p, 0, (size_t)N * F * sizeof(Cx<T>), c->stream));
+    if (w.rhs_cached)
+        BB_CUDA(cudaMemsetAsync(w.B.p, 0, (size_t)N * F * sizeof(Cx<T>), c->stream));
+    else  // matrix-free: the kernels add into b directly
+        BB_CUDA(cudaMemsetAsync(w.b.p, 0, sizeof(Cx<double>) * (size_t)N * R, c->stream));
     BB_CUDA(cudaEventRecord(c->ev[8], c->stream));
     for (int img = -1; img < c->nimg; ++img) {  // the mesh itself, then one pass per symmetry image
         if (sizeof(T) == 4) {
             switch (c->Q) {
-                case 1: launch_sym<1>(c, k, eta, img); break;
-                case 3: launch_sym<3>(c, k, eta, img); break;
-                default: launch_sym<6>(c, k, eta, img); break;
+                case 1: launch_sym<1>(c, k, eta, img, R, q); break;
+                case 3: launch_sym<3>(c, k, eta, img, R, q); break;
+                default: launch_sym<6>(c, k, eta, img, R, q); break;
             }
         } else {
             switch (c->Q) {
-                case 1: launch_regular<T, 1>(c, k, eta, img); break;
-                case 3: launch_regular<T, 3>(c, k, eta, img); break;
-                default: launch_regular<T, 6>(c, k, eta, img); break;
+                case 1: launch_regular<T, 1>(c, k, eta, img, R, q); break;
+                case 3: launch_regular<T, 3>(c, k, eta, img, R, q); break;
+                default: launch_regular<T, 6>(c, k, eta, img, R, q); break;
             }
         }
     }
@@ -946,9 +1077,8 @@ template <typename T> static void assemble_t(beat_b200_ctx *c, double k, double 
         s.normals = c->d_normals.as<double>();
         s.curls = c->d_curls.as<double>();
         s.A = w.A.as<Cx<T>>();
-        s.B = w.B.as<Cx<T>>();
+        s.rhs = rhs_out<T>(c, R, q);
         s.ld = w.ld;
-        s.F = F;
         s.npairs = c->npairs;
         s.k = k;
         s.eta = eta;
@@ -973,9 +1103,8 @@ template <typename T> static void assemble_t(beat_b200_ctx *c, double k, double 
         d.Q = c->Q;
         d.RI = c->Q == 1 ? 0 : c->Q == 3 ? 1 : 2;
         d.A = w.A.as<Cx<T>>();
-        d.B = w.B.as<Cx<T>>();
+        d.rhs = rhs_out<T>(c, R, q);
         d.ld = w.ld;
-        d.F = F;
         d.npairs = c->nimg_pairs;
         d.k = k;
         d.eta = eta;
@@ -988,17 +1117,19 @@ template <typename T> static void assemble_t(beat_b200_ctx *c, double k, double 
     }
     BB_CUDA(cudaEventRecord(c->ev[2], c->stream));
     identity_kernel<T><<<(F + 255) / 256, 256, 0, c->stream>>>(c->d_faces.as<int>(), c->d_areas.as<double>(), F,
-                                                               c->Q, eta, w.A.as<Cx<T>>(), w.ld, w.B.as<Cx<T>>());
+                                                               c->Q, eta, w.A.as<Cx<T>>(), w.ld, rhs_out<T>(c, R, q));
     BB_CUDA(cudaGetLastError());
     if (c->nweighted > 0) {
         row_weight_kernel<T><<<dim3(32, c->nweighted), 256, 0, c->stream>>>(
             c->rw_vert.as<int>(), c->rw_weight.as<double>(), c->nweighted, w.A.as<Cx<T>>(), w.ld, N,
-            w.B.as<Cx<T>>(), F);
+            rhs_out<T>(c, R, q));
         BB_CUDA(cudaGetLastError());
     }
-    BB_CUDA(cudaMemsetAsync(w.b.p, 0, sizeof(Cx<double>) * (size_t)N * R, c->stream));
-    tall_gemm<T>(c->stream, c->sm_count, w.B.as<Cx<T>>(), F, N, F, reinterpret_cast<const double *>(q), w.b.as<double>(),
-                 R, 1.0);
+    if (w.rhs_cached) {
+        BB_CUDA(cudaMemsetAsync(w.b.p, 0, sizeof(Cx<double>) * (size_t)N * R, c->stream));
+        tall_gemm<T>(c->stream, c->sm_count, w.B.as<Cx<T>>(), F, N, F, reinterpret_cast<const double *>(q),
+                     w.b.as<double>(), R, 1.0);
+    }
     BB_CUDA(cudaEventRecord(c->ev[3], c->stream));
     if (ms_total || ms_singular) {
         BB_CUDA(cudaEventSynchronize(c->ev[3]));

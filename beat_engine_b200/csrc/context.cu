@@ -636,8 +636,24 @@ void set_mesh(beat_b200_ctx *c, int V, const double *verts, int F, const int32_t
 // ---------------------------------------------------------------------------
 // workspaces
 // ---------------------------------------------------------------------------
-void ensure_workspace(beat_b200_ctx *c, int precision, int R) {
+// exterior_use_rhs_operator, exterior_rhs_policy.jl:25-44: the system matrix
+// and the mapping are resident together, with 512 MiB for the transients
+int rhs_use_operator(int mode, int excitations, int64_t matrix_bytes, int64_t operator_bytes,
+                     int64_t available_bytes) {
+    if (mode != BEAT_B200_RHS_AUTO && mode != BEAT_B200_RHS_MATRIX_FREE && mode != BEAT_B200_RHS_CACHED) return -1;
+    if (mode == BEAT_B200_RHS_MATRIX_FREE) return 0;
+    if (excitations < 1) return 0;
+    if (mode == BEAT_B200_RHS_AUTO && excitations < 2) return 0;
+    const int64_t margin = 512ll << 20;
+    return operator_bytes > 0 && matrix_bytes >= 0 && matrix_bytes + operator_bytes + margin <= available_bytes;
+}
+
+void ensure_workspace(beat_b200_ctx *c, int precision, int R, int rhs_request) {
     BB_REQUIRE(c->F > 0, BEAT_B200_STATE, "no mesh: call beat_b200_set_mesh first");
+    BB_REQUIRE(rhs_request >= BEAT_B200_RHS_AUTO && rhs_request <= BEAT_B200_RHS_CACHED, BEAT_B200_INVALID_ARG,
+               "unknown right-hand-side mode");
+    BB_REQUIRE(!(c->adm_set && rhs_request == BEAT_B200_RHS_MATRIX_FREE), BEAT_B200_INVALID_ARG,
+               "an admittance needs the cached right-hand-side mapping B; the matrix-free mode was requested");
     Workspace &w = c->ws;
     const int N = c->V, F = c->F;
     const int64_t ld = ((int64_t)N + 127) / 128 * 128;
@@ -653,9 +669,33 @@ void ensure_workspace(beat_b200_ctx *c, int precision, int R) {
     w.N = N;
     w.F = F;
     w.ld = ld;
+    // the mode: free device memory plus what this context's matrix buffers hold
+    const int64_t matrix_bytes = (int64_t)N * ld * (int64_t)csz * (precision == BEAT_B200_FP64 ? 1 : 2);
+    const int64_t operator_bytes = (int64_t)N * F * (int64_t)csz;
+    size_t free_b = 0, total_b = 0;
+    BB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const int64_t available = (int64_t)free_b + (int64_t)(w.A.bytes + w.Aop.bytes + w.B.bytes);
+    bool cached;
+    if (c->adm_set) {
+        cached = true;  // the admittance term A += B diag(a) P needs B
+        BB_REQUIRE(rhs_use_operator(BEAT_B200_RHS_CACHED, std::max(R, 1), matrix_bytes, operator_bytes, available) ==
+                       1,
+                   BEAT_B200_OOM, "an admittance needs the right-hand-side mapping B, which does not fit in memory");
+    } else {
+        cached = rhs_use_operator(rhs_request, R, matrix_bytes, operator_bytes, available) == 1;
+    }
+    if (!cached) w.B.free_();
     w.A.alloc((size_t)N * ld * csz);
     if (precision != BEAT_B200_FP64) w.Aop.alloc((size_t)N * ld * csz);
-    w.B.alloc((size_t)N * F * csz);
+    if (cached) {
+        try {
+            w.B.alloc((size_t)N * F * csz);
+        } catch (const Error &e) {
+            if (e.code != BEAT_B200_OOM || c->adm_set) throw;
+            cached = false;  // the mapping did not fit after all: integrate the columns instead
+        }
+    }
+    w.rhs_cached = cached ? 1 : 0;
     if (R > w.R || !w.b.p) {
         w.R = std::max(R, 1);
         w.b.free_();

@@ -122,6 +122,7 @@ struct Workspace {
     DevBuf io;            // device staging of the host-buffer entry points (grow-only)
     DevBuf qeff;          // Neumann data with the admittance term, for the field (grow-only)
     DevBuf grad;          // field gradient: near (point, face) pairs and error word (grow-only)
+    int rhs_cached = 1;   // B (N x F) assembled and resident, else matrix-free right-hand sides
     int solve_epoch = 0;  // flag value of the latest substitution launch
     int lu_valid = 0;     // factors match the current operator
 };
@@ -216,7 +217,12 @@ namespace bb {
 // context.cu
 void set_mesh(beat_b200_ctx *c, int V, const double *verts, int F, const int32_t *faces,
               int quad_order, int sing_order);
-void ensure_workspace(beat_b200_ctx *c, int precision, int R);
+// allocates the per-solve buffers and decides the right-hand-side mode
+// (BEAT_B200_RHS_*) for the next assembly: ws.rhs_cached
+void ensure_workspace(beat_b200_ctx *c, int precision, int R, int rhs_request = BEAT_B200_RHS_AUTO);
+// exterior_use_rhs_operator: 1 cached, 0 matrix-free, -1 unknown mode
+int rhs_use_operator(int mode, int excitations, int64_t matrix_bytes, int64_t operator_bytes,
+                     int64_t available_bytes);
 void release_workspace(beat_b200_ctx *c);
 int64_t device_bytes(const beat_b200_ctx *c);
 int read_status(beat_b200_ctx *c);

@@ -69,6 +69,23 @@ typedef struct {
  * GMRES refinement (diagnostics; the result is then FP32-LU accurate only) */
 #define BEAT_B200_FLAG_NO_REFINE 1
 
+/* Right-hand-side modes (exterior_rhs_policy.jl:15-44).  Cached: the P1 x DP0
+ * mapping B (N x F) is assembled with the system and b = B q is one tall
+ * product; B stays resident for the admittance term and the adjoint.
+ * Matrix-free: the element-pair kernels add B-tile x q straight into b, so
+ * no N x F array exists; unlike the reference's matrix_free path (one pair
+ * integration per excitation) this is one pass for every column.  Auto: the
+ * reference's rule, cached from two excitations on when the system matrix,
+ * B and a 512 MiB margin fit in the free device memory plus what the context
+ * already holds; an admittance always needs B.  If B cannot be allocated the
+ * solve falls back to matrix-free, as the reference does. */
+#define BEAT_B200_RHS_AUTO 0
+#define BEAT_B200_RHS_MATRIX_FREE 1
+#define BEAT_B200_RHS_CACHED 2
+/* opts.flags bits 1-2 request a mode (both clear = auto, both set = invalid) */
+#define BEAT_B200_FLAG_RHS_MATRIX_FREE 2
+#define BEAT_B200_FLAG_RHS_CACHED 4
+
 typedef struct {
     double assembly_ms;     /* regular + singular + identity + RHS */
     double singular_ms;     /* Duffy pass alone (part of assembly_ms) */
@@ -85,7 +102,8 @@ typedef struct {
     int32_t precision;
     int32_t lu_block;
     int32_t lu_split_terms;
-    int32_t reserved;
+    int32_t rhs_mode;       /* BEAT_B200_RHS_MATRIX_FREE or _CACHED: the mode that ran (the
+                               mapping then held N x F x 8 (mixed) or 16 (FP64) bytes) */
 } beat_b200_diag;
 
 /* ABI check: returns BEAT_B200_ABI_VERSION. */
@@ -163,6 +181,14 @@ int32_t beat_b200_assemble(beat_b200_ctx *ctx, double k_signed, double eta_im, i
 /* Free the per-solve workspaces (system matrix, factors, Krylov vectors);
  * the mesh stays.  The next solve reallocates them. */
 int32_t beat_b200_release_workspace(beat_b200_ctx *ctx);
+
+/* exterior_use_rhs_operator (exterior_rhs_policy.jl:31-44): 1 when the
+ * cached mapping is used for `excitations` right-hand sides with a system
+ * matrix of matrix_bytes, a mapping of operator_bytes and available_bytes of
+ * device memory, 0 when matrix-free, -1 for an unknown mode.  Pure host
+ * logic: needs no device and no context. */
+int32_t beat_b200_rhs_use_operator(int32_t mode, int32_t excitations, int64_t matrix_bytes,
+                                   int64_t operator_bytes, int64_t available_bytes);
 
 /* Bytes of device memory the context holds right now. */
 int64_t beat_b200_device_bytes(const beat_b200_ctx *ctx);
