@@ -30,7 +30,7 @@ EXPORTS = (
     "beat_b200_release_workspace", "beat_b200_device_bytes", "beat_b200_stream", "beat_b200_resolve_noalloc",
     "beat_b200_sweep", "beat_b200_sweep_device", "beat_b200_set_admittance", "beat_b200_adjoint",
     "beat_b200_set_symmetry", "beat_b200_field_gradient", "beat_b200_field_gradient_device",
-    "beat_b200_rhs_use_operator",
+    "beat_b200_rhs_use_operator", "beat_b200_assemble_coupled_device", "beat_b200_coupled_blocks_device",
 )
 
 SYMMETRY_MODES = {"off": 0, "x": 1, "xy": 2, "ground": 3}
@@ -121,6 +121,11 @@ def load(path: str = LIB_PATH):
     L.beat_b200_farfield_device.restype = i32
     L.beat_b200_rhs_use_operator.argtypes = [i32, i32, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64]
     L.beat_b200_rhs_use_operator.restype = i32
+    L.beat_b200_assemble_coupled_device.argtypes = [vp, f64, i32, vp, vp]
+    L.beat_b200_assemble_coupled_device.restype = i32
+    L.beat_b200_coupled_blocks_device.argtypes = [vp, i32, vp, i32, vp, vp, vp, ctypes.c_int64, vp, i32, vp, vp,
+                                                  i32, vp, vp]
+    L.beat_b200_coupled_blocks_device.restype = i32
     L.beat_b200_field_gradient.argtypes = [vp, f64, i32, dp, i32, dp, dp, dp]
     L.beat_b200_field_gradient.restype = i32
     L.beat_b200_field_gradient_device.argtypes = [vp, f64, i32, dp, i32, vp, vp, vp]
@@ -260,6 +265,23 @@ class Context:
 
     def field(self, k_signed, points, p, q):
         return self._eval(self.lib.beat_b200_field, k_signed, points, p, q)
+
+    def assemble_coupled_device(self, k_signed: float, precision: int, d_a_ptr: int, d_c_ptr: int):
+        """beat_b200_assemble_coupled_device: A (N x N) and C (N x F), column-major,
+        into device buffers (complex64 in the mixed form, complex128 in FP64)."""
+        self._check(self.lib.beat_b200_assemble_coupled_device(self.handle, float(k_signed), precision,
+                                                               ctypes.c_void_p(d_a_ptr), ctypes.c_void_p(d_c_ptr)))
+
+    def coupled_blocks_device(self, precision: int, d_c_ptr: int, ncols: int, d_colptr: int, d_rowval: int,
+                              d_nzval: int, nnz: int, d_interface: int, nmotion: int = 0, d_motion: int = 0,
+                              d_motion_out: int = 0, nprescribed: int = 0, d_prescribed: int = 0,
+                              d_prescribed_out: int = 0):
+        """beat_b200_coupled_blocks_device: C Q (CSC, 1-based), C motion, -C prescribed."""
+        v = ctypes.c_void_p
+        self._check(self.lib.beat_b200_coupled_blocks_device(
+            self.handle, precision, v(d_c_ptr), ncols, v(d_colptr), v(d_rowval), v(d_nzval), int(nnz),
+            v(d_interface), nmotion, v(d_motion), v(d_motion_out), nprescribed, v(d_prescribed),
+            v(d_prescribed_out)))
 
     def field_gradient(self, k_signed, points, p, q):
         """Pressure and gradient at points: M x 4 x R complex128 (value, d/dx,

@@ -407,6 +407,21 @@ int32_t beat_b200_field_gradient_device(beat_b200_ctx *c, double k, int32_t M, c
     });
 }
 
+int32_t beat_b200_assemble_coupled_device(beat_b200_ctx *c, double k, int32_t precision, void *d_A, void *d_C) {
+    return guarded(c, [&] { assemble_coupled(c, k, precision, d_A, d_C); });
+}
+
+int32_t beat_b200_coupled_blocks_device(beat_b200_ctx *c, int32_t precision, const void *d_C, int32_t ncols,
+                                        const int32_t *d_colptr, const int32_t *d_rowval, const void *d_nzval,
+                                        int64_t nnz, void *d_interface, int32_t nmotion, const void *d_motion,
+                                        void *d_motion_out, int32_t nprescribed, const void *d_prescribed,
+                                        void *d_prescribed_out) {
+    return guarded(c, [&] {
+        coupled_blocks(c, precision, d_C, ncols, d_colptr, d_rowval, d_nzval, nnz, d_interface, nmotion, d_motion,
+                       d_motion_out, nprescribed, d_prescribed, d_prescribed_out);
+    });
+}
+
 int32_t beat_b200_rhs_use_operator(int32_t mode, int32_t excitations, int64_t matrix_bytes, int64_t operator_bytes,
                                    int64_t available_bytes) {
     return rhs_use_operator(mode, excitations, matrix_bytes, operator_bytes, available_bytes);

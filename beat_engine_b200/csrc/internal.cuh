@@ -270,6 +270,13 @@ IrResult gmres_refine_adjoint(beat_b200_ctx *c, int R, double *x_dev, const doub
 // field.cu
 void farfield(beat_b200_ctx *c, double k, int M, const double *dirs_host, int R, const double *p_dev,
               const double *q_dev, double *out_dev, bool far);
+// coupled.cu: the coupled FEM-BEM path's combined operators (column-major
+// device buffers; element type by precision) and their block products
+void assemble_coupled(beat_b200_ctx *c, double k, int precision, void *d_A, void *d_C);
+void coupled_blocks(beat_b200_ctx *c, int precision, const void *d_C, int ncols, const int *colptr,
+                    const int *rowval, const void *nzval, int64_t nnz, void *d_interface, int nm,
+                    const void *d_motion, void *d_motion_out, int np, const void *d_prescribed,
+                    void *d_prescribed_out);
 // pressure and its gradient, M x 4 x R complex (value, d/dx, d/dy, d/dz)
 void field_gradient(beat_b200_ctx *c, double k, int M, const double *pts_host, int R, const double *p_dev,
                     const double *q_dev, double *out_dev);

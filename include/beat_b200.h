@@ -182,6 +182,34 @@ int32_t beat_b200_assemble(beat_b200_ctx *ctx, double k_signed, double eta_im, i
  * the mesh stays.  The next solve reallocates them. */
 int32_t beat_b200_release_workspace(beat_b200_ctx *ctx);
 
+/* Coupled FEM-BEM combined BEM operators, replacing
+ * assemble_coupled_burton_miller_cuda (src/BeatEngineCudaCoupledBurtonMiller.jl:
+ * 537-593): A = 1/2 M - D + alpha H (N x N) and C = S + alpha (K' + 1/2 M_p1dp0)
+ * (N x F), alpha = i / k_signed (burton_miller_coupling), with the context's
+ * symmetry images and orbit row weights; no admittance term (the coupled
+ * path's admittance lives on the FEM side).  Written column-major into the
+ * caller's device buffers d_A and d_C (either may be NULL), complex float in
+ * the mixed form (FP32 regular quadrature, FP64 touching pairs) or complex
+ * double in the FP64 form.  Overwrites the context's system (a later adjoint
+ * needs a new solve). */
+int32_t beat_b200_assemble_coupled_device(beat_b200_ctx *ctx, double k_signed, int32_t precision,
+                                          void *d_A, void *d_C);
+
+/* build_cuda_combined_bem_blocks (src/BeatEngineCudaCoupledBurtonMiller.jl:
+ * 595-640) on a column-major C (N x F) from beat_b200_assemble_coupled_device:
+ * interface = C Q for the F x ncols sparse interface map Q in CSC form
+ * (colptr: ncols + 1 entries, rowval / nzval: nnz entries, 1-based as Julia
+ * stores them), motion_out = C motion (F x nmotion), prescribed_out =
+ * -C prescribed (F x nprescribed).  All device buffers, column-major, of the
+ * precision's complex type; an index outside the map gives
+ * BEAT_B200_INVALID_ARG. */
+int32_t beat_b200_coupled_blocks_device(beat_b200_ctx *ctx, int32_t precision, const void *d_C,
+                                        int32_t ncols, const int32_t *d_colptr,
+                                        const int32_t *d_rowval, const void *d_nzval, int64_t nnz,
+                                        void *d_interface, int32_t nmotion, const void *d_motion,
+                                        void *d_motion_out, int32_t nprescribed,
+                                        const void *d_prescribed, void *d_prescribed_out);
+
 /* exterior_use_rhs_operator (exterior_rhs_policy.jl:31-44): 1 when the
  * cached mapping is used for `excitations` right-hand sides with a system
  * matrix of matrix_bytes, a mapping of operator_bytes and available_bytes of
