@@ -31,6 +31,7 @@ EXPORTS = (
     "beat_b200_sweep", "beat_b200_sweep_device", "beat_b200_set_admittance", "beat_b200_adjoint",
     "beat_b200_set_symmetry", "beat_b200_field_gradient", "beat_b200_field_gradient_device",
     "beat_b200_rhs_use_operator", "beat_b200_assemble_coupled_device", "beat_b200_coupled_blocks_device",
+    "beat_b200_adjoint_shape",
 )
 
 SYMMETRY_MODES = {"off": 0, "x": 1, "xy": 2, "ground": 3}
@@ -121,6 +122,8 @@ def load(path: str = LIB_PATH):
     L.beat_b200_farfield_device.restype = i32
     L.beat_b200_rhs_use_operator.argtypes = [i32, i32, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64]
     L.beat_b200_rhs_use_operator.restype = i32
+    L.beat_b200_adjoint_shape.argtypes = [vp, f64, i32, dp, i32, dp, dp, dp, ctypes.POINTER(Opts), dp, dp, dp]
+    L.beat_b200_adjoint_shape.restype = i32
     L.beat_b200_assemble_coupled_device.argtypes = [vp, f64, i32, vp, vp]
     L.beat_b200_assemble_coupled_device.restype = i32
     L.beat_b200_coupled_blocks_device.argtypes = [vp, i32, vp, i32, vp, vp, vp, ctypes.c_int64, vp, i32, vp, vp,
@@ -378,6 +381,24 @@ class Context:
                                                ctypes.byref(opts) if opts is not None else None, _dp(w),
                                                _dp(ga) if ga is not None else None))
         return w, ga
+
+    def adjoint_shape(self, k_signed: float, dirs, p, q, g, opts: Opts | None = None):
+        """beat_b200_adjoint_shape: (dJ/d conj(q0): F x R, dJ/d conj(a): F,
+        dJ/dX: V x 3) after a solve at k_signed with Neumann data q."""
+        dd = np.ascontiguousarray(dirs, dtype=np.float64).reshape(-1, 3)
+        M = dd.shape[0]
+        pf, qf = _c128_f(p, self.V), _c128_f(q, self.F)
+        R = pf.shape[1]
+        gf = _c128_f(g, M)
+        if gf.shape[1] != R or qf.shape[1] != R:
+            raise ValueError("p, q and g need the same number of columns")
+        w = np.zeros((self.F, R), dtype=np.complex128, order="F")
+        ga = np.zeros(self.F, dtype=np.complex128)
+        gx = np.zeros((self.V, 3), dtype=np.float64)
+        self._check(self.lib.beat_b200_adjoint_shape(self.handle, float(k_signed), M, _dp(dd), R, _dp(pf), _dp(qf),
+                                                     _dp(gf), ctypes.byref(opts) if opts is not None else None,
+                                                     _dp(w), _dp(ga), _dp(gx)))
+        return w, ga, gx
 
     def release_workspace(self):
         self._check(self.lib.beat_b200_release_workspace(self.handle))

@@ -15,7 +15,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbeatb200.so")
-SOURCES = ["context.cu", "assembly.cu", "lu.cu", "tc_gemm.cu", "gmres.cu", "field.cu", "adjoint.cu", "coupled.cu", "abi.cu",
+SOURCES = ["context.cu", "assembly.cu", "lu.cu", "tc_gemm.cu", "gmres.cu", "field.cu", "adjoint.cu", "coupled.cu", "shape.cu", "abi.cu",
            "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -108,6 +108,7 @@ void solve_core(beat_b200_ctx *c, double k, double eta, int R, const double *d_q
     BB_CUDA(cudaEventRecord(c->ev[5], c->stream));
     const int st = read_status(c);
     c->last_k = k;
+    c->last_eta = eta;
     BB_REQUIRE(!(st & DEV_BARRIER_TIMEOUT), BEAT_B200_TIMEOUT, "LU panel: grid barrier ran out of its wait budget");
     BB_REQUIRE(!(st & DEV_ZERO_PIVOT), BEAT_B200_SINGULAR, "LU: exact zero pivot (singular system)");
     IrResult ir{0, 1, 0.0};
@@ -614,6 +615,45 @@ int32_t beat_b200_adjoint(beat_b200_ctx *c, double k_signed, int32_t M, const do
         BB_REQUIRE(ir.converged, BEAT_B200_NOT_CONVERGED,
                    "adjoint refinement missed its tolerance (worst relative residual " + std::to_string(ir.residual) +
                        ")");
+    });
+}
+
+int32_t beat_b200_adjoint_shape(beat_b200_ctx *c, double k_signed, int32_t M, const double *dirs, int32_t R,
+                                const double *p, const double *q, const double *g, const beat_b200_opts *opts,
+                                double *w_out, double *ga_out, double *gX_out) {
+    return guarded(c, [&] {
+        BB_REQUIRE(dirs && p && q && g && gX_out, BEAT_B200_INVALID_ARG, "adjoint: null pointer");
+        BB_REQUIRE(c->F > 0, BEAT_B200_STATE, "no mesh: call beat_b200_set_mesh first");
+        BB_REQUIRE(M >= 1 && R >= 1, BEAT_B200_INVALID_ARG, "adjoint: M and R must be >= 1");
+        BB_REQUIRE(c->nimg == 0, BEAT_B200_STATE, "shape gradient: symmetry images are not supported");
+        const beat_b200_opts o = resolve_opts(opts);
+        const int N = c->V, F = c->F;
+        const size_t np = (size_t)N * R, ng = (size_t)M * R, nw = (size_t)F * R;
+        DevBuf &io = c->ws.io;
+        // p, q, g, w, ga (complex), then gX (3N) and the directions (3M), doubles
+        io.alloc(sizeof(double2) * (np + 2 * nw + ng + F) + sizeof(double) * (3 * (size_t)N + 3 * (size_t)M));
+        double2 *dp = io.as<double2>(), *dq = dp + np, *dg = dq + nw, *dw = dg + ng, *dga = dw + nw;
+        double *dgx = reinterpret_cast<double *>(dga + F), *ddirs = dgx + 3 * (size_t)N;
+        BB_CUDA(cudaMemcpyAsync(dp, p, sizeof(double2) * np, cudaMemcpyHostToDevice, c->stream));
+        BB_CUDA(cudaMemcpyAsync(dq, q, sizeof(double2) * nw, cudaMemcpyHostToDevice, c->stream));
+        BB_CUDA(cudaMemcpyAsync(dg, g, sizeof(double2) * ng, cudaMemcpyHostToDevice, c->stream));
+        BB_CUDA(cudaMemcpyAsync(ddirs, dirs, sizeof(double) * 3 * M, cudaMemcpyHostToDevice, c->stream));
+        IrResult ir{0, 1, 0.0};
+        const double *z = nullptr;
+        adjoint(c, k_signed, M, dirs, R, (const double *)dp, (const double *)dg, (double *)dw, (double *)dga, o, &ir,
+                &z);
+        BB_REQUIRE(ir.converged, BEAT_B200_NOT_CONVERGED,
+                   "adjoint refinement missed its tolerance (worst relative residual " + std::to_string(ir.residual) +
+                       ")");
+        // the boundary's Neumann data: q0 - diag(a) P p with an admittance
+        c->ws.qeff.alloc(sizeof(double2) * nw);
+        effective_neumann(c, R, (const double *)dp, (const double *)dq, c->ws.qeff.as<double>());
+        shape_gradient(c, k_signed, c->last_eta, M, ddirs, R, (const double *)dp, c->ws.qeff.as<double>(),
+                       (const double *)dg, z, dgx);
+        if (w_out) BB_CUDA(cudaMemcpyAsync(w_out, dw, sizeof(double2) * nw, cudaMemcpyDeviceToHost, c->stream));
+        if (ga_out) BB_CUDA(cudaMemcpyAsync(ga_out, dga, sizeof(double2) * F, cudaMemcpyDeviceToHost, c->stream));
+        BB_CUDA(cudaMemcpyAsync(gX_out, dgx, sizeof(double) * 3 * (size_t)N, cudaMemcpyDeviceToHost, c->stream));
+        BB_CUDA(cudaStreamSynchronize(c->stream));
     });
 }
 

@@ -371,7 +371,8 @@ void lu_solve_adjoint(beat_b200_ctx *c, int R, const double *in, double *out) {
 // the adjoint driver
 // ---------------------------------------------------------------------------
 void adjoint(beat_b200_ctx *c, double k, int M, const double *dirs_host, int R, const double *p_dev,
-             const double *g_dev, double *w_dev, double *ga_dev, const beat_b200_opts &o, IrResult *ir) {
+             const double *g_dev, double *w_dev, double *ga_dev, const beat_b200_opts &o, IrResult *ir,
+             const double **z_out) {
     Workspace &w = c->ws;
     BB_REQUIRE(w.lu_valid, BEAT_B200_STATE, "adjoint: no factorisation on this context (solve first)");
     BB_REQUIRE(w.rhs_cached, BEAT_B200_STATE,
@@ -441,6 +442,7 @@ void adjoint(beat_b200_ctx *c, double k, int M, const double *dirs_host, int R, 
     BB_CUDA(cudaStreamSynchronize(c->stream));
     const int st = read_status(c);
     BB_REQUIRE(!(st & DEV_ZERO_PIVOT), BEAT_B200_SINGULAR, "adjoint: zero pivot in the factors");
+    if (z_out) *z_out = reinterpret_cast<const double *>(z);  // stays valid until the next use of ws.field
 }
 
 }  // namespace bb

@@ -188,6 +188,7 @@ struct beat_b200_ctx {
     bb::DevBuf adm;               // F complex FP64 coefficients a_f
     bool adm_set = false;
     double last_k = 0.0;          // signed wavenumber of the factors in the workspace
+    double last_eta = 0.0;        // Burton-Miller coupling (imaginary part) of that solve
 
     // singular (touching) pairs
     int64_t npairs = 0;
@@ -259,7 +260,13 @@ void apply_admittance_lhs(beat_b200_ctx *c, int precision);  // A += B diag(a) P
 void effective_neumann(beat_b200_ctx *c, int R, const double *p_dev, const double *q_dev, double *q_eff);
 void lu_solve_adjoint(beat_b200_ctx *c, int R, const double *in, double *out);  // out = A^-H in (stored factors)
 void adjoint(beat_b200_ctx *c, double k, int M, const double *dirs_host, int R, const double *p_dev,
-             const double *g_dev, double *w_dev, double *ga_dev, const beat_b200_opts &o, IrResult *ir);
+             const double *g_dev, double *w_dev, double *ga_dev, const beat_b200_opts &o, IrResult *ir,
+             const double **z_out = nullptr);
+// shape.cu: gradient with respect to the vertices (V x 3) from the adjoint
+// solution z, the solve's p, its effective Neumann data q and g (device)
+void shape_gradient(beat_b200_ctx *c, double k, double eta, int M, const double *dirs_dev, int R,
+                    const double *p_dev, const double *q_dev, const double *g_dev, const double *z_dev,
+                    double *gX_dev);
 // gmres.cu: Y (cols x R) += alpha M^H X (X: rows x R); M complex row-major rows x cols
 template <typename T>
 void tall_gemm_h(cudaStream_t st, int sm_count, const Cx<T> *M, int64_t ld, int rows, int cols, const double *X,

@@ -297,6 +297,19 @@ int32_t beat_b200_adjoint(beat_b200_ctx *ctx, double k_signed, int32_t M, const 
                           int32_t R, const double *p, const double *g, const beat_b200_opts *opts,
                           double *w_out, double *ga_out);
 
+/* beat_b200_adjoint plus the gradient with respect to the vertex positions:
+ * gX_out (V x 3 doubles, the layout of set_mesh's vertices) is dJ/dX of the
+ * same real functional, by reverse-mode differentiation of the discrete
+ * assembly (regular and Duffy element pairs, identity), the far field and,
+ * with an admittance, its Neumann term.  q is the Neumann data (F x R) of the
+ * last solve, which the shape derivative needs besides p; w_out and ga_out
+ * are as in beat_b200_adjoint and may be NULL.  Symmetry images are not
+ * supported (BEAT_B200_STATE).  No counterpart in the reference. */
+int32_t beat_b200_adjoint_shape(beat_b200_ctx *ctx, double k_signed, int32_t M, const double *dirs,
+                                int32_t R, const double *p, const double *q, const double *g,
+                                const beat_b200_opts *opts, double *w_out, double *ga_out,
+                                double *gX_out);
+
 /* The CUDA stream (cudaStream_t) every kernel of this context is launched
  * on, so a caller can order its own work or record timing events on it.
  * Entry points return only after their work on it has completed. */
