@@ -1187,21 +1187,6 @@ __global__ void __launch_bounds__(256) offdiag_product_kernel(const Cx<T> *A, in
     }
 }
 
-// out[2] (+)= M[r, :] V[:, c..c+1] over a 64 x 64 shared tile (row stride SBP)
-// and a 64 x SRC shared block
-__device__ __forceinline__ void tile_rows_times_block(const Cx<double> *M, const Cx<double> *V, int r, int c,
-                                                      double *o_re, double *o_im) {
-#pragma unroll 16
-    for (int q = 0; q < SB; ++q) {
-        const Cx<double> m = M[r * SBP + q];
-        const Cx<double> v0 = V[q * SRC + c], v1 = V[q * SRC + c + 1];
-        o_re[0] += m.re * v0.re - m.im * v0.im;
-        o_im[0] += m.re * v0.im + m.im * v0.re;
-        o_re[1] += m.re * v1.re - m.im * v1.im;
-        o_im[1] += m.re * v1.im + m.im * v1.re;
-    }
-}
-
 // Block substitution in one kernel.  The solution is cut into 64-row blocks;
 // each CTA claims the next block from a counter (so it only ever waits on
 // blocks already claimed by running CTAs).  For block b it folds in
@@ -1210,7 +1195,28 @@ __device__ __forceinline__ void tile_rows_times_block(const Cx<double> *M, const
 // being solved, and then X_b = Z_b - H_b X_neighbour: one 64 x 64 x R product
 // on the critical path per block.  Waits are bounded: on expiry the kernel
 // sets a status bit and continues, so it always terminates.
-constexpr int SUBST_THREADS = 512;
+//
+// Arithmetic is in the factors' type: FP64 for the FP64 form, FP32 for the
+// mixed form's factors (there the substitution is the preconditioner of the
+// FP64 refinement).  The folded-in products are shared by NG warp groups of
+// 128 threads (4 for FP32, 2 for FP64), group g taking steps g, g + NG, ...
+// with its own factor tile (cp.async, zero-filled past the matrix edge) and
+// X block, synchronised by its own named barrier, so that one SM always has
+// several independent tile products in flight; each thread keeps a 2-row x
+// 4-column block of the 64 x 16 product in registers.  The groups' partial
+// sums meet in shared memory and group 0 finishes the block.
+template <typename T> struct SubstTile {
+    // padded row length: rows start on 16-byte boundaries (cp.async) and a
+    // warp's 8 rows fall on distinct banks
+    static constexpr int LP = SB + (sizeof(Cx<T>) == 16 ? 1 : 2);
+    // the X block column-major with a padded column: the loads (consecutive
+    // rows) and the product's reads (four columns at one row) spread over banks
+    static constexpr int XP = SB + 1;
+    static constexpr int NG = sizeof(Cx<T>) == 16 ? 2 : 4;
+    static constexpr int THREADS = 128 * NG;
+    static constexpr int GROUP = SB * LP + SRC * XP;  // complex entries per group
+    static constexpr size_t smem() { return sizeof(Cx<T>) * (size_t)NG * GROUP; }
+};
 
 __device__ __forceinline__ bool wait_flag(const int *flag, int epoch, int *status, unsigned spin_limit) {
     unsigned it = 0;
@@ -1225,98 +1231,170 @@ __device__ __forceinline__ bool wait_flag(const int *flag, int epoch, int *statu
     }
 }
 
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, int src_bytes) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+// barrier of one 128-thread warp group (ids 1.. ; 0 is __syncthreads)
+__device__ __forceinline__ void group_bar(int grp) {
+    asm volatile("bar.sync %0, 128;" ::"r"(grp + 1) : "memory");
+}
+
+// acc[2][4] += M[rows rp, rp + 32][:] V[:][4 cg .. 4 cg + 3], V column-major
+// with column stride XP
+template <typename C, int LP, int XP>
+__device__ __forceinline__ void subst_product(const Cx<C> *M, const Cx<C> *V, int rp, int cg, C (&ar)[2][4],
+                                              C (&ai)[2][4]) {
+#pragma unroll 8
+    for (int q = 0; q < SB; ++q) {
+        const Cx<C> m0 = M[rp * LP + q], m1 = M[(rp + 32) * LP + q];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const Cx<C> v = V[(4 * cg + e) * XP + q];
+            ar[0][e] += m0.re * v.re - m0.im * v.im;
+            ai[0][e] += m0.re * v.im + m0.im * v.re;
+            ar[1][e] += m1.re * v.re - m1.im * v.im;
+            ai[1][e] += m1.re * v.im + m1.im * v.re;
+        }
+    }
+}
+
 template <typename T, bool LOWER>
-__global__ void __launch_bounds__(SUBST_THREADS) block_subst_kernel(const Cx<T> *A, int64_t ld, int n,
-                                                                    const Cx<double> *Dinv, double2 *X, int R,
-                                                                    int r0, int *counter, int *flags, int epoch,
-                                                                    int *status, unsigned spin_limit) {
+__global__ void __launch_bounds__(SubstTile<T>::THREADS, 1) block_subst_kernel(const Cx<T> *A, int64_t ld, int n,
+                                                                           const Cx<double> *Dinv, double2 *X, int R,
+                                                                           int r0, int *counter, int *flags,
+                                                                           int epoch, int *status,
+                                                                           unsigned spin_limit) {
+    using C = T;
+    using ST = SubstTile<T>;
+    constexpr int LP = ST::LP, XP = ST::XP, NG = ST::NG;
+    constexpr int CH = 16 / sizeof(Cx<T>);  // complex entries per 16-byte chunk
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Cx<double> *Lt = reinterpret_cast<Cx<double> *>(smem_raw);  // SB x SBP: off-diagonal tile
-    Cx<double> *Dt = Lt + SB * SBP;                               // SB x SBP: D_b^-1
-    Cx<double> *Ht = Dt + SB * SBP;                               // SB x SBP: H_b
-    Cx<double> *Xj = Ht + SB * SBP;                               // SB x SRC
+    Cx<C> *base = reinterpret_cast<Cx<C> *>(smem_raw);
     __shared__ int s_blk;
     const int nblk = (n + SB - 1) / SB;
     if (threadIdx.x == 0) s_blk = atomicAdd(counter, 1);
     __syncthreads();
     const int claim = s_blk;
     if (claim >= nblk) return;
+    const int tid = threadIdx.x, grp = tid >> 7, gt = tid & 127;
+    Cx<C> *Lg = base + (size_t)grp * ST::GROUP;  // this group's factor tile [SB][LP]
+    Cx<C> *Xg = Lg + SB * LP;                    // this group's X block [SRC][XP]
     const int b = LOWER ? claim : nblk - 1 - claim;
     const int rb = b * SB, rows = min(SB, n - rb);
     const int rc = min(SRC, R - r0);
-    const int r = threadIdx.x >> 3, c = (threadIdx.x & 7) * 2;  // row, first of 2 columns
-    // independent of every other block: D_b^-1, H_b and B_b
+    const int rp = gt >> 2, cg = gt & 3;  // rows rp, rp + 32; columns 4 cg .. 4 cg + 3
+    // the factor tile of block row b, block column j, into dst (cp.async)
+    auto issue_tile = [&](int j, Cx<C> *dst) {
+        const int cj = j * SB, cols = min(SB, n - cj);
+        for (int i = gt; i < SB * (SB / CH); i += 128) {
+            const int a = i / (SB / CH), q = (i % (SB / CH)) * CH;
+            const int valid = (a < rows) ? max(0, min(CH, cols - q)) : 0;
+            const Cx<T> *src = valid > 0 ? A + (int64_t)(rb + a) * ld + cj + q : A;
+            cp_async16(dst + a * LP + q, src, valid * (int)sizeof(Cx<T>));
+        }
+        cp_async_commit();
+    };
+    // X_j (FP64, columns r0 .. r0 + rc) into dst in the compute type
+    auto load_x = [&](int j, Cx<C> *dst) {
+        const int cj = j * SB, cols = min(SB, n - cj);
+        for (int i = gt; i < SB * SRC; i += 128) {
+            const int q = i / SB, a = i % SB;  // consecutive threads: consecutive rows of one column
+            const double2 v = (a < cols && q < rc) ? __ldcg(&X[(size_t)(r0 + q) * n + cj + a]) : make_double2(0, 0);
+            dst[q * XP + a] = Cx<C>{(C)v.x, (C)v.y};
+        }
+    };
+    // an FP64 64 x 64 block (D_b^-1 or H_b) into dst in the compute type
+    auto load_block = [&](const Cx<double> *src, Cx<C> *dst) {
+        for (int i = gt; i < SB * SB; i += 128) {
+            const Cx<double> v = src[i];
+            dst[(i / SB) * LP + i % SB] = Cx<C>{(C)v.re, (C)v.im};
+        }
+    };
+    C ar[2][4], ai[2][4];
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) ar[h][e] = ai[h][e] = C(0);
+    // every finished block except the neighbour, shared round-robin by the groups
+    const int nsteps = claim > 1 ? claim - 1 : 0;
+    for (int step = grp; step < nsteps; step += NG) {
+        const int j = LOWER ? step : nblk - 1 - step;
+        issue_tile(j, Lg);
+        if (gt == 0) wait_flag(flags + j, epoch, status, spin_limit);
+        group_bar(grp);
+        load_x(j, Xg);
+        cp_async_wait_all();
+        group_bar(grp);
+        subst_product<C, LP, XP>(Lg, Xg, rp, cg, ar, ai);
+        group_bar(grp);
+    }
+    // the groups' partial sums meet in shared memory (each in its own X block)
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) Xg[(4 * cg + e) * XP + rp + 32 * h] = Cx<C>{ar[h][e], ai[h][e]};
+    __syncthreads();
+    if (grp != 0) return;  // group 0 finishes the block; only group barriers from here on
+    Cx<C> *X0 = Xg, *D0 = Lg, *H0 = base + ST::GROUP;  // group 1's tile holds H_b
     const Cx<double> *Di = Dinv + ((size_t)(LOWER ? 0 : 1) * nblk + b) * SB * SB;
     const Cx<double> *Hi = Dinv + ((size_t)(LOWER ? 2 : 3) * nblk + b) * SB * SB;
-    batched_copy<SUBST_THREADS, 8, Cx<double>>(SB * SB, [&](int i) { return Di[i]; },
-                                                [&](int i, Cx<double> v) { Dt[(i / SB) * SBP + i % SB] = v; });
-    batched_copy<SUBST_THREADS, 8, Cx<double>>(SB * SB, [&](int i) { return Hi[i]; },
-                                                [&](int i, Cx<double> v) { Ht[(i / SB) * SBP + i % SB] = v; });
-    double acc_re[2] = {0, 0}, acc_im[2] = {0, 0};
-    double b_re[2], b_im[2];
+    load_block(Di, D0);
+    load_block(Hi, H0);
+    // Z_b = D_b^-1 (B_b - sum of the partials)
 #pragma unroll
-    for (int e = 0; e < 2; ++e) {
-        double2 v = make_double2(0, 0);
-        if (r < rows && c + e < rc) v = X[(size_t)(r0 + c + e) * n + rb + r];
-        b_re[e] = v.x;
-        b_im[e] = v.y;
-    }
-    auto load_x = [&](int j) {
-        const int cj = j * SB, cols = min(SB, n - cj);
-        batched_copy<SUBST_THREADS, 2, double2>(
-            SB * SRC,
-            [&](int i) {
-                const int q = i / SB, a = i % SB;  // consecutive threads: consecutive rows of one column
-                return (a < cols && q < rc) ? __ldcg(&X[(size_t)(r0 + q) * n + cj + a]) : make_double2(0, 0);
-            },
-            [&](int i, double2 v) { Xj[(i % SB) * SRC + i / SB] = Cx<double>{v.x, v.y}; });
-    };
-    // all finished blocks except the neighbour
-    for (int step = 0; step + 1 < claim; ++step) {
-        const int j = LOWER ? step : nblk - 1 - step;
-        const int cj = j * SB, cols = min(SB, n - cj);
-        batched_copy<SUBST_THREADS, 8, Cx<double>>(
-            SB * SB,
-            [&](int i) {
-                const int a = i / SB, q = i % SB;
-                return (a < rows && q < cols) ? to_d(A[(int64_t)(rb + a) * ld + cj + q]) : Cx<double>{0.0, 0.0};
-            },
-            [&](int i, Cx<double> v) { Lt[(i / SB) * SBP + i % SB] = v; });
-        if (threadIdx.x == 0) wait_flag(flags + j, epoch, status, spin_limit);
-        __syncthreads();
-        load_x(j);
-        __syncthreads();
-        tile_rows_times_block(Lt, Xj, r, c, acc_re, acc_im);
-        __syncthreads();
-    }
-    // Z_b = D_b^-1 (B_b - acc)
+    for (int h = 0; h < 2; ++h)
 #pragma unroll
-    for (int e = 0; e < 2; ++e) Xj[r * SRC + c + e] = Cx<double>{b_re[e] - acc_re[e], b_im[e] - acc_im[e]};
-    __syncthreads();
-    double z_re[2] = {0, 0}, z_im[2] = {0, 0};
-    tile_rows_times_block(Dt, Xj, r, c, z_re, z_im);
-    __syncthreads();
+        for (int e = 0; e < 4; ++e) {
+            const int r = rp + 32 * h, cc = 4 * cg + e;
+            C sr = C(0), si = C(0);
+#pragma unroll
+            for (int g = 0; g < NG; ++g) {
+                const Cx<C> v = base[(size_t)g * ST::GROUP + SB * LP + cc * XP + r];
+                sr += v.re;
+                si += v.im;
+            }
+            double2 v = make_double2(0, 0);
+            if (r < rows && cc < rc) v = X[(size_t)(r0 + cc) * n + rb + r];
+            X0[cc * XP + r] = Cx<C>{(C)v.x - sr, (C)v.y - si};
+            ar[h][e] = ai[h][e] = C(0);
+        }
+    group_bar(0);
+    subst_product<C, LP, XP>(D0, X0, rp, cg, ar, ai);
+    group_bar(0);
     if (claim > 0) {
         // X_b = Z_b - H_b X_neighbour
         const int jn = LOWER ? b - 1 : b + 1;
-        if (threadIdx.x == 0) wait_flag(flags + jn, epoch, status, spin_limit);
-        __syncthreads();
-        load_x(jn);
-        __syncthreads();
-        double h_re[2] = {0, 0}, h_im[2] = {0, 0};
-        tile_rows_times_block(Ht, Xj, r, c, h_re, h_im);
+        if (gt == 0) wait_flag(flags + jn, epoch, status, spin_limit);
+        group_bar(0);
+        load_x(jn, X0);
+        group_bar(0);
+        C hr[2][4], hi[2][4];
 #pragma unroll
-        for (int e = 0; e < 2; ++e) {
-            z_re[e] -= h_re[e];
-            z_im[e] -= h_im[e];
-        }
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) hr[h][e] = hi[h][e] = C(0);
+        subst_product<C, LP, XP>(H0, X0, rp, cg, hr, hi);
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                ar[h][e] -= hr[h][e];
+                ai[h][e] -= hi[h][e];
+            }
     }
 #pragma unroll
-    for (int e = 0; e < 2; ++e)
-        if (r < rows && c + e < rc) X[(size_t)(r0 + c + e) * n + rb + r] = make_double2(z_re[e], z_im[e]);
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int r = rp + 32 * h, cc = 4 * cg + e;
+            if (r < rows && cc < rc) X[(size_t)(r0 + cc) * n + rb + r] = make_double2(ar[h][e], ai[h][e]);
+        }
     __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(flags + b), "r"(epoch) : "memory");
+    group_bar(0);
+    if (gt == 0) asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(flags + b), "r"(epoch) : "memory");
 }
 
 template <typename T> static void diag_inverses(beat_b200_ctx *c) {
@@ -1343,7 +1421,7 @@ template <typename T> static void lu_solve_t(beat_b200_ctx *c, int R, const doub
     int *counter = w.small_solve.as<int>();
     int *flags = counter + 32;
     if (w.solve_epoch == 0) BB_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * nblk, c->stream));
-    const size_t smem = sizeof(Cx<double>) * (3 * SB * SBP + SB * SRC);
+    const size_t smem = SubstTile<T>::smem();
     BB_CUDA(cudaFuncSetAttribute(block_subst_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     BB_CUDA(cudaFuncSetAttribute(block_subst_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     permute_rows_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(reinterpret_cast<const double2 *>(in), X,
@@ -1354,10 +1432,10 @@ template <typename T> static void lu_solve_t(beat_b200_ctx *c, int R, const doub
             const int epoch = ++w.solve_epoch;
             BB_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), c->stream));
             if (pass == 0)
-                block_subst_kernel<T, true><<<nblk, SUBST_THREADS, smem, c->stream>>>(
+                block_subst_kernel<T, true><<<nblk, SubstTile<T>::THREADS, smem, c->stream>>>(
                     A, w.ld, n, Dinv, X, R, r0, counter, flags, epoch, c->status.as<int>(), 1u << 22);
             else
-                block_subst_kernel<T, false><<<nblk, SUBST_THREADS, smem, c->stream>>>(
+                block_subst_kernel<T, false><<<nblk, SubstTile<T>::THREADS, smem, c->stream>>>(
                     A, w.ld, n, Dinv, X, R, r0, counter, flags, epoch, c->status.as<int>(), 1u << 22);
         }
     }
@@ -1398,7 +1476,7 @@ static void lu_resolve_into_t(beat_b200_ctx *c, int R, const double *b, double *
     int *counter = scratch;
     int *flags = scratch + 32;
     BB_CUDA(cudaMemsetAsync(scratch, 0, sizeof(int) * (size_t)(nblk + 32), c->stream));
-    const size_t smem = sizeof(Cx<double>) * (3 * SB * SBP + SB * SRC);
+    const size_t smem = SubstTile<T>::smem();
     BB_CUDA(cudaFuncSetAttribute(block_subst_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     BB_CUDA(cudaFuncSetAttribute(block_subst_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     permute_rows_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(reinterpret_cast<const double2 *>(b), X,
@@ -1410,10 +1488,10 @@ static void lu_resolve_into_t(beat_b200_ctx *c, int R, const double *b, double *
             ++epoch;
             BB_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), c->stream));
             if (pass == 0)
-                block_subst_kernel<T, true><<<nblk, SUBST_THREADS, smem, c->stream>>>(
+                block_subst_kernel<T, true><<<nblk, SubstTile<T>::THREADS, smem, c->stream>>>(
                     A, w.ld, n, Dinv, X, R, r0, counter, flags, epoch, c->status.as<int>(), 1u << 22);
             else
-                block_subst_kernel<T, false><<<nblk, SUBST_THREADS, smem, c->stream>>>(
+                block_subst_kernel<T, false><<<nblk, SubstTile<T>::THREADS, smem, c->stream>>>(
                     A, w.ld, n, Dinv, X, R, r0, counter, flags, epoch, c->status.as<int>(), 1u << 22);
         }
     }
