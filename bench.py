@@ -381,21 +381,23 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "fallback"}
 
 
-# DRAM traffic of regular_pairs_kernel<float, 6> measured by ncu on the F = 5,120 icosphere
-# (profiles/regular_pairs_kernel_F5120.md): dram read + write bytes per launch and the
-# algorithmic output of that launch (A: N^2 c64, B: N x F c64).  Traffic grows with the output
-# written (the zeroed A and B are read back by the red.global.add flush), so a launch on another
-# mesh is scaled by its output bytes.
-REGULAR_TRAFFIC_F5120 = {"bytes": 158.676736e6 + 112.227840e6, "output_bytes": 2562 * 2562 * 8 + 2562 * 5120 * 8}
+# DRAM traffic of sym_pairs_kernel<6> (the mixed form's element-pair kernel) measured by ncu on
+# the F = 5,120 icosphere (profiles/sym_pairs_kernel_F5120.md): dram read + write bytes per launch
+# and the algorithmic output of that launch (A: N^2 c64, B: N x F c64).  Traffic grows with the
+# output written (the zeroed A and B are read back by the red.global.add flush), so a launch on
+# another mesh is scaled by its output bytes.
+SYM_TRAFFIC_F5120 = {"bytes": 158.947328e6 + 120.576256e6, "output_bytes": 2562 * 2562 * 8 + 2562 * 5120 * 8}
 
 
 def roofline(args, mesh, stages, peaks):
-    """Roofline of the regular element-pair assembly kernel (the dominant
-    kernel of the step).  achieved = algorithmic bytes per launch / its
-    CUDA-event duration; algorithmic bytes = the output it produces, A (N^2)
-    and the RHS operator B (N x F), c64 entries in the mixed form, c128 in
-    FP64.  The kernel is bound by FP32 FMA/SFU issue, not HBM: the compute
-    fraction is reported beside it."""
+    """Roofline of the element-pair assembly kernel (the dominant kernel of
+    the step: sym_pairs_kernel in the mixed form, regular_pairs_kernel in
+    FP64).  achieved = algorithmic bytes per launch / its CUDA-event
+    duration; algorithmic bytes = the output it produces, A (N^2) and the RHS
+    operator B (N x F), c64 entries in the mixed form, c128 in FP64.  The
+    kernel is bound by FP32 FMA/SFU issue, not HBM: the compute fraction
+    (72 flops per ordered point pair, the algorithmic count) is reported
+    beside it."""
     F, N = mesh.num_faces, mesh.num_vertices
     esz = 16 if args.precision == "fp64" else 8
     regular_pairs = F * F - (13 * F - 60)
@@ -406,10 +408,12 @@ def roofline(args, mesh, stages, peaks):
     peak = peaks["hbm_gbs"]
     traffic = None
     if esz == 8:
-        traffic = REGULAR_TRAFFIC_F5120["bytes"] * alg_bytes / REGULAR_TRAFFIC_F5120["output_bytes"]
+        traffic = SYM_TRAFFIC_F5120["bytes"] * alg_bytes / SYM_TRAFFIC_F5120["output_bytes"]
     flops = point_pairs * 72.0
     fp_peak = 148 * 128 * 2 * 1.965e9 / (2 if args.precision == "fp64" else 1)
-    return {"kernel": "regular_pairs_kernel (element-pair Galerkin assembly)", "bound": "hbm",
+    kernel = ("regular_pairs_kernel<double, 6> (element-pair Galerkin assembly)" if esz == 16 else
+              "sym_pairs_kernel<6> (element-pair Galerkin assembly, both orders per unordered pair)")
+    return {"kernel": kernel, "bound": "hbm",
             "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": (achieved / peak) if achieved else None, "traffic": traffic,
             "traffic_basis": "ncu dram read+write of the F=5,120 launch scaled by output bytes" if traffic else None,
