@@ -1147,18 +1147,19 @@ __global__ void __launch_bounds__(SB) diag_inverse_kernel(const Cx<T> *A, int64_
     for (int i = 0; i < SB; ++i) out[i * SB + c] = X[i][c];
 }
 
-// H_b = D_b^-1 M_b for the block next to the diagonal on the solve's
-// critical path: M_b = L[b, b-1] (lower, blockIdx.y = 0) or U[b, b+1] (upper,
-// blockIdx.y = 1).  With it, X_b = Z_b - H_b X_{b-1 or b+1}, where Z_b is
-// everything else and can be formed while the neighbouring block is solved.
+// H_b^(d) = D_b^-1 M_b for the two blocks nearest the diagonal on the solve's
+// critical path: M_b = L[b, b-d] (lower) or U[b, b+d] (upper), d = 1, 2
+// (blockIdx.y = 2 (d - 1) + upper; stored in slot 2 + blockIdx.y).  With them,
+// X_b = Z_b - H^(2)_b X_{b-+2} - H^(1)_b X_{b-+1}, where Z_b holds everything
+// else and is formed while the two neighbouring blocks are solved.
 template <typename T>
 __global__ void __launch_bounds__(256) offdiag_product_kernel(const Cx<T> *A, int64_t ld, int n, Cx<double> *Dinv) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cx<double> *Dt = reinterpret_cast<Cx<double> *>(smem_raw);  // SB x SBP
     Cx<double> *Mt = Dt + SB * SBP;                               // SB x SBP
-    const int nblk = gridDim.x, b = blockIdx.x, upper = blockIdx.y;
-    const int nb2 = upper ? b + 1 : b - 1;
-    Cx<double> *H = Dinv + ((size_t)(2 + upper) * nblk + b) * SB * SB;
+    const int nblk = gridDim.x, b = blockIdx.x, upper = blockIdx.y & 1, dist = 1 + (blockIdx.y >> 1);
+    const int nb2 = upper ? b + dist : b - dist;
+    Cx<double> *H = Dinv + ((size_t)(2 + blockIdx.y) * nblk + b) * SB * SB;
     if (nb2 < 0 || nb2 >= nblk) {
         for (int i = threadIdx.x; i < SB * SB; i += blockDim.x) H[i] = Cx<double>{0.0, 0.0};
         return;
@@ -1190,11 +1191,12 @@ __global__ void __launch_bounds__(256) offdiag_product_kernel(const Cx<T> *A, in
 // Block substitution in one kernel.  The solution is cut into 64-row blocks;
 // each CTA claims the next block from a counter (so it only ever waits on
 // blocks already claimed by running CTAs).  For block b it folds in
-// L_bj X_j (or U_bj X_j) for every finished block j other than the
-// neighbour, forms Z_b = D_b^-1 (B_b - that sum) while the neighbour is still
-// being solved, and then X_b = Z_b - H_b X_neighbour: one 64 x 64 x R product
-// on the critical path per block.  Waits are bounded: on expiry the kernel
-// sets a status bit and continues, so it always terminates.
+// L_bj X_j (or U_bj X_j) for every finished block j at distance 3 or more,
+// forms Z_b = D_b^-1 (B_b - that sum), subtracts H^(2)_b X_{b-+2} once that
+// block is done, and then X_b = Z_b - H^(1)_b X_{b-+1}: the chain from one
+// block to the next is a single 64 x 64 x R product, run by the whole CTA.
+// Waits are bounded: on expiry the kernel sets a status bit and continues, so
+// it always terminates.
 //
 // Arithmetic is in the factors' type: FP64 for the FP64 form, FP32 for the
 // mixed form's factors (there the substitution is the preconditioner of the
@@ -1204,7 +1206,7 @@ __global__ void __launch_bounds__(256) offdiag_product_kernel(const Cx<T> *A, in
 // X block, synchronised by its own named barrier, so that one SM always has
 // several independent tile products in flight; each thread keeps a 2-row x
 // 4-column block of the 64 x 16 product in registers.  The groups' partial
-// sums meet in shared memory and group 0 finishes the block.
+// sums meet in shared memory for the tail.
 template <typename T> struct SubstTile {
     // padded row length: rows start on 16-byte boundaries (cp.async) and a
     // warp's 8 rows fall on distinct banks
@@ -1318,8 +1320,8 @@ __global__ void __launch_bounds__(SubstTile<T>::THREADS, 1) block_subst_kernel(c
     for (int h = 0; h < 2; ++h)
 #pragma unroll
         for (int e = 0; e < 4; ++e) ar[h][e] = ai[h][e] = C(0);
-    // every finished block except the neighbour, shared round-robin by the groups
-    const int nsteps = claim > 1 ? claim - 1 : 0;
+    // every finished block at distance >= 3, shared round-robin by the groups
+    const int nsteps = claim > 2 ? claim - 2 : 0;
     for (int step = grp; step < nsteps; step += NG) {
         const int j = LOWER ? step : nblk - 1 - step;
         issue_tile(j, Lg);
@@ -1337,18 +1339,72 @@ __global__ void __launch_bounds__(SubstTile<T>::THREADS, 1) block_subst_kernel(c
 #pragma unroll
         for (int e = 0; e < 4; ++e) Xg[(4 * cg + e) * XP + rp + 32 * h] = Cx<C>{ar[h][e], ai[h][e]};
     __syncthreads();
-    if (grp != 0) return;  // group 0 finishes the block; only group barriers from here on
-    Cx<C> *X0 = Xg, *D0 = Lg, *H0 = base + ST::GROUP;  // group 1's tile holds H_b
+
+    // tail, the whole CTA.  Thread tid owns rows tr, tr + 32 and columns tc,
+    // tc + 1 of the 64 x 16 block; with 512 threads the 64-term sums are split
+    // between the two lanes of a pair (even and odd terms, so that the pair's
+    // loads fall on distinct banks) and combined by one shuffle.
+    constexpr int THREADS = ST::THREADS, QS = THREADS / 256;  // lanes per 2 x 2 block
+    const int tile = tid / QS, qh = tid % QS;
+    const int tr = tile >> 3, tc = (tile & 7) * 2;
+    Cx<C> *T0 = base, *T1 = base + ST::GROUP;  // groups 0 and 1's tiles
+    // H^(1)_b: group 2's tile when there is one (loaded with D and H^(2)),
+    // else group 0's after the D product
+    Cx<C> *TH1 = NG >= 3 ? base + 2 * ST::GROUP : T0;
+    Cx<C> *X0 = base + SB * LP;                // group 0's X block
+    auto load_block_all = [&](const Cx<double> *src, Cx<C> *dst) {
+        for (int i = tid; i < SB * SB; i += THREADS) {
+            const Cx<double> v = src[i];
+            dst[(i / SB) * LP + i % SB] = Cx<C>{(C)v.re, (C)v.im};
+        }
+    };
+    auto load_x_all = [&](int j) {
+        const int cj = j * SB, cols = min(SB, n - cj);
+        for (int i = tid; i < SB * SRC; i += THREADS) {
+            const int q = i / SB, a = i % SB;
+            const double2 v = (a < cols && q < rc) ? __ldcg(&X[(size_t)(r0 + q) * n + cj + a]) : make_double2(0, 0);
+            X0[q * XP + a] = Cx<C>{(C)v.x, (C)v.y};
+        }
+    };
+    // o[h][e] = M[tr + 32 h, :] X0[:, tc + e]
+    auto tail_product = [&](const Cx<C> *M, C (&orr)[2][2], C (&oi)[2][2]) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) orr[h][e] = oi[h][e] = C(0);
+#pragma unroll 8
+        for (int i = 0; i < SB / QS; ++i) {
+            const int q = QS * i + qh;
+            const Cx<C> m0 = M[tr * LP + q], m1 = M[(tr + 32) * LP + q];
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const Cx<C> v = X0[(tc + e) * XP + q];
+                orr[0][e] += m0.re * v.re - m0.im * v.im;
+                oi[0][e] += m0.re * v.im + m0.im * v.re;
+                orr[1][e] += m1.re * v.re - m1.im * v.im;
+                oi[1][e] += m1.re * v.im + m1.im * v.re;
+            }
+        }
+        if (QS == 2) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    orr[h][e] += __shfl_xor_sync(0xffffffffu, orr[h][e], 1);
+                    oi[h][e] += __shfl_xor_sync(0xffffffffu, oi[h][e], 1);
+                }
+        }
+    };
     const Cx<double> *Di = Dinv + ((size_t)(LOWER ? 0 : 1) * nblk + b) * SB * SB;
-    const Cx<double> *Hi = Dinv + ((size_t)(LOWER ? 2 : 3) * nblk + b) * SB * SB;
-    load_block(Di, D0);
-    load_block(Hi, H0);
-    // Z_b = D_b^-1 (B_b - sum of the partials)
+    const Cx<double> *H1 = Dinv + ((size_t)(LOWER ? 2 : 3) * nblk + b) * SB * SB;
+    const Cx<double> *H2 = Dinv + ((size_t)(LOWER ? 4 : 5) * nblk + b) * SB * SB;
+    // B_b - sum of the partials
+    C vr[2][2], vi[2][2];
 #pragma unroll
     for (int h = 0; h < 2; ++h)
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const int r = rp + 32 * h, cc = 4 * cg + e;
+        for (int e = 0; e < 2; ++e) {
+            const int r = tr + 32 * h, cc = tc + e;
             C sr = C(0), si = C(0);
 #pragma unroll
             for (int g = 0; g < NG; ++g) {
@@ -1358,54 +1414,79 @@ __global__ void __launch_bounds__(SubstTile<T>::THREADS, 1) block_subst_kernel(c
             }
             double2 v = make_double2(0, 0);
             if (r < rows && cc < rc) v = X[(size_t)(r0 + cc) * n + rb + r];
-            X0[cc * XP + r] = Cx<C>{(C)v.x - sr, (C)v.y - si};
-            ar[h][e] = ai[h][e] = C(0);
+            vr[h][e] = (C)v.x - sr;
+            vi[h][e] = (C)v.y - si;
         }
-    group_bar(0);
-    subst_product<C, LP, XP>(D0, X0, rp, cg, ar, ai);
-    group_bar(0);
-    if (claim > 0) {
-        // X_b = Z_b - H_b X_neighbour
-        const int jn = LOWER ? b - 1 : b + 1;
-        if (gt == 0) wait_flag(flags + jn, epoch, status, spin_limit);
-        group_bar(0);
-        load_x(jn, X0);
-        group_bar(0);
-        C hr[2][4], hi[2][4];
+    __syncthreads();  // partials read: the groups' buffers are free
+    if (qh == 0)
 #pragma unroll
         for (int h = 0; h < 2; ++h)
 #pragma unroll
-            for (int e = 0; e < 4; ++e) hr[h][e] = hi[h][e] = C(0);
-        subst_product<C, LP, XP>(H0, X0, rp, cg, hr, hi);
+            for (int e = 0; e < 2; ++e) X0[(tc + e) * XP + tr + 32 * h] = Cx<C>{vr[h][e], vi[h][e]};
+    load_block_all(Di, T0);
+    if (claim >= 2) load_block_all(H2, T1);
+    if (NG >= 3 && claim >= 1) load_block_all(H1, TH1);
+    __syncthreads();
+    // Z_b = D_b^-1 (B_b - sum)
+    C zr[2][2], zi[2][2], hr[2][2], hi[2][2];
+    tail_product(T0, zr, zi);
+    __syncthreads();  // T0 and X0 free
+    if (NG < 3 && claim >= 1) load_block_all(H1, TH1);  // overlaps the waits below
+    auto subtract = [&]() {
 #pragma unroll
         for (int h = 0; h < 2; ++h)
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                ar[h][e] -= hr[h][e];
-                ai[h][e] -= hi[h][e];
+            for (int e = 0; e < 2; ++e) {
+                zr[h][e] -= hr[h][e];
+                zi[h][e] -= hi[h][e];
             }
+    };
+    if (claim >= 2) {
+        // Z_b -= H^(2)_b X_{b-+2}
+        if (tid == 0) wait_flag(flags + (LOWER ? b - 2 : b + 2), epoch, status, spin_limit);
+        __syncthreads();
+        load_x_all(LOWER ? b - 2 : b + 2);
+        __syncthreads();
+        tail_product(T1, hr, hi);
+        subtract();
+        __syncthreads();  // X0 free
     }
+    if (claim >= 1) {
+        // X_b = Z_b - H^(1)_b X_{b-+1}
+        if (tid == 0) wait_flag(flags + (LOWER ? b - 1 : b + 1), epoch, status, spin_limit);
+        __syncthreads();
+        load_x_all(LOWER ? b - 1 : b + 1);
+        __syncthreads();
+        tail_product(TH1, hr, hi);
+        subtract();
+    }
+    {  // lane qh of a pair stores row tr + 32 qh (with one lane per block, both rows)
 #pragma unroll
-    for (int h = 0; h < 2; ++h)
+        for (int h = 0; h < 2; ++h) {
+            if (QS == 2 && h != qh) continue;
+            const int r = tr + 32 * h;
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const int r = rp + 32 * h, cc = 4 * cg + e;
-            if (r < rows && cc < rc) X[(size_t)(r0 + cc) * n + rb + r] = make_double2(ar[h][e], ai[h][e]);
+            for (int e = 0; e < 2; ++e)
+                if (r < rows && tc + e < rc)
+                    X[(size_t)(r0 + tc + e) * n + rb + r] = make_double2(zr[h][e], zi[h][e]);
         }
-    __threadfence();
-    group_bar(0);
-    if (gt == 0) asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(flags + b), "r"(epoch) : "memory");
+    }
+    // the CTA barrier orders every thread's stores before thread 0's release
+    // (release is cumulative), and consumers acquire the flag before a barrier
+    // and their loads
+    __syncthreads();
+    if (tid == 0) asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(flags + b), "r"(epoch) : "memory");
 }
 
 template <typename T> static void diag_inverses(beat_b200_ctx *c) {
     Workspace &w = c->ws;
     const int n = c->V, nblk = (n + SB - 1) / SB;
-    w.dinv.alloc(sizeof(Cx<double>) * 4 * (size_t)nblk * SB * SB);
+    w.dinv.alloc(sizeof(Cx<double>) * 6 * (size_t)nblk * SB * SB);  // D (L, U), H^(1) (L, U), H^(2) (L, U)
     const size_t smem = 2 * sizeof(Cx<double>) * SB * SBP;
     BB_CUDA(cudaFuncSetAttribute(diag_inverse_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     diag_inverse_kernel<T><<<dim3(nblk, 2), SB, smem, c->stream>>>(w.A.as<Cx<T>>(), w.ld, n, w.dinv.as<Cx<double>>());
     BB_CUDA(cudaFuncSetAttribute(offdiag_product_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    offdiag_product_kernel<T><<<dim3(nblk, 2), 256, smem, c->stream>>>(w.A.as<Cx<T>>(), w.ld, n,
+    offdiag_product_kernel<T><<<dim3(nblk, 4), 256, smem, c->stream>>>(w.A.as<Cx<T>>(), w.ld, n,
                                                                      w.dinv.as<Cx<double>>());
     BB_CUDA(cudaGetLastError());
 }
