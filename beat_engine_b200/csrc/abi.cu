@@ -159,7 +159,10 @@ void solve_core(beat_b200_ctx *c, double k, double eta, int R, const double *d_q
 // ---------------------------------------------------------------------------
 // frequency sweep over solve lanes
 // ---------------------------------------------------------------------------
-constexpr int SWEEP_LANES = 2;
+// lanes per sweep: measured on B200 at F = 20,480, R = 16, mixed form (24
+// frequencies, mean of three runs): 2 lanes 10.3, 3 lanes 10.7, 4 lanes 11.2,
+// 6 lanes 10.9 freq-solves/s
+constexpr int SWEEP_LANES = 4;
 
 // lane i of c (lane 0 is c itself); created on first use with c's mesh
 beat_b200_ctx *sweep_lane(beat_b200_ctx *c, int i) {
@@ -178,11 +181,45 @@ beat_b200_ctx *sweep_lane(beat_b200_ctx *c, int i) {
     return c->lanes[i - 1];
 }
 
+static int64_t held_matrix_bytes(const beat_b200_ctx *l) {
+    return (int64_t)(l->ws.A.bytes + l->ws.Aop.bytes + l->ws.B.bytes);
+}
+
+// How many lanes to run: up to SWEEP_LANES, as many as there are frequencies,
+// and only as many as can hold a system matrix (with the FP32 operator copy in
+// the mixed form, and the N x F mapping when the right-hand sides may be
+// cached) beside a 512 MiB margin in the free device memory; buffers a lane
+// already holds count as available.  Lane 0 always runs.
+static int sweep_lane_count(beat_b200_ctx *c, int nfreq, const beat_b200_opts &o, int R) {
+    const int want = std::min(SWEEP_LANES, nfreq);
+    if (want <= 1) return 1;
+    const int64_t ld = ((int64_t)c->V + 127) / 128 * 128;
+    const bool fp64 = o.precision == BEAT_B200_FP64;
+    const int64_t csz = fp64 ? 16 : 8;
+    const int req = rhs_request(o);
+    const bool may_cache =
+        c->adm_set || req == BEAT_B200_RHS_CACHED || (req == BEAT_B200_RHS_AUTO && R >= 2);
+    const int64_t per_lane = (int64_t)c->V * ld * csz * (fp64 ? 1 : 2) +
+                             (may_cache ? (int64_t)c->V * c->F * csz : 0) + (512ll << 20);
+    size_t free_b = 0, total_b = 0;
+    BB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    int64_t avail = (int64_t)free_b - std::max<int64_t>(0, per_lane - held_matrix_bytes(c));
+    int lanes = 1;
+    for (int i = 1; i < want; ++i) {
+        const beat_b200_ctx *l = i - 1 < (int)c->lanes.size() ? c->lanes[i - 1] : nullptr;
+        const int64_t need = std::max<int64_t>(0, per_lane - (l ? held_matrix_bytes(l) : 0));
+        if (need > avail) break;
+        avail -= need;
+        ++lanes;
+    }
+    return lanes;
+}
+
 // Runs work(lane_ctx, f) for f = 0..nfreq-1, frequency f on lane f % L, one
 // host thread per lane (lane 0 on the calling thread).  The first error (by
 // frequency) is rethrown after every lane has stopped.
-template <typename W> void run_sweep(beat_b200_ctx *c, int nfreq, W &&work) {
-    const int L = std::min(SWEEP_LANES, nfreq);
+template <typename W> void run_sweep(beat_b200_ctx *c, int nfreq, int lanes, W &&work) {
+    const int L = std::max(1, std::min(lanes, nfreq));
     std::vector<beat_b200_ctx *> lane(L);
     for (int i = 0; i < L; ++i) lane[i] = sweep_lane(c, i);
     for (int i = 1; i < L; ++i) {  // the lanes solve with this context's admittance
@@ -504,7 +541,7 @@ int32_t beat_b200_sweep_device(beat_b200_ctx *c, int32_t nfreq, const double *k_
         BB_REQUIRE(c->F > 0, BEAT_B200_STATE, "no mesh: call beat_b200_set_mesh first");
         const beat_b200_opts o = resolve_opts(opts);
         const size_t qs = (size_t)c->F * R * 2, ps = (size_t)c->V * R * 2, fs = (size_t)M * R * 2;
-        run_sweep(c, nfreq, [&](beat_b200_ctx *l, int f) {
+        run_sweep(c, nfreq, sweep_lane_count(c, nfreq, o, R), [&](beat_b200_ctx *l, int f) {
             const double *q = (const double *)d_q + f * qs;
             double *p = (double *)d_p + f * ps;
             solve_core(l, k_signed[f], eta_im[f], R, q, o, p, diags ? diags + f : nullptr);
@@ -524,7 +561,7 @@ int32_t beat_b200_sweep(beat_b200_ctx *c, int32_t nfreq, const double *k_signed,
         BB_REQUIRE(c->F > 0, BEAT_B200_STATE, "no mesh: call beat_b200_set_mesh first");
         const beat_b200_opts o = resolve_opts(opts);
         const size_t qs = (size_t)c->F * R * 2, ps = (size_t)c->V * R * 2, fs = (size_t)M * R * 2;
-        run_sweep(c, nfreq, [&](beat_b200_ctx *l, int f) {
+        run_sweep(c, nfreq, sweep_lane_count(c, nfreq, o, R), [&](beat_b200_ctx *l, int f) {
             ensure_workspace(l, o.precision, R, rhs_request(o));
             Workspace &w = l->ws;
             BB_CUDA(cudaMemcpyAsync(w.q.p, q + f * qs, qs * sizeof(double), cudaMemcpyHostToDevice, l->stream));

@@ -14,7 +14,7 @@ for all R.
 
 ``value``: device-timed throughput with q already in HBM: the K timed steps
 (frequencies) run as one beat_b200_sweep_device call, which pipelines them over
-two solve lanes (one frequency's assembly beside another's factorisation).
+up to four solve lanes (one frequency's assembly beside another's factorisation).
 ``e2e``: the same through the host C-ABI sweep (beat_b200_sweep) from pinned
 host buffers.  ``stages_ms`` are one frequency solved alone.
 
@@ -187,7 +187,7 @@ def config_dict(args, mesh):
             "precision_form": args.precision, "lu_split_terms": args.split,
             "l2": "inputs larger than L2: every step rewrites A (N^2 complex) and the N x F RHS operator",
             "parallelism": f"frequency replicas x{args.gpus} (no collective); "
-                           "2 solve lanes per GPU (pipelined frequency sweep)"}
+                           "up to 4 solve lanes per GPU (pipelined frequency sweep)"}
 
 
 # --------------------------------------------------------------------------
@@ -272,7 +272,7 @@ def run_gpu(args):
         torch.cuda.synchronize()
         e0.record(stream)
         sweep_diags = sweep(timed)
-        # the sweep returns after both lanes finished: this event follows all of its work
+        # the sweep returns after every lane finished: this event follows all of its work
         e1.record(stream)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
