@@ -211,7 +211,7 @@ def run_gpu(args):
     import torch
     import torch.distributed as dist
 
-    from beat_engine_b200 import _lib
+    from beat_engine_b200 import _lib, sharding
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -235,8 +235,13 @@ def run_gpu(args):
     p_dev = torch.empty((R, N), dtype=torch.complex128, device=dev)
     ff_dev = torch.empty((R, M), dtype=torch.complex128, device=dev)
 
+    # this rank's share of the job's frequency list (round-robin, as
+    # beat_engine_b200.sharding splits a multi-GPU sweep); each rank solves
+    # its own frequencies, nothing crosses between ranks
+    share = sharding.partition(world * (args.steps + args.warmup + args.e2e_steps + 16), world)[rank]
+
     def freq(i):
-        return FREQS[(rank + i) % len(FREQS)]
+        return FREQS[share[i] % len(FREQS)]
 
     def step(i, diags=None):
         # one frequency on its own (launch count, isolated stage times)
