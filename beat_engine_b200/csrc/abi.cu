@@ -151,9 +151,20 @@ void solve_core(beat_b200_ctx *c, double k, double eta, int R, const double *d_q
         diag->lu_split_terms = o.lu_split_terms;
         diag->rhs_mode = w.rhs_cached ? BEAT_B200_RHS_CACHED : BEAT_B200_RHS_MATRIX_FREE;
     }
-    BB_REQUIRE(ir.converged || o.precision == BEAT_B200_FP64 || (o.flags & BEAT_B200_FLAG_NO_REFINE),
-               BEAT_B200_NOT_CONVERGED,
+    if (ir.converged || o.precision == BEAT_B200_FP64 || (o.flags & BEAT_B200_FLAG_NO_REFINE)) return;
+    BB_REQUIRE(!(o.flags & BEAT_B200_FLAG_NO_FALLBACK), BEAT_B200_NOT_CONVERGED,
                "GMRES refinement missed its tolerance (worst relative residual " + std::to_string(ir.residual) + ")");
+    // the refinement did not converge: solve this frequency in the FP64 form
+    // (non-convergence reported in diag, not raised)
+    beat_b200_opts o64 = o;
+    o64.precision = BEAT_B200_FP64;
+    o64.lu_block = 64;
+    solve_core(c, k, eta, R, d_q, o64, d_x, diag);
+    if (diag) {
+        diag->ir_iterations = ir.iterations;
+        diag->ir_converged = 0;
+        diag->ir_residual = ir.residual;
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -25,10 +25,20 @@
 
 namespace bb {
 
+// BEAT_B200_FAULT_OOM_BYTES (test hook): allocations of at least that many bytes fail
+static size_t injected_oom_bytes() {
+    const char *e = getenv("BEAT_B200_FAULT_OOM_BYTES");
+    return e ? (size_t)strtoull(e, nullptr, 10) : 0;
+}
+
 void DevBuf::alloc(size_t n) {
     if (n <= bytes && p) return;
     free_();
     if (n == 0) return;
+    const size_t lim = injected_oom_bytes();
+    if (lim && n >= lim)
+        throw Error{BEAT_B200_OOM, "cudaMalloc of " + std::to_string(n) +
+                                       " bytes failed: injected by BEAT_B200_FAULT_OOM_BYTES"};
     cudaError_t e = cudaMalloc(&p, n);
     if (e != cudaSuccess) {
         p = nullptr;

@@ -85,6 +85,18 @@ typedef struct {
 /* opts.flags bits 1-2 request a mode (both clear = auto, both set = invalid) */
 #define BEAT_B200_FLAG_RHS_MATRIX_FREE 2
 #define BEAT_B200_FLAG_RHS_CACHED 4
+/* opts.flags: a mixed-form solve whose refinement misses its tolerance
+ * returns BEAT_B200_NOT_CONVERGED instead of falling back.  By default the
+ * frequency is then solved again in the FP64 form (the reference's dense solve
+ * does the same: BeatEngineDenseSolve.jl:1067-1085, non-convergence is
+ * reported, never raised) and diag.precision reports BEAT_B200_FP64 with
+ * diag.ir_converged = 0 and the failed refinement's iterations and residual. */
+#define BEAT_B200_FLAG_NO_FALLBACK 8
+
+/* Test hook (environment, read at every device allocation):
+ * BEAT_B200_FAULT_OOM_BYTES=n makes each allocation of n bytes or more fail
+ * as out of memory, to exercise the out-of-memory paths (the right-hand-side
+ * mapping's fallback, BEAT_B200_OOM) without exhausting the device. */
 
 typedef struct {
     double assembly_ms;     /* regular + singular + identity + RHS */
