@@ -203,6 +203,79 @@ def oscillating_sphere(refinements: int, radius: float, tag: int = 2) -> Boundar
     return BoundaryMesh(radius * np.array(verts), np.array(faces), np.full(len(faces), tag))
 
 
+def rounded_box_enclosure(n_faces_target: int, size=(0.2, 0.3, 0.25), fillet: float = 0.02,
+                          piston_radius: float = 0.05, jitter: float = 0.05, seed: int = 0,
+                          body_tag: int = 1, piston_tag: int = 2) -> BoundaryMesh:
+    """Loudspeaker-like enclosure: a box of ``size`` (x width, y height,
+    z depth) with edges and corners rounded to ``fillet``, and a circular
+    piston of ``piston_radius`` centred on the front face (z = +depth / 2)
+    whose faces carry ``piston_tag``.
+
+    Triangulated at one target edge length so that there are about
+    ``n_faces_target`` triangles: each face of a cube is cut into a grid whose
+    cell counts follow the box's extents, every cell into two triangles, and
+    each lattice point b (in box coordinates) is mapped onto the rounded box by
+    p = c + fillet (b - c) / |b - c|, c = b clamped to the box shrunk by the
+    fillet.  That gives flat faces, cylindrical edges and spherical corners.
+    Vertices are jittered by up to ``jitter`` x the edge length along the
+    grid directions free on their cube face (seeded), which keeps them on the
+    surface; windings are outward."""
+    half = np.asarray(size, dtype=np.float64) / 2.0
+    area = 2.0 * (size[0] * size[1] + size[1] * size[2] + size[0] * size[2])
+    h = math.sqrt(2.0 * area / n_faces_target)
+    n = [max(2, int(round(s / h))) for s in size]
+    index: dict = {}
+    lattice: list = []
+
+    def vid(i, j, k):
+        key = (i, j, k)
+        if key not in index:
+            index[key] = len(lattice)
+            lattice.append(key)
+        return index[key]
+
+    faces = []
+    for axis in range(3):
+        u, v = [a for a in range(3) if a != axis]
+        for side in (0, n[axis]):
+            outward = 1.0 if side else -1.0
+            for a in range(n[u]):
+                for b in range(n[v]):
+                    corner = []
+                    for du, dv in ((0, 0), (1, 0), (1, 1), (0, 1)):
+                        ijk = [0, 0, 0]
+                        ijk[axis], ijk[u], ijk[v] = side, a + du, b + dv
+                        corner.append(vid(*ijk))
+                    # (u, v, axis) is right-handed for axis = 0, 2 and left-handed for 1
+                    right = (axis != 1) == (outward > 0)
+                    t1, t2 = (corner[0], corner[1], corner[2]), (corner[0], corner[2], corner[3])
+                    if not right:
+                        t1, t2 = (corner[0], corner[2], corner[1]), (corner[0], corner[3], corner[2])
+                    faces.extend([t1, t2])
+    L = np.asarray(lattice, dtype=np.float64)
+    rng = np.random.default_rng(seed)
+    step = np.array([2.0 / n[a] for a in range(3)])  # lattice spacing in cube coordinates
+    cube = L * step - 1.0
+    free = (L > 0) & (L < np.asarray(n))  # coordinates not pinned to a cube face
+    cube += free * rng.uniform(-jitter, jitter, size=cube.shape) * step
+    box = cube * half
+    inner = np.clip(box, -(half - fillet), half - fillet)
+    d = box - inner
+    dl = np.linalg.norm(d, axis=1)
+    verts = inner + fillet * d / dl[:, None]
+    F = np.asarray(faces, dtype=np.int64)
+    c = verts[F].mean(axis=1)
+    tags = np.full(len(F), body_tag)
+    front = (c[:, 2] > half[2] - 1e-9) & (np.hypot(c[:, 0], c[:, 1]) <= piston_radius)
+    tags[front] = piston_tag
+    mesh = BoundaryMesh(verts, F, tags)
+    # outward: the normals point away from the box's centre and the volume is positive
+    vol = np.einsum("ij,ij->i", verts[F[:, 0]], np.cross(verts[F[:, 1]], verts[F[:, 2]])).sum() / 6.0
+    if vol <= 0 or np.any(np.einsum("ij,ij->i", mesh.normals, mesh.centroids) <= 0):
+        raise RuntimeError("rounded box has an inward normal")
+    return mesh
+
+
 def fibonacci_sphere(n_points: int, radius: float) -> np.ndarray:
     """``fibonacci_sphere`` of ``src/BeatEngineCore.jl:828-840`` (``n x 3``)."""
     golden = math.pi * (3.0 - math.sqrt(5.0))
