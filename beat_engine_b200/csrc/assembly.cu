@@ -656,7 +656,7 @@ template <typename T> struct SingArgs {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(256) singular_pairs_kernel(SingArgs<T> g) {
+__global__ void __launch_bounds__(256, 2) singular_pairs_kernel(SingArgs<T> g) {
     const int lane = threadIdx.x & 31;
     const int64_t pair = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     if (pair >= g.npairs) return;
@@ -808,7 +808,7 @@ __device__ __forceinline__ void bm_point_d(const double *x, const double *y, con
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) image_delta_kernel(ImgArgs<T> g) {
+__global__ void __launch_bounds__(256, 2) image_delta_kernel(ImgArgs<T> g) {
     const int lane = threadIdx.x & 31;
     const int64_t pair = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     if (pair >= g.npairs) return;
