@@ -49,9 +49,9 @@ beat_b200_opts resolve_opts(const beat_b200_opts *o) {
     if (r.lu_split_terms != 1 && r.lu_split_terms != 3) r.lu_split_terms = 3;
     BB_REQUIRE(r.precision == BEAT_B200_FP64 || r.precision == BEAT_B200_MIXED_FP32_IR, BEAT_B200_INVALID_ARG,
                "unknown precision form");
-    if (r.lu_block <= 0) r.lu_block = r.precision == BEAT_B200_FP64 ? 64 : 128;
-    BB_REQUIRE(r.lu_block == 32 || r.lu_block == 64 || r.lu_block == 128, BEAT_B200_INVALID_ARG,
-               "lu_block must be 32, 64 or 128");
+    if (r.lu_block <= 0) r.lu_block = 128;  // measured best for both forms at N = 10,242
+    BB_REQUIRE(r.lu_block == 32 || r.lu_block == 64 || r.lu_block == 128 || r.lu_block == 256,
+               BEAT_B200_INVALID_ARG, "lu_block must be 32, 64, 128 or 256");
     BB_REQUIRE((r.flags & (BEAT_B200_FLAG_RHS_MATRIX_FREE | BEAT_B200_FLAG_RHS_CACHED)) !=
                    (BEAT_B200_FLAG_RHS_MATRIX_FREE | BEAT_B200_FLAG_RHS_CACHED),
                BEAT_B200_INVALID_ARG, "flags request both right-hand-side modes");
@@ -158,7 +158,7 @@ void solve_core(beat_b200_ctx *c, double k, double eta, int R, const double *d_q
     // (non-convergence reported in diag, not raised)
     beat_b200_opts o64 = o;
     o64.precision = BEAT_B200_FP64;
-    o64.lu_block = 64;
+    o64.lu_block = 128;
     solve_core(c, k, eta, R, d_q, o64, d_x, diag);
     if (diag) {
         diag->ir_iterations = ir.iterations;

@@ -505,6 +505,104 @@ __global__ void __launch_bounds__(256, 2) gemm_update_kernel(Cx<T> *A, int64_t l
 }
 
 // ---------------------------------------------------------------------------
+// FP64 tensor-core (DMMA) complex GEMM for the FP64 form's updates:
+// C[r0.., c0..] -= L U on the same 64 x 64 complex output tiles as
+// gemm_update_kernel.  Eight warps as 2 x 4, each a 32 x 16 complex warp tile
+// of 8 x 8 blocks computed with mma.sync.m8n8k4.f64 (4 real products per
+// complex block: re += Lr Ur - Li Ui, im += Lr Ui + Li Ur).  L and U are
+// staged as separate real / imaginary planes, K in chunks of 16, with row
+// paddings that keep each fragment load to its two 128-byte wavefronts.
+// Fragments (PTX ISA, m8n8k4 .f64): A a0 at (lane / 4, lane % 4); B b0 at
+// (lane % 4, lane / 4); C c0, c1 at (lane / 4, 2 (lane % 4) + 0, 1).
+// ---------------------------------------------------------------------------
+constexpr int DM_KC = 16, DM_LP = DM_KC + 4, DM_UP = GT + 4;
+
+__device__ __forceinline__ void dmma884(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(256, 2) dmma_update_kernel(Cx<double> *A, int64_t ld, int n, int k, int kk,
+                                                            int row0, int col0, int col_end) {
+    __shared__ double sLr[GT][DM_LP], sLi[GT][DM_LP];  // L chunk: 64 rows x 16
+    __shared__ double sUr[DM_KC][DM_UP], sUi[DM_KC][DM_UP];  // U chunk: 16 x 64 columns
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wr = warp >> 2, wc = warp & 3;  // warp tile: rows 32 wr .., columns 16 wc ..
+    const int g = lane >> 2, t = lane & 3;
+    const int r0 = row0 + blockIdx.y * GT, c0 = col0 + blockIdx.x * GT;
+    double cr[4][2][2], ci[4][2][2];  // [row block][column block][fragment]
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
+    for (int kc = 0; kc < kk; kc += DM_KC) {
+        // stage the chunk: 64 x 16 of L and 16 x 64 of U, four complex entries each per thread
+#pragma unroll
+        for (int u = 0; u < GT * DM_KC / 256; ++u) {
+            const int idx = tid + u * 256;
+            const int i = idx / DM_KC, q = idx % DM_KC, r = r0 + i, kq = kc + q;
+            const Cx<double> vl = (r < n && kq < kk) ? A[(int64_t)r * ld + k + kq] : Cx<double>{0.0, 0.0};
+            sLr[i][q] = vl.re;
+            sLi[i][q] = vl.im;
+            const int q2 = idx / GT, j = idx % GT, c = c0 + j, kq2 = kc + q2;
+            const Cx<double> vu = (c < col_end && kq2 < kk) ? A[(int64_t)(k + kq2) * ld + c] : Cx<double>{0.0, 0.0};
+            sUr[q2][j] = vu.re;
+            sUi[q2][j] = vu.im;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k4 = 0; k4 < DM_KC; k4 += 4) {
+            double ar[4], ai[4], nai[4], br[2], bi[2];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                ar[i] = sLr[32 * wr + 8 * i + g][k4 + t];
+                ai[i] = sLi[32 * wr + 8 * i + g][k4 + t];
+                nai[i] = -ai[i];
+            }
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                br[j] = sUr[k4 + t][16 * wc + 8 * j + g];
+                bi[j] = sUi[k4 + t][16 * wc + 8 * j + g];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    dmma884(cr[i][j], ar[i], br[j]);
+                    dmma884(cr[i][j], nai[i], bi[j]);
+                    dmma884(ci[i][j], ar[i], bi[j]);
+                    dmma884(ci[i][j], ai[i], br[j]);
+                }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int r = r0 + 32 * wr + 8 * i + g, c = c0 + 16 * wc + 8 * j + 2 * t + e;
+                if (r < n && c < col_end) {
+                    Cx<double> &d = A[(int64_t)r * ld + c];
+                    d.re -= cr[i][j][e];
+                    d.im -= ci[i][j][e];
+                }
+            }
+}
+
+// the trailing / in-panel update C -= L U: tensor cores (DMMA) in FP64, SIMT in FP32
+template <typename T>
+static void launch_update(cudaStream_t st, dim3 grid, Cx<T> *A, int64_t ld, int n, int k, int kk, int row0, int col0,
+                          int col_end) {
+    if constexpr (sizeof(T) == 8)
+        dmma_update_kernel<<<grid, 256, 0, st>>>(A, ld, n, k, kk, row0, col0, col_end);
+    else
+        gemm_update_kernel<T><<<grid, 256, 0, st>>>(A, ld, n, k, kk, row0, col0, col_end);
+}
+
+// ---------------------------------------------------------------------------
 // Sub-panel factorisation on one thread-block cluster.  CP_CTAS CTAs hold all
 // rows of a w-column sub-panel (256-byte rows) in shared memory; rows never
 // move: each row carries its logical position, and an interchange only swaps
@@ -1014,8 +1112,13 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
                                      (int)tb_smem));
     c->barrier.alloc(sizeof(unsigned) * 4096);
     BB_CUDA(cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+    // the unblocked U12 solve (used only when the blocked one does not apply)
     const size_t trsm_smem = sizeof(Cx<T>) * ((size_t)nb * nb + (size_t)nb * TRSM_COLS);
-    BB_CUDA(cudaFuncSetAttribute(trsm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
+    if (!blocked) {
+        BB_REQUIRE(trsm_smem <= 227 * 1024, BEAT_B200_INVALID_ARG,
+                   "LU: lu_block " + std::to_string(nb) + " is too wide for the unblocked U12 solve");
+        BB_CUDA(cudaFuncSetAttribute(trsm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
+    }
     iota_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(w.perm.as<int>(), n);
     BB_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream));
     const size_t trsm_w_smem = sizeof(Cx<T>) * ((size_t)W * W + (size_t)W * TRSM_COLS);
@@ -1066,7 +1169,7 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
                     trsm_kernel<T><<<(cols + TRSM_COLS - 1) / TRSM_COLS, 256, trsm_w_smem, c->stream>>>(
                         A, ld, n, ks, W, ks + W, pe);
                 dim3 grid((cols + GT - 1) / GT, (n - ks - W + GT - 1) / GT);
-                gemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(A, ld, n, ks, W, ks + W, ks + W, pe);
+                launch_update<T>(c->stream, grid, A, ld, n, ks, W, ks + W, ks + W, pe);
                 BB_CUDA(cudaGetLastError());
             }
         }
@@ -1081,7 +1184,7 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
             BB_CUDA(cudaGetLastError());
             if (!(sizeof(T) == 4 && tc_trailing_update(c, k, nb, split_terms))) {
                 dim3 grid((rest + GT - 1) / GT, (rest + GT - 1) / GT);
-                gemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(A, ld, n, k, nb, k + nb, k + nb, n);
+                launch_update<T>(c->stream, grid, A, ld, n, k, nb, k + nb, k + nb, n);
                 BB_CUDA(cudaGetLastError());
             }
         }
