@@ -364,14 +364,29 @@ template <typename T, int Q> static size_t regular_smem_bytes() {
 // has its own shared-memory accumulators, flushed like the one-order kernel.
 // ---------------------------------------------------------------------------
 constexpr int SYM_F = 32, SYM_V = 40;  // square tile: faces, distinct vertices (context.cu)
-// accumulators as separate re / im planes with odd row strides: a warp's
-// lanes (one tau, 32 sigma) hit rows spread over all banks
-constexpr int SYM_AS = SYM_V + 1, SYM_BS = SYM_F + 1;
-constexpr int SYM_ACC = 2 * SYM_V * SYM_AS + 2 * SYM_V * SYM_BS;  // floats per plane
+// Accumulators.  A warp takes one tau and 32 sigma (one per lane), so the
+// entries a lane adds to are keyed by sigma's vertex *slot* (s = b * SYM_F +
+// sigma, the slot-face index) rather than by sigma's vertex: two lanes whose
+// faces share a vertex would otherwise add to the same word in the same
+// instruction, and shared-memory float atomics retry once per colliding lane.
+// The slot-face entries are folded onto tile J's vertices at the flush.
+//   C1 [vI][s]      order 1, test vertex of tau x trial slot of sigma
+//   C2 [s][vI]      order 2, test slot of sigma x trial vertex of tau
+//   B1 [vI][sigma]  order 1 right-hand side (test vertex of tau x face sigma)
+//   D2 [s][tau]     order 2 right-hand side (test slot of sigma x face tau)
+// Re / im planes; a warp's lanes step 1 or an odd stride through each, so
+// they spread over all banks.
+constexpr int SYM_S = 3 * SYM_F;                  // slot-face indices of a tile
+constexpr int SYM_C2S = SYM_V + 1, SYM_BS = SYM_F + 1;
+constexpr int SYM_C1 = 0;
+constexpr int SYM_C2 = SYM_C1 + SYM_V * SYM_S;
+constexpr int SYM_B1 = SYM_C2 + SYM_S * SYM_C2S;
+constexpr int SYM_D2 = SYM_B1 + SYM_V * SYM_BS;
+constexpr int SYM_ACC = SYM_D2 + SYM_S * SYM_BS;  // floats per plane
 
 template <int Q> static size_t sym_smem_bytes() {
     return sizeof(float) * 2 * SYM_ACC + sizeof(float) * 2 * SYM_F * (Q * 3 + 3 + 9 + 2) +
-           sizeof(int) * 4 * 3 * SYM_F;
+           sizeof(int) * (4 * 3 * SYM_F + SYM_V + 1 + SYM_S);
 }
 
 template <int Q>
@@ -380,10 +395,6 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
     constexpr int RI = Q == 1 ? 0 : Q == 3 ? 1 : 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *acc_re = reinterpret_cast<T *>(smem_raw), *acc_im = acc_re + SYM_ACC;
-    constexpr int A1 = 0;                      // [vI][vJ]: test vertex of tau, trial vertex of sigma
-    constexpr int A2 = A1 + SYM_V * SYM_AS;    // [vJ][vI]: test vertex of sigma, trial vertex of tau
-    constexpr int B1 = A2 + SYM_V * SYM_AS;    // [vI][sigma]
-    constexpr int B2 = B1 + SYM_V * SYM_BS;    // [vJ][tau]
     T *xq = acc_im + SYM_ACC;                  // tile I: [tau][Q][3]
     T *xn = xq + SYM_F * Q * 3;                // [tau][3]
     T *xc = xn + SYM_F * 3;                    // [tau][9]
@@ -398,6 +409,8 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
     int *xlv = xgv + 3 * SYM_F;                      // [tau][3] tile-local vertex ids
     int *ygv = xlv + 3 * SYM_F;                      // [3][sigma]
     int *ylv = ygv + 3 * SYM_F;                      // [3][sigma]
+    int *inc_start = ylv + 3 * SYM_F;                // [vJ + 1]: slot-face indices of tile J's vertex vJ
+    int *inc_list = inc_start + SYM_V + 1;           //   are inc_list[inc_start[vJ] .. inc_start[vJ + 1])
 
     // unordered tile pair (I, J), I <= J, from the linear block index
     const int64_t bi = blockIdx.x;
@@ -413,7 +426,9 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
     const int tv0 = g.t_vstart[I], nvI = g.t_vstart[I + 1] - tv0;
     const int sv0 = g.t_vstart[J], nvJ = g.t_vstart[J + 1] - sv0;
 
-    for (int i = tid; i < 2 * SYM_ACC; i += REG_THREADS) acc_re[i] = T(0);
+    static_assert((2 * SYM_ACC) % 4 == 0, "accumulators are zeroed as float4");
+    for (int i = tid; i < 2 * SYM_ACC / 4; i += REG_THREADS)
+        reinterpret_cast<float4 *>(acc_re)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int i = tid; i < nI * Q * 3; i += REG_THREADS) xq[i] = g.qpts[(size_t)t0 * Q * 3 + i];
     for (int i = tid; i < nI * 3; i += REG_THREADS) {
         xn[i] = g.normal[(size_t)t0 * 3 + i];
@@ -444,6 +459,17 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
         xp[i] = xq[i * Q * 3] * xn[3 * i] + xq[i * Q * 3 + 1] * xn[3 * i + 1] + xq[i * Q * 3 + 2] * xn[3 * i + 2];
     for (int i = tid; i < nJ; i += REG_THREADS)
         yp[i] = yq[i] * yn[i] + yq[SYM_F + i] * yn[SYM_F + i] + yq[2 * SYM_F + i] * yn[2 * SYM_F + i];
+    // incidences of tile J's vertices, in slot-face order: vertex v's list
+    // starts after every incidence of a smaller local vertex
+    if (tid < nvJ) {
+        int before = 0;
+        for (int s = 0; s < 3 * SYM_F; ++s)
+            if (s % SYM_F < nJ) before += ylv[s] < tid;
+        inc_start[tid] = before;
+        for (int s = 0; s < 3 * SYM_F; ++s)
+            if (s % SYM_F < nJ && ylv[s] == tid) inc_list[before++] = s;
+        if (tid == nvJ - 1) inc_start[nvJ] = before;
+    }
     __syncthreads();
 
     const T k = g.k, eta = g.eta;
@@ -546,22 +572,21 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
         const T jac = T(4) * xa[ti] * ya[sj] * ((g.image && diag && sj == ti) ? T(0.5) : T(1));
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            const int ra = xlv[3 * ti + a];      // vertex a of tau, tile I local
-            const int sa = ylv[a * SYM_F + sj];  // vertex a of sigma, tile J local
+            const int ra = xlv[3 * ti + a];  // vertex a of tau, tile I local
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
                 const T d = xc[9 * ti + 3 * a] * yc[(3 * b) * SYM_F + sj] +
                             xc[9 * ti + 3 * a + 1] * yc[(3 * b + 1) * SYM_F + sj] +
                             xc[9 * ti + 3 * a + 2] * yc[(3 * b + 2) * SYM_F + sj];  // curl_tau[a] . curl_sigma[b]
-                const int o1 = A1 + ra * SYM_AS + ylv[b * SYM_F + sj];
+                const int o1 = SYM_C1 + ra * SYM_S + b * SYM_F + sj;
                 red_add(&acc_re[o1], (L1[3 * a + b][0] + d * ccr) * jac);
                 red_add(&acc_im[o1], (L1[3 * a + b][1] + d * cci) * jac);
                 // order 2 entry (sigma vertex b, tau vertex a) uses curl_sigma[b] . curl_tau[a] = d
-                const int o2 = A2 + ylv[b * SYM_F + sj] * SYM_AS + ra;
+                const int o2 = SYM_C2 + (b * SYM_F + sj) * SYM_C2S + ra;
                 red_add(&acc_re[o2], (L2[3 * b + a][0] + d * ccr) * jac);
                 red_add(&acc_im[o2], (L2[3 * b + a][1] + d * cci) * jac);
             }
-            const int e1 = B1 + ra * SYM_BS + sj;
+            const int e1 = SYM_B1 + ra * SYM_BS + sj;
             red_add(&acc_re[e1], R1[a][0] * jac);
             red_add(&acc_im[e1], R1[a][1] * jac);
             T r2r = T(0), r2i = T(0);
@@ -571,16 +596,23 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
                 r2r += bq * U2[qs][0];
                 r2i += bq * U2[qs][1];
             }
-            const int e2 = B2 + sa * SYM_BS + ti;
+            const int e2 = SYM_D2 + (a * SYM_F + sj) * SYM_BS + ti;
             red_add(&acc_re[e2], r2r * jac);
             red_add(&acc_im[e2], r2i * jac);
         }
     }
     __syncthreads();
+    // fold the slot-face entries onto tile J's vertices and flush
     for (int i = tid; i < nvI * nvJ; i += REG_THREADS) {
         const int li = i / nvJ, lj = i % nvJ;
-        const Cx<T> v{acc_re[A1 + li * SYM_AS + lj], acc_im[A1 + li * SYM_AS + lj]};
-        const Cx<T> u{acc_re[A2 + lj * SYM_AS + li], acc_im[A2 + lj * SYM_AS + li]};
+        Cx<T> v{T(0), T(0)}, u{T(0), T(0)};
+        for (int e = inc_start[lj]; e < inc_start[lj + 1]; ++e) {
+            const int s = inc_list[e];
+            v.re += acc_re[SYM_C1 + li * SYM_S + s];
+            v.im += acc_im[SYM_C1 + li * SYM_S + s];
+            u.re += acc_re[SYM_C2 + s * SYM_C2S + li];
+            u.im += acc_im[SYM_C2 + s * SYM_C2S + li];
+        }
         const int gi_ = g.t_verts[tv0 + li], gj_ = g.t_verts[sv0 + lj];
         if (v.re != T(0) || v.im != T(0)) red_add_cx(&g.A[(int64_t)gi_ * g.ld + gj_], v.re, v.im);
         if (u.re != T(0) || u.im != T(0)) red_add_cx(&g.A[(int64_t)gj_ * g.ld + gi_], u.re, u.im);
@@ -588,13 +620,18 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
     if (g.B) {
         for (int i = tid; i < nvI * nJ; i += REG_THREADS) {
             const int li = i / nJ, sj = i % nJ;
-            const Cx<T> v{acc_re[B1 + li * SYM_BS + sj], acc_im[B1 + li * SYM_BS + sj]};
+            const Cx<T> v{acc_re[SYM_B1 + li * SYM_BS + sj], acc_im[SYM_B1 + li * SYM_BS + sj]};
             if (v.re != T(0) || v.im != T(0))
                 red_add_cx(&g.B[(int64_t)g.t_verts[tv0 + li] * g.F + g.face_id[s0 + sj]], v.re, v.im);
         }
         for (int i = tid; i < nvJ * nI; i += REG_THREADS) {
             const int lj = i / nI, ti = i % nI;
-            const Cx<T> v{acc_re[B2 + lj * SYM_BS + ti], acc_im[B2 + lj * SYM_BS + ti]};
+            Cx<T> v{T(0), T(0)};
+            for (int e = inc_start[lj]; e < inc_start[lj + 1]; ++e) {
+                const int s = inc_list[e];
+                v.re += acc_re[SYM_D2 + s * SYM_BS + ti];
+                v.im += acc_im[SYM_D2 + s * SYM_BS + ti];
+            }
             if (v.re != T(0) || v.im != T(0))
                 red_add_cx(&g.B[(int64_t)g.t_verts[sv0 + lj] * g.F + g.face_id[t0 + ti]], v.re, v.im);
         }
@@ -604,6 +641,19 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
     // B2 q (tile J vertices x tile I faces); q of both tiles' faces staged
     // MF_RC columns at a time over the (now unused) geometry region
     float2 *qs = reinterpret_cast<float2 *>(xq);  // [2][SYM_F][MF_RC]: tile I faces, then tile J faces
+    // order 2 rows folded onto tile J's vertices, over the (read) C1 block
+    constexpr int B2V = SYM_C1;  // [vJ][tau]
+    __syncthreads();
+    for (int i = tid; i < nvJ * nI; i += REG_THREADS) {
+        const int lj = i / nI, ti = i % nI;
+        T vr = T(0), vi = T(0);
+        for (int e = inc_start[lj]; e < inc_start[lj + 1]; ++e) {
+            vr += acc_re[SYM_D2 + inc_list[e] * SYM_BS + ti];
+            vi += acc_im[SYM_D2 + inc_list[e] * SYM_BS + ti];
+        }
+        acc_re[B2V + lj * SYM_BS + ti] = vr;
+        acc_im[B2V + lj * SYM_BS + ti] = vi;
+    }
     for (int r0 = 0; r0 < g.R; r0 += MF_RC) {
         const int rc = min(MF_RC, g.R - r0);
         __syncthreads();
@@ -620,7 +670,7 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
         for (int i = tid; i < (nvI + nvJ) * rc; i += REG_THREADS) {
             const int row = i / rc, r = i % rc;
             const bool first = row < nvI;
-            const int base = first ? B1 + row * SYM_BS : B2 + (row - nvI) * SYM_BS;
+            const int base = first ? SYM_B1 + row * SYM_BS : B2V + (row - nvI) * SYM_BS;
             const int nf = first ? nJ : nI;
             const float2 *qh = qs + (first ? SYM_F * MF_RC : 0);
             T sr = T(0), si = T(0);
@@ -1029,6 +1079,8 @@ static void launch_sym(beat_b200_ctx *c, double k, double eta, int img, int R, c
     }
     const size_t smem = sym_smem_bytes<Q>();
     BB_CUDA(cudaFuncSetAttribute(sym_pairs_kernel<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    BB_CUDA(cudaFuncSetAttribute(sym_pairs_kernel<Q>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared));  // two CTAs per SM
     const int64_t nt = c->sym_tiles.ntiles;
     const int64_t blocks = nt * (nt + 1) / 2;
     BB_REQUIRE(blocks < (1ll << 31), BEAT_B200_INVALID_ARG, "assembly: mesh too large for the tile-pair grid");
