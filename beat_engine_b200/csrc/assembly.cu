@@ -29,6 +29,7 @@ namespace bb {
 
 constexpr int TT = 64, VT = 80;  // test tile: faces, distinct vertices (context.cu)
 constexpr int TS = 16, VS = 32;  // trial tile
+constexpr int REG_S = 3 * TS;    // slot-face indices of a trial tile
 constexpr int REG_THREADS = 256;
 
 // rule tables: index 0 -> 1-point, 1 -> 3-point, 2 -> 6-point (order 4)
@@ -152,8 +153,11 @@ template <typename T, int Q>
 __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_pairs_kernel(RegArgs<T> g) {
     constexpr int RI = Q == 1 ? 0 : Q == 3 ? 1 : 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Cx<T> *sA = reinterpret_cast<Cx<T> *>(smem_raw);  // VT x VS
-    Cx<T> *sB = sA + VT * VS;                         // VT x TS
+    // test vertex x trial vertex *slot* (s = b * TS + trial face): lanes that
+    // share a test vertex never add to one word together (see the symmetric
+    // kernel below); folded onto the trial tile's vertices at the flush
+    Cx<T> *sC = reinterpret_cast<Cx<T> *>(smem_raw);  // VT x REG_S
+    Cx<T> *sB = sC + VT * REG_S;                      // VT x TS
     T *tq = reinterpret_cast<T *>(sB + VT * TS);      // TT x Q x 3
     T *tn = tq + TT * Q * 3;                          // TT x 3
     T *tc = tn + TT * 3;                              // TT x 9
@@ -168,6 +172,8 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
     int *tlv = tgv + TT * 3;                          // TT x 3
     int *sgv = tlv + TT * 3;                          // 3 x TS
     int *slv = sgv + TS * 3;                          // 3 x TS
+    int *inc_start = slv + TS * 3;                    // VS + 1: trial vertex -> its slot-face indices
+    int *inc_list = inc_start + VS + 1;               // REG_S
 
     const int tid = threadIdx.x;
     const int t0 = g.t_fstart[blockIdx.y], nt = g.t_fstart[blockIdx.y + 1] - t0;
@@ -175,7 +181,7 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
     const int tv0 = g.t_vstart[blockIdx.y], nvt = g.t_vstart[blockIdx.y + 1] - tv0;
     const int sv0 = g.s_vstart[blockIdx.x], nvs = g.s_vstart[blockIdx.x + 1] - sv0;
 
-    for (int i = tid; i < VT * VS; i += REG_THREADS) sA[i] = Cx<T>{T(0), T(0)};
+    for (int i = tid; i < VT * REG_S; i += REG_THREADS) sC[i] = Cx<T>{T(0), T(0)};
     for (int i = tid; i < VT * TS; i += REG_THREADS) sB[i] = Cx<T>{T(0), T(0)};
     for (int i = tid; i < nt * Q * 3; i += REG_THREADS) tq[i] = g.qpts[(size_t)t0 * Q * 3 + i];
     for (int i = tid; i < nt * 3; i += REG_THREADS) {
@@ -206,6 +212,15 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
         tpl[i] = tq[i * Q * 3] * tn[3 * i] + tq[i * Q * 3 + 1] * tn[3 * i + 1] + tq[i * Q * 3 + 2] * tn[3 * i + 2];
     for (int i = tid; i < ns; i += REG_THREADS)
         spl[i] = sq[i] * sn[i] + sq[TS + i] * sn[TS + i] + sq[2 * TS + i] * sn[2 * TS + i];
+    if (tid < nvs) {  // incidences of the trial tile's vertices, in slot-face order
+        int before = 0;
+        for (int s = 0; s < REG_S; ++s)
+            if (s % TS < ns) before += slv[s] < tid;
+        inc_start[tid] = before;
+        for (int s = 0; s < REG_S; ++s)
+            if (s % TS < ns && slv[s] == tid) inc_list[before++] = s;
+        if (tid == nvs - 1) inc_start[nvs] = before;
+    }
     __syncthreads();
 
     const T k = g.k, eta = g.eta;
@@ -290,8 +305,7 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
                 const T d = tc[9 * tl + 3 * a] * sc[(3 * b) * TS + sl] +
                             tc[9 * tl + 3 * a + 1] * sc[(3 * b + 1) * TS + sl] +
                             tc[9 * tl + 3 * a + 2] * sc[(3 * b + 2) * TS + sl];
-                const int col = slv[b * TS + sl];
-                Cx<T> *dst = &sA[row * VS + col];
+                Cx<T> *dst = &sC[row * REG_S + b * TS + sl];
                 red_add(&dst->re, (L[3 * a + b][0] + d * ccr) * jac);
                 red_add(&dst->im, (L[3 * a + b][1] + d * cci) * jac);
             }
@@ -303,7 +317,12 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
     __syncthreads();
     for (int i = tid; i < nvt * nvs; i += REG_THREADS) {
         const int lt = i / nvs, ls = i % nvs;
-        const Cx<T> v = sA[lt * VS + ls];
+        Cx<T> v{T(0), T(0)};
+        for (int e = inc_start[ls]; e < inc_start[ls + 1]; ++e) {
+            const Cx<T> c = sC[lt * REG_S + inc_list[e]];
+            v.re += c.re;
+            v.im += c.im;
+        }
         if (v.re != T(0) || v.im != T(0))
             red_add_cx(&g.A[(int64_t)g.t_verts[tv0 + lt] * g.ld + g.s_verts[sv0 + ls]], v.re, v.im);
     }
@@ -347,8 +366,8 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
 }
 
 template <typename T, int Q> static size_t regular_smem_bytes() {
-    return sizeof(Cx<T>) * (VT * VS + VT * TS) + sizeof(T) * (TT * (Q * 3 + 3 + 9 + 2) + TS * (Q * 3 + 3 + 9 + 2)) +
-           sizeof(int) * (TT * 6 + TS * 6);
+    return sizeof(Cx<T>) * (VT * REG_S + VT * TS) + sizeof(T) * (TT * (Q * 3 + 3 + 9 + 2) + TS * (Q * 3 + 3 + 9 + 2)) +
+           sizeof(int) * (TT * 6 + TS * 6 + VS + 1 + REG_S);
 }
 
 // ---------------------------------------------------------------------------
@@ -596,9 +615,10 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
                 r2r += bq * U2[qs][0];
                 r2i += bq * U2[qs][1];
             }
+            // (sigma slot a, face tau) belongs to this element pair alone: a plain store
             const int e2 = SYM_D2 + (a * SYM_F + sj) * SYM_BS + ti;
-            red_add(&acc_re[e2], r2r * jac);
-            red_add(&acc_im[e2], r2i * jac);
+            acc_re[e2] = r2r * jac;
+            acc_im[e2] = r2i * jac;
         }
     }
     __syncthreads();
@@ -1041,6 +1061,8 @@ static void launch_regular(beat_b200_ctx *c, double k, double eta, int img, int 
     }
     const size_t smem = regular_smem_bytes<T, Q>();
     BB_CUDA(cudaFuncSetAttribute(regular_pairs_kernel<T, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    BB_CUDA(cudaFuncSetAttribute(regular_pairs_kernel<T, Q>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared));
     dim3 grid(c->trial_tiles.ntiles, c->test_tiles.ntiles);
     regular_pairs_kernel<T, Q><<<grid, REG_THREADS, smem, c->stream>>>(g);
     BB_CUDA(cudaGetLastError());
