@@ -87,6 +87,30 @@ __device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
 
 __device__ __forceinline__ void red_add(double *p, double v) { atomicAdd(p, v); }
 __device__ __forceinline__ void red_add(float *p, float v) { atomicAdd(p, v); }
+// Adds v[i] to base[off[i]] for every i, atomically.  Shared-memory float
+// adds are compare-and-swap loops, each a dependent load -> add -> swap
+// chain; here the loads, then the swaps, of all N adds are in flight
+// together, and only a swap that lost to another warp's add is redone as an
+// ordinary atomic add.  (ABA is harmless: the swap writes old + v over old.)
+template <int N>
+__device__ __forceinline__ void batch_add(float *base, const int (&off)[N], const float (&v)[N]) {
+    static_assert(N <= 32, "one failure bit per add");
+    unsigned old[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) old[i] = *reinterpret_cast<volatile unsigned *>(base + off[i]);
+    unsigned fail = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        const unsigned got =
+            atomicCAS(reinterpret_cast<unsigned *>(base + off[i]), old[i], __float_as_uint(__uint_as_float(old[i]) + v[i]));
+        fail |= (got != old[i] ? 1u : 0u) << i;
+    }
+    if (fail) {
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+            if (fail >> i & 1u) atomicAdd(base + off[i], v[i]);
+    }
+}
 __device__ __forceinline__ void red_add_cx(Cx<double> *p, double re, double im) {
     atomicAdd(&p->re, re);
     atomicAdd(&p->im, im);
@@ -592,22 +616,31 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             const int ra = xlv[3 * ti + a];  // vertex a of tau, tile I local
+            int off[14];  // this vertex's 14 adds (re and im planes)
+            float val[14];
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
                 const T d = xc[9 * ti + 3 * a] * yc[(3 * b) * SYM_F + sj] +
                             xc[9 * ti + 3 * a + 1] * yc[(3 * b + 1) * SYM_F + sj] +
                             xc[9 * ti + 3 * a + 2] * yc[(3 * b + 2) * SYM_F + sj];  // curl_tau[a] . curl_sigma[b]
                 const int o1 = SYM_C1 + ra * SYM_S + b * SYM_F + sj;
-                red_add(&acc_re[o1], (L1[3 * a + b][0] + d * ccr) * jac);
-                red_add(&acc_im[o1], (L1[3 * a + b][1] + d * cci) * jac);
+                off[4 * b] = o1;
+                val[4 * b] = (L1[3 * a + b][0] + d * ccr) * jac;
+                off[4 * b + 1] = o1 + SYM_ACC;
+                val[4 * b + 1] = (L1[3 * a + b][1] + d * cci) * jac;
                 // order 2 entry (sigma vertex b, tau vertex a) uses curl_sigma[b] . curl_tau[a] = d
                 const int o2 = SYM_C2 + (b * SYM_F + sj) * SYM_C2S + ra;
-                red_add(&acc_re[o2], (L2[3 * b + a][0] + d * ccr) * jac);
-                red_add(&acc_im[o2], (L2[3 * b + a][1] + d * cci) * jac);
+                off[4 * b + 2] = o2;
+                val[4 * b + 2] = (L2[3 * b + a][0] + d * ccr) * jac;
+                off[4 * b + 3] = o2 + SYM_ACC;
+                val[4 * b + 3] = (L2[3 * b + a][1] + d * cci) * jac;
             }
-            const int e1 = SYM_B1 + ra * SYM_BS + sj;
-            red_add(&acc_re[e1], R1[a][0] * jac);
-            red_add(&acc_im[e1], R1[a][1] * jac);
+            off[12] = SYM_B1 + ra * SYM_BS + sj;
+            val[12] = R1[a][0] * jac;
+            off[13] = off[12] + SYM_ACC;
+            val[13] = R1[a][1] * jac;
+            // tau's other elements in flight on other warps may share vertex a
+            batch_add<14>(acc_re, off, val);
             T r2r = T(0), r2i = T(0);
 #pragma unroll
             for (int qs = 0; qs < Q; ++qs) {
