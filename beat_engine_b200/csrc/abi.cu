@@ -330,7 +330,8 @@ int32_t beat_b200_destroy(beat_b200_ctx *c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     release_workspace(c);
     for (DevBuf *b : {&c->pos_face, &c->pos_qpts64, &c->pos_qpts32, &c->pos_normal64, &c->pos_normal32,
-                      &c->pos_curl64, &c->pos_curl32, &c->pos_area64, &c->pos_area32, &c->pos_gvert, &c->d_verts,
+                      &c->pos_curl64, &c->pos_curl32, &c->pos_area64, &c->pos_area32, &c->pos_plane32,
+                      &c->pos_gvert, &c->d_verts,
                       &c->d_faces, &c->d_normals, &c->d_areas, &c->d_curls, &c->d_qpts, &c->vf_start, &c->vf_face,
                       &c->adm, &c->ip_test, &c->ip_trial, &c->ip_rule, &c->ip_img, &c->ip_jac, &c->ip_nn,
                       &c->rw_vert, &c->rw_weight, &c->sp_test, &c->sp_trial,

@@ -30,6 +30,7 @@ namespace bb {
 constexpr int TT = 64, VT = 80;  // test tile: faces, distinct vertices (context.cu)
 constexpr int TS = 16, VS = 32;  // trial tile
 constexpr int REG_S = 3 * TS;    // slot-face indices of a trial tile
+constexpr int REG_INC = VS + 1 + REG_S;  // Tiling::inc_stride() of the trial tiles
 constexpr int REG_THREADS = 256;
 
 // rule tables: index 0 -> 1-point, 1 -> 3-point, 2 -> 6-point (order 4)
@@ -111,6 +112,37 @@ __device__ __forceinline__ void batch_add(float *base, const int (&off)[N], cons
             if (fail >> i & 1u) atomicAdd(base + off[i], v[i]);
     }
 }
+// the same for double words (64-bit compare-and-swap)
+template <int N>
+__device__ __forceinline__ void batch_add(double *base, const int (&off)[N], const double (&v)[N]) {
+    static_assert(N <= 32, "one failure bit per add");
+    using U = unsigned long long;
+    U old[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) old[i] = *reinterpret_cast<volatile U *>(base + off[i]);
+    unsigned fail = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        const double sum = __longlong_as_double((long long)old[i]) + v[i];
+        const U got = atomicCAS(reinterpret_cast<U *>(base + off[i]), old[i], (U)__double_as_longlong(sum));
+        fail |= (got != old[i] ? 1u : 0u) << i;
+    }
+    if (fail) {
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+            if (fail >> i & 1u) atomicAdd(base + off[i], v[i]);
+    }
+}
+// 4-byte global -> shared copy through the asynchronous copy unit: a CTA's
+// tile arrays are all in flight at once and waited for together
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 __device__ __forceinline__ void red_add_cx(Cx<double> *p, double re, double im) {
     atomicAdd(&p->re, re);
     atomicAdd(&p->im, im);
@@ -152,10 +184,12 @@ template <typename T> struct RegArgs {
     const T *normal;    // F x 3
     const T *curl;      // F x 9
     const T *area;      // F
+    const T *plane = nullptr;  // F: plane offset . normal (FP32 symmetric kernel)
     const int *gvert;   // F x 3
     const int *face_id; // F
     const int *t_fstart, *t_vstart, *t_verts, *t_local;
     const int *s_fstart, *s_vstart, *s_verts, *s_local;
+    const int *t_inc = nullptr, *s_inc = nullptr;  // per-tile vertex incidences (Tiling::incidence)
     Cx<T> *A;
     Cx<T> *B;
     int64_t ld;         // row stride of A (complex entries)
@@ -195,8 +229,7 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
     int *tgv = reinterpret_cast<int *>(spl + TS);     // TT x 3
     int *tlv = tgv + TT * 3;                          // TT x 3
     int *sgv = tlv + TT * 3;                          // 3 x TS
-    int *slv = sgv + TS * 3;                          // 3 x TS
-    int *inc_start = slv + TS * 3;                    // VS + 1: trial vertex -> its slot-face indices
+    int *inc_start = sgv + TS * 3;                    // VS + 1: trial vertex -> its slot-face indices
     int *inc_list = inc_start + VS + 1;               // REG_S
 
     const int tid = threadIdx.x;
@@ -223,28 +256,19 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
         int s = i / 3, j = i % 3;
         sn[j * TS + s] = g.xs[j] * g.normal[(size_t)s0 * 3 + i];
         sgv[j * TS + s] = g.gvert[(size_t)s0 * 3 + i];
-        slv[j * TS + s] = g.s_local[(size_t)s0 * 3 + i];
     }
     for (int i = tid; i < ns * 9; i += REG_THREADS) {
         int s = i / 9, j = i % 9;
         sc[j * TS + s] = g.xdet * g.xs[j % 3] * g.curl[(size_t)s0 * 9 + i];
     }
     for (int i = tid; i < ns; i += REG_THREADS) sa[i] = g.area[s0 + i];
+    for (int i = tid; i < REG_INC; i += REG_THREADS) inc_start[i] = g.s_inc[(size_t)blockIdx.x * REG_INC + i];
     __syncthreads();
     // every point y of a flat face has the same y . n
     for (int i = tid; i < nt; i += REG_THREADS)
         tpl[i] = tq[i * Q * 3] * tn[3 * i] + tq[i * Q * 3 + 1] * tn[3 * i + 1] + tq[i * Q * 3 + 2] * tn[3 * i + 2];
     for (int i = tid; i < ns; i += REG_THREADS)
         spl[i] = sq[i] * sn[i] + sq[TS + i] * sn[TS + i] + sq[2 * TS + i] * sn[2 * TS + i];
-    if (tid < nvs) {  // incidences of the trial tile's vertices, in slot-face order
-        int before = 0;
-        for (int s = 0; s < REG_S; ++s)
-            if (s % TS < ns) before += slv[s] < tid;
-        inc_start[tid] = before;
-        for (int s = 0; s < REG_S; ++s)
-            if (s % TS < ns && slv[s] == tid) inc_list[before++] = s;
-        if (tid == nvs - 1) inc_start[nvs] = before;
-    }
     __syncthreads();
 
     const T k = g.k, eta = g.eta;
@@ -324,18 +348,24 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             const int row = tlv[3 * tl + a];
+            int off[8];  // this vertex's 8 adds, in T words from sC
+            T val[8];
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
                 const T d = tc[9 * tl + 3 * a] * sc[(3 * b) * TS + sl] +
                             tc[9 * tl + 3 * a + 1] * sc[(3 * b + 1) * TS + sl] +
                             tc[9 * tl + 3 * a + 2] * sc[(3 * b + 2) * TS + sl];
-                Cx<T> *dst = &sC[row * REG_S + b * TS + sl];
-                red_add(&dst->re, (L[3 * a + b][0] + d * ccr) * jac);
-                red_add(&dst->im, (L[3 * a + b][1] + d * cci) * jac);
+                const int o = 2 * (row * REG_S + b * TS + sl);
+                off[2 * b] = o;
+                val[2 * b] = (L[3 * a + b][0] + d * ccr) * jac;
+                off[2 * b + 1] = o + 1;
+                val[2 * b + 1] = (L[3 * a + b][1] + d * cci) * jac;
             }
-            Cx<T> *db = &sB[row * TS + sl];
-            red_add(&db->re, Rv[a][0] * jac);
-            red_add(&db->im, Rv[a][1] * jac);
+            off[6] = 2 * (VT * REG_S + row * TS + sl);
+            val[6] = Rv[a][0] * jac;
+            off[7] = off[6] + 1;
+            val[7] = Rv[a][1] * jac;
+            batch_add<8>(reinterpret_cast<T *>(sC), off, val);
         }
     }
     __syncthreads();
@@ -391,7 +421,7 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
 
 template <typename T, int Q> static size_t regular_smem_bytes() {
     return sizeof(Cx<T>) * (VT * REG_S + VT * TS) + sizeof(T) * (TT * (Q * 3 + 3 + 9 + 2) + TS * (Q * 3 + 3 + 9 + 2)) +
-           sizeof(int) * (TT * 6 + TS * 6 + VS + 1 + REG_S);
+           sizeof(int) * (TT * 6 + TS * 3 + REG_INC);
 }
 
 // ---------------------------------------------------------------------------
@@ -427,9 +457,11 @@ constexpr int SYM_B1 = SYM_C2 + SYM_S * SYM_C2S;
 constexpr int SYM_D2 = SYM_B1 + SYM_V * SYM_BS;
 constexpr int SYM_ACC = SYM_D2 + SYM_S * SYM_BS;  // floats per plane
 
+constexpr int SYM_INC = SYM_V + 1 + SYM_S;  // Tiling::inc_stride() of the square tiles
+
 template <int Q> static size_t sym_smem_bytes() {
     return sizeof(float) * 2 * SYM_ACC + sizeof(float) * 2 * SYM_F * (Q * 3 + 3 + 9 + 2) +
-           sizeof(int) * (4 * 3 * SYM_F + SYM_V + 1 + SYM_S);
+           sizeof(int) * (3 * 3 * SYM_F + SYM_INC);
 }
 
 template <int Q>
@@ -447,12 +479,11 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
     T *yn = yq + SYM_F * Q * 3;                // [3][sigma]
     T *yc = yn + 3 * SYM_F;                    // [9][sigma]
     T *ya = yc + 9 * SYM_F;                    // [sigma]
-    T *yp = ya + SYM_F;                        // [sigma]: plane offset y . n_sigma
+    T *yp = ya + SYM_F;                        // [sigma]: plane offset y . n_sigma (a reflection keeps it)
     int *xgv = reinterpret_cast<int *>(yp + SYM_F);  // [tau][3] global vertex ids
     int *xlv = xgv + 3 * SYM_F;                      // [tau][3] tile-local vertex ids
     int *ygv = xlv + 3 * SYM_F;                      // [3][sigma]
-    int *ylv = ygv + 3 * SYM_F;                      // [3][sigma]
-    int *inc_start = ylv + 3 * SYM_F;                // [vJ + 1]: slot-face indices of tile J's vertex vJ
+    int *inc_start = ygv + 3 * SYM_F;                // [vJ + 1]: slot-face indices of tile J's vertex vJ
     int *inc_list = inc_start + SYM_V + 1;           //   are inc_list[inc_start[vJ] .. inc_start[vJ + 1])
 
     // unordered tile pair (I, J), I <= J, from the linear block index
@@ -472,48 +503,55 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
     static_assert((2 * SYM_ACC) % 4 == 0, "accumulators are zeroed as float4");
     for (int i = tid; i < 2 * SYM_ACC / 4; i += REG_THREADS)
         reinterpret_cast<float4 *>(acc_re)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int i = tid; i < nI * Q * 3; i += REG_THREADS) xq[i] = g.qpts[(size_t)t0 * Q * 3 + i];
+    // the tile arrays: every copy in flight at once, one wait
+    for (int i = tid; i < nI * Q * 3; i += REG_THREADS) cp_async4(&xq[i], &g.qpts[(size_t)t0 * Q * 3 + i]);
     for (int i = tid; i < nI * 3; i += REG_THREADS) {
-        xn[i] = g.normal[(size_t)t0 * 3 + i];
-        xgv[i] = g.gvert[(size_t)t0 * 3 + i];
-        xlv[i] = g.t_local[(size_t)t0 * 3 + i];
+        cp_async4(&xn[i], &g.normal[(size_t)t0 * 3 + i]);
+        cp_async4(&xgv[i], &g.gvert[(size_t)t0 * 3 + i]);
+        cp_async4(&xlv[i], &g.t_local[(size_t)t0 * 3 + i]);
     }
-    for (int i = tid; i < nI * 9; i += REG_THREADS) xc[i] = g.curl[(size_t)t0 * 9 + i];
-    for (int i = tid; i < nI; i += REG_THREADS) xa[i] = g.area[t0 + i];
-    // (an image pass reflects tile J: pairs (tau, S sigma) and (sigma, S tau)
-    // have the same distances, |x - Sy| = |Sx - y|, and swap dn_s / dn_t)
+    for (int i = tid; i < nI * 9; i += REG_THREADS) cp_async4(&xc[i], &g.curl[(size_t)t0 * 9 + i]);
+    for (int i = tid; i < nI; i += REG_THREADS) {
+        cp_async4(&xa[i], &g.area[t0 + i]);
+        cp_async4(&xp[i], &g.plane[t0 + i]);
+    }
     for (int i = tid; i < nJ * Q * 3; i += REG_THREADS) {
         const int s = i / (Q * 3), j = i % (Q * 3);
-        yq[j * SYM_F + s] = g.xs[j % 3] * g.qpts[(size_t)s0 * Q * 3 + i];
+        cp_async4(&yq[j * SYM_F + s], &g.qpts[(size_t)s0 * Q * 3 + i]);
     }
     for (int i = tid; i < nJ * 3; i += REG_THREADS) {
         const int s = i / 3, j = i % 3;
-        yn[j * SYM_F + s] = g.xs[j] * g.normal[(size_t)s0 * 3 + i];
-        ygv[j * SYM_F + s] = g.gvert[(size_t)s0 * 3 + i];
-        ylv[j * SYM_F + s] = g.t_local[(size_t)s0 * 3 + i];
+        cp_async4(&yn[j * SYM_F + s], &g.normal[(size_t)s0 * 3 + i]);
+        cp_async4(&ygv[j * SYM_F + s], &g.gvert[(size_t)s0 * 3 + i]);
     }
     for (int i = tid; i < nJ * 9; i += REG_THREADS) {
         const int s = i / 9, j = i % 9;
-        yc[j * SYM_F + s] = g.xdet * g.xs[j % 3] * g.curl[(size_t)s0 * 9 + i];
+        cp_async4(&yc[j * SYM_F + s], &g.curl[(size_t)s0 * 9 + i]);
     }
-    for (int i = tid; i < nJ; i += REG_THREADS) ya[i] = g.area[s0 + i];
-    __syncthreads();
-    for (int i = tid; i < nI; i += REG_THREADS)
-        xp[i] = xq[i * Q * 3] * xn[3 * i] + xq[i * Q * 3 + 1] * xn[3 * i + 1] + xq[i * Q * 3 + 2] * xn[3 * i + 2];
-    for (int i = tid; i < nJ; i += REG_THREADS)
-        yp[i] = yq[i] * yn[i] + yq[SYM_F + i] * yn[SYM_F + i] + yq[2 * SYM_F + i] * yn[2 * SYM_F + i];
-    // incidences of tile J's vertices, in slot-face order: vertex v's list
-    // starts after every incidence of a smaller local vertex
-    if (tid < nvJ) {
-        int before = 0;
-        for (int s = 0; s < 3 * SYM_F; ++s)
-            if (s % SYM_F < nJ) before += ylv[s] < tid;
-        inc_start[tid] = before;
-        for (int s = 0; s < 3 * SYM_F; ++s)
-            if (s % SYM_F < nJ && ylv[s] == tid) inc_list[before++] = s;
-        if (tid == nvJ - 1) inc_start[nvJ] = before;
+    for (int i = tid; i < nJ; i += REG_THREADS) {
+        cp_async4(&ya[i], &g.area[s0 + i]);
+        cp_async4(&yp[i], &g.plane[s0 + i]);
     }
+    for (int i = tid; i < SYM_INC; i += REG_THREADS) cp_async4(&inc_start[i], &g.t_inc[(size_t)J * SYM_INC + i]);
+    cp_async_wait_all();
     __syncthreads();
+    if (g.image) {
+        // an image pass reflects tile J: pairs (tau, S sigma) and (sigma, S tau)
+        // have the same distances, |x - Sy| = |Sx - y|, and swap dn_s / dn_t
+        for (int i = tid; i < nJ * Q * 3; i += REG_THREADS) {
+            const int s = i / (Q * 3), j = i % (Q * 3);
+            yq[j * SYM_F + s] *= g.xs[j % 3];
+        }
+        for (int i = tid; i < nJ * 3; i += REG_THREADS) {
+            const int s = i / 3, j = i % 3;
+            yn[j * SYM_F + s] *= g.xs[j];
+        }
+        for (int i = tid; i < nJ * 9; i += REG_THREADS) {
+            const int s = i / 9, j = i % 9;
+            yc[j * SYM_F + s] *= g.xdet * g.xs[j % 3];
+        }
+        __syncthreads();
+    }
 
     const T k = g.k, eta = g.eta;
     const T inv4pi = T(0.07957747154594767);  // 1 / (4 pi)
@@ -1076,6 +1114,8 @@ static void launch_regular(beat_b200_ctx *c, double k, double eta, int img, int 
     g.s_vstart = c->trial_tiles.vert_start.as<int>();
     g.s_verts = c->trial_tiles.verts.as<int>();
     g.s_local = c->trial_tiles.local_vert.as<int>();
+    g.s_inc = c->trial_tiles.incidence.as<int>();
+    BB_REQUIRE(c->trial_tiles.inc_stride() == REG_INC, BEAT_B200_STATE, "assembly: trial tile shape mismatch");
     g.A = c->ws.A.as<Cx<T>>();
     g.B = c->ws.rhs_cached ? c->ws.B.as<Cx<T>>() : nullptr;
     g.q = q;
@@ -1109,12 +1149,15 @@ static void launch_sym(beat_b200_ctx *c, double k, double eta, int img, int R, c
     g.normal = c->pos_normal32.as<float>();
     g.curl = c->pos_curl32.as<float>();
     g.area = c->pos_area32.as<float>();
+    g.plane = c->pos_plane32.as<float>();
     g.gvert = c->pos_gvert.as<int>();
     g.face_id = c->pos_face.as<int>();
     g.t_fstart = c->sym_tiles.face_start.as<int>();
     g.t_vstart = c->sym_tiles.vert_start.as<int>();
     g.t_verts = c->sym_tiles.verts.as<int>();
     g.t_local = c->sym_tiles.local_vert.as<int>();
+    g.t_inc = c->sym_tiles.incidence.as<int>();
+    BB_REQUIRE(c->sym_tiles.inc_stride() == SYM_INC, BEAT_B200_STATE, "assembly: square tile shape mismatch");
     g.s_fstart = g.s_vstart = g.s_verts = g.s_local = nullptr;
     g.A = c->ws.A.as<Cx<float>>();
     g.B = c->ws.rhs_cached ? c->ws.B.as<Cx<float>>() : nullptr;

@@ -256,10 +256,25 @@ static void build_tiling(Tiling &t, int max_faces, int max_verts, const std::vec
     t.tile_faces = max_faces;
     t.tile_verts = max_verts;
     t.ntiles = (int)fstart.size() - 1;
+    // vertex -> slot-face incidences of every tile (counting sort, s increasing)
+    const int stride = t.inc_stride();
+    std::vector<int> inc((size_t)t.ntiles * stride, 0);
+    for (int ti = 0; ti < t.ntiles; ++ti) {
+        const int f0 = fstart[ti], nf = fstart[ti + 1] - f0, nv = vstart[ti + 1] - vstart[ti];
+        int *start = &inc[(size_t)ti * stride], *list = start + max_verts + 1;
+        for (int b = 0; b < 3; ++b)
+            for (int f = 0; f < nf; ++f) ++start[local[3 * (size_t)(f0 + f) + b] + 1];
+        for (int v = 0; v < nv; ++v) start[v + 1] += start[v];
+        std::vector<int> fill(start, start + nv);
+        for (int b = 0; b < 3; ++b)
+            for (int f = 0; f < nf; ++f) list[fill[local[3 * (size_t)(f0 + f) + b]]++] = b * max_faces + f;
+        for (int v = nv + 1; v <= max_verts; ++v) start[v] = start[nv];
+    }
     upload(t.face_start, fstart);
     upload(t.vert_start, vstart);
     upload(t.verts, verts);
     upload(t.local_vert, local);
+    upload(t.incidence, inc);
 }
 
 // element-pair kernel tile shapes (must match assembly.cu)
@@ -415,7 +430,7 @@ void set_mesh(beat_b200_ctx *c, int V, const double *verts, int F, const int32_t
 
     std::vector<int> pos_gv(3 * (size_t)F);
     std::vector<double> pq64(3 * (size_t)F * Q), pn64(3 * (size_t)F), pc64(9 * (size_t)F), pa64(F);
-    std::vector<float> pq32(3 * (size_t)F * Q), pn32(3 * (size_t)F), pc32(9 * (size_t)F), pa32(F);
+    std::vector<float> pq32(3 * (size_t)F * Q), pn32(3 * (size_t)F), pc32(9 * (size_t)F), pa32(F), pp32(F);
     for (int p = 0; p < F; ++p) {
         int f = order[p];
         for (int i = 0; i < 3; ++i) {
@@ -433,6 +448,9 @@ void set_mesh(beat_b200_ctx *c, int V, const double *verts, int F, const int32_t
         }
         pa64[p] = c->areas[f];
         pa32[p] = (float)c->areas[f];
+        // every point y of a flat face has the same y . n (FP32, multiply then two fused adds)
+        const float *q0 = &pq32[3 * (size_t)p * Q], *n = &pn32[3 * (size_t)p];
+        pp32[p] = std::fmaf(q0[2], n[2], std::fmaf(q0[1], n[1], q0[0] * n[0]));
     }
     upload(c->pos_face, order);
     upload(c->pos_qpts64, pq64);
@@ -443,6 +461,7 @@ void set_mesh(beat_b200_ctx *c, int V, const double *verts, int F, const int32_t
     upload(c->pos_curl32, pc32);
     upload(c->pos_area64, pa64);
     upload(c->pos_area32, pa32);
+    upload(c->pos_plane32, pp32);
     upload(c->pos_gvert, pos_gv);
     build_tiling(c->test_tiles, TEST_TILE_FACES, TEST_TILE_VERTS, pos_gv, F);
     build_tiling(c->trial_tiles, TRIAL_TILE_FACES, TRIAL_TILE_VERTS, pos_gv, F);
@@ -737,7 +756,8 @@ int64_t device_bytes(const beat_b200_ctx *c) {
                             &w.small, &w.q, &w.small_solve, &w.dinv, &w.field, &w.io, &w.qeff, &w.grad})
         s += (int64_t)b->bytes;
     for (const DevBuf *b : {&c->pos_face, &c->pos_qpts64, &c->pos_qpts32, &c->pos_normal64, &c->pos_normal32,
-                            &c->pos_curl64, &c->pos_curl32, &c->pos_area64, &c->pos_area32, &c->pos_gvert,
+                            &c->pos_curl64, &c->pos_curl32, &c->pos_area64, &c->pos_area32, &c->pos_plane32,
+                            &c->pos_gvert,
                             &c->d_verts, &c->d_faces, &c->d_normals, &c->d_areas, &c->d_curls, &c->d_qpts,
                             &c->vf_start, &c->vf_face, &c->adm, &c->ip_test, &c->ip_trial, &c->ip_rule,
                             &c->ip_img, &c->ip_jac, &c->ip_nn, &c->rw_vert, &c->rw_weight,
@@ -745,7 +765,8 @@ int64_t device_bytes(const beat_b200_ctx *c) {
                             &c->rule_data, &c->status, &c->barrier})
         s += (int64_t)b->bytes;
     for (const Tiling *t : {&c->test_tiles, &c->trial_tiles, &c->sym_tiles})
-        s += (int64_t)(t->face_start.bytes + t->vert_start.bytes + t->verts.bytes + t->local_vert.bytes);
+        s += (int64_t)(t->face_start.bytes + t->vert_start.bytes + t->verts.bytes + t->local_vert.bytes +
+                       t->incidence.bytes);
     return s;
 }
 

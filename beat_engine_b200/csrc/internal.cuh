@@ -98,6 +98,11 @@ struct Tiling {
     DevBuf vert_start;    // ntiles + 1
     DevBuf verts;         // concatenated global vertex ids per tile
     DevBuf local_vert;    // F x 3 (by sorted position): index of each face vertex in its tile
+    // per tile, inc_stride() ints: start[tile_verts + 1] then list[3 tile_faces]; the
+    // slot-face indices s = b * tile_faces + f (vertex slot b of the tile's face f)
+    // of local vertex v are list[start[v] .. start[v + 1]), in increasing s
+    DevBuf incidence;
+    int inc_stride() const { return tile_verts + 1 + 3 * tile_faces; }
 };
 
 struct Workspace {
@@ -157,6 +162,7 @@ struct beat_b200_ctx {
     bb::DevBuf pos_curl32;
     bb::DevBuf pos_area64;        // F
     bb::DevBuf pos_area32;
+    bb::DevBuf pos_plane32;       // F: plane offset (first rule point) . normal, FP32
     bb::DevBuf pos_gvert;         // F x 3 global vertex ids
     bb::Tiling test_tiles, trial_tiles;
     bb::Tiling sym_tiles;         // square tiles of the symmetric element-pair kernel
