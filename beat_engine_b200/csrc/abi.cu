@@ -170,10 +170,11 @@ void solve_core(beat_b200_ctx *c, double k, double eta, int R, const double *d_q
 // ---------------------------------------------------------------------------
 // frequency sweep over solve lanes
 // ---------------------------------------------------------------------------
-// lanes per sweep: measured on B200 at F = 20,480, R = 16, mixed form (24
-// frequencies, mean of three runs): 2 lanes 10.3, 3 lanes 10.7, 4 lanes 11.2,
-// 6 lanes 10.9 freq-solves/s
-constexpr int SWEEP_LANES = 4;
+// lanes per sweep, measured on B200 at F = 20,480, R = 16, 24 frequencies:
+// mixed form 4 lanes 14.5, 6 lanes 15.0, 8 lanes 14.8 freq-solves/s (the
+// end-to-end sweep 15.0, 15.8, 15.9); FP64 form 4 lanes 4.19, 6 lanes 3.49
+// (its lanes are twice the size and its assembly alone fills the GPU)
+constexpr int SWEEP_LANES = 6, SWEEP_LANES_FP64 = 4;
 
 // lane i of c (lane 0 is c itself); created on first use with c's mesh
 beat_b200_ctx *sweep_lane(beat_b200_ctx *c, int i) {
@@ -196,16 +197,17 @@ static int64_t held_matrix_bytes(const beat_b200_ctx *l) {
     return (int64_t)(l->ws.A.bytes + l->ws.Aop.bytes + l->ws.B.bytes);
 }
 
-// How many lanes to run: up to SWEEP_LANES, as many as there are frequencies,
+// How many lanes to run: up to SWEEP_LANES (SWEEP_LANES_FP64 in the FP64
+// form), as many as there are frequencies,
 // and only as many as can hold a system matrix (with the FP32 operator copy in
 // the mixed form, and the N x F mapping when the right-hand sides may be
 // cached) beside a 512 MiB margin in the free device memory; buffers a lane
 // already holds count as available.  Lane 0 always runs.
 static int sweep_lane_count(beat_b200_ctx *c, int nfreq, const beat_b200_opts &o, int R) {
-    const int want = std::min(SWEEP_LANES, nfreq);
+    const bool fp64 = o.precision == BEAT_B200_FP64;
+    const int want = std::min(fp64 ? SWEEP_LANES_FP64 : SWEEP_LANES, nfreq);
     if (want <= 1) return 1;
     const int64_t ld = ((int64_t)c->V + 127) / 128 * 128;
-    const bool fp64 = o.precision == BEAT_B200_FP64;
     const int64_t csz = fp64 ? 16 : 8;
     const int req = rhs_request(o);
     const bool may_cache =

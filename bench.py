@@ -14,7 +14,8 @@ for all R.
 
 ``value``: device-timed throughput with q already in HBM: the K timed steps
 (frequencies) run as one beat_b200_sweep_device call, which pipelines them over
-up to four solve lanes (one frequency's assembly beside another's factorisation).
+up to six solve lanes, four in the FP64 form (one frequency's assembly beside
+another's factorisation).
 ``e2e``: the same through the host C-ABI sweep (beat_b200_sweep) from pinned
 host buffers.  ``stages_ms`` are one frequency solved alone.
 
@@ -187,7 +188,7 @@ def config_dict(args, mesh):
             "precision_form": args.precision, "lu_split_terms": args.split,
             "l2": "inputs larger than L2: every step rewrites A (N^2 complex) and the N x F RHS operator",
             "parallelism": f"frequency replicas x{args.gpus} (no collective); "
-                           "up to 4 solve lanes per GPU (pipelined frequency sweep)"}
+                           "up to 6 solve lanes per GPU, 4 in the FP64 form (pipelined frequency sweep)"}
 
 
 # --------------------------------------------------------------------------

@@ -254,8 +254,9 @@ int32_t beat_b200_resolve_noalloc(beat_b200_ctx *ctx, int32_t R, const void *d_b
  * which calls solve_exterior_direct_cuda once per frequency (:1338) and
  * overlaps the next frequency's assembly with the current solve only on its
  * Metal path (start_sweep_assembly_pipeline, :1265).  Frequencies are
- * pipelined over up to four solve lanes (each with its own stream and
- * workspace, the further ones created on first use with a copy of the mesh;
+ * pipelined over up to six solve lanes, four in the FP64 form (each with its
+ * own stream and workspace, the further ones created on first use with a
+ * copy of the mesh;
  * no more lanes than frequencies, nor than have room for a system matrix in
  * the free device memory), one host thread per lane: one frequency's
  * assembly runs beside the others' factorisations.

@@ -41,7 +41,7 @@ def sweep_inputs(F, R, ks, seed):
 
 @pytest.mark.parametrize("precision,tol", [(_lib.MIXED_FP32_IR, 1e-6), (_lib.FP64, 1e-10)])
 def test_sweep_matches_one_solve_per_frequency(ctx, sphere3, precision, tol):
-    ks = [7.0, 36.6, -52.0, 110.0, 20.0]  # both phasor signs, odd count over two lanes
+    ks = [7.0, 36.6, -52.0, 110.0, 20.0]  # both phasor signs, one frequency per lane
     k, eta, q = sweep_inputs(sphere3.num_faces, 3, ks, 5)
     dirs = M.fibonacci_sphere(17, 1.0)
     opts = _lib.Context.opts(precision)
