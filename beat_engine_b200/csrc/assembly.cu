@@ -38,6 +38,7 @@ __constant__ double c_rw64[3][6];
 __constant__ double c_rb64[3][6][3];
 __constant__ float c_rw32[3][6];
 __constant__ float c_rb32[3][6][3];
+__constant__ float2 c_rb32x2[3][6][3];  // (b, b): the packed-pair operand of the same basis value
 
 template <typename T> struct RuleRef;
 template <> struct RuleRef<double> {
@@ -70,6 +71,11 @@ void upload_rule_tables(const std::vector<double> &pts, const std::vector<double
     BB_CUDA(cudaMemcpyToSymbol(c_rb64, b64, sizeof(b64)));
     BB_CUDA(cudaMemcpyToSymbol(c_rw32, w32, sizeof(w32)));
     BB_CUDA(cudaMemcpyToSymbol(c_rb32, b32, sizeof(b32)));
+    float2 b32x2[3][6][3];
+    for (int i = 0; i < 3; ++i)
+        for (int q = 0; q < 6; ++q)
+            for (int a = 0; a < 3; ++a) b32x2[i][q][a] = make_float2(b32[i][q][a], b32[i][q][a]);
+    BB_CUDA(cudaMemcpyToSymbol(c_rb32x2, b32x2, sizeof(b32x2)));
 }
 
 __device__ __forceinline__ void sincos_t(double x, double *s, double *c) { sincos_cw(x, s, c); }
@@ -88,6 +94,31 @@ __device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
 
 __device__ __forceinline__ void red_add(double *p, double v) { atomicAdd(p, v); }
 __device__ __forceinline__ void red_add(float *p, float v) { atomicAdd(p, v); }
+// Packed FP32 pairs (sm_100 f32x2 arithmetic): two lanes of one instruction,
+// (re, im) of a complex value or one value twice.
+using F2 = unsigned long long;
+__device__ __forceinline__ F2 pk2(float lo, float hi) {
+    F2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void up2(F2 v, float &lo, float &hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) {
+    F2 d;
+    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ F2 add2(F2 a, F2 b) {
+    F2 d;
+    asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ F2 rule_b2(int r, int q, int a) {
+    return *reinterpret_cast<const F2 *>(&c_rb32x2[r][q][a]);
+}
+
 // Adds v[i] to base[off[i]] for every i, atomically.  Shared-memory float
 // adds are compare-and-swap loops, each a dependent load -> add -> swap
 // chain; here the loads, then the swaps, of all N adds are in flight
@@ -581,9 +612,10 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
             const T x0 = xq[(ti * Q + qt) * 3], x1 = xq[(ti * Q + qt) * 3 + 1], x2 = xq[(ti * Q + qt) * 3 + 2];
             const T wt = RuleRef<T>::w(RI, qt) * inv4pi;
             const T xns = dsig - (x0 * nsx + x1 * nsy + x2 * nsz);  // r . n_sigma for every y on sigma
-            T S0r = 0, S0i = 0, S1r = 0, S1i = 0, S2r = 0, S2i = 0;  // order 1: sum over trial points
-            T P0r = 0, P0i = 0, P1r = 0, P1i = 0, P2r = 0, P2i = 0;  // order 2: sum over test points
-            T Gr = 0, Gi = 0, Wr = 0, Wi = 0;
+            // order 1 sums over the trial points S_b, order 2 sums P_b, the green
+            // sum G and -W (W = sum of c dG/dr), each a packed (re, im) pair
+            F2 S0 = 0, S1 = 0, S2 = 0, P0 = 0, P1 = 0, P2 = 0, G2 = 0, NW = 0;
+            const T nxns = -xns;
 #pragma unroll
             for (int qs = 0; qs < Q; ++qs) {
                 const T y0 = yq[(qs * 3) * SYM_F + sj], y1 = yq[(qs * 3 + 1) * SYM_F + sj],
@@ -597,34 +629,36 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
                 const T gr = cs_ * scl, gi = sn_ * scl;
                 const T gsr = -gr * ir - gi * k;
                 const T gsi = gr * k - gi * ir;
-                const T a = xns * ir;                                         // r . n_sigma / r
-                const T c = (dtau - (y0 * ntx + y1 * nty + y2 * ntz)) * ir;  // -r . n_tau / r
-                const T b0 = RuleRef<T>::b(RI, qs, 0), b1v = RuleRef<T>::b(RI, qs, 1),
-                        b2v = RuleRef<T>::b(RI, qs, 2);
-                // order 1
-                const T lr1 = k2n * gi - gsr * a, li1 = -(gsi * a + k2n * gr);
-                Gr += gr;
-                Gi += gi;
-                Wr += c * gsr;
-                Wi += c * gsi;
-                S0r += b0 * lr1;
-                S0i += b0 * li1;
-                S1r += b1v * lr1;
-                S1i += b1v * li1;
-                S2r += b2v * lr1;
-                S2i += b2v * li1;
-                // order 2
-                const T lr2 = k2n * gi - gsr * c, li2 = -(gsi * c + k2n * gr);
-                P0r += b0 * lr2;
-                P0i += b0 * li2;
-                P1r += b1v * lr2;
-                P1i += b1v * li2;
-                P2r += b2v * lr2;
-                P2i += b2v * li2;
-                const T ea = eta * a;
+                const T na = nxns * ir;                                        // -r . n_sigma / r
+                const T nc = ((y0 * ntx + y1 * nty + y2 * ntz) - dtau) * ir;  // r . n_tau / r
+                const F2 g2 = pk2(gr, gi), gs = pk2(gsr, gsi);
+                const F2 kk = pk2(k2n * gi, -(k2n * gr));
+                const F2 l1 = fma2(pk2(na, na), gs, kk);  // order 1: -i k2n g - grad*dn_s
+                const F2 l2 = fma2(pk2(nc, nc), gs, kk);  // order 2: dn_s = c
+                G2 = add2(G2, g2);
+                NW = fma2(pk2(nc, nc), gs, NW);
+                const F2 b0 = rule_b2(RI, qs, 0), b1 = rule_b2(RI, qs, 1), b2 = rule_b2(RI, qs, 2);
+                S0 = fma2(b0, l1, S0);
+                S1 = fma2(b1, l1, S1);
+                S2 = fma2(b2, l1, S2);
+                P0 = fma2(b0, l2, P0);
+                P1 = fma2(b1, l2, P1);
+                P2 = fma2(b2, l2, P2);
+                const T ea = -eta * na;
                 U2[qs][0] += ea * gsi - gr;  // -g - i eta grad*dn_t with dn_t = a
                 U2[qs][1] -= ea * gsr + gi;
             }
+            T S0r, S0i, S1r, S1i, S2r, S2i, P0r, P0i, P1r, P1i, P2r, P2i, Gr, Gi, Wr, Wi;
+            up2(S0, S0r, S0i);
+            up2(S1, S1r, S1i);
+            up2(S2, S2r, S2i);
+            up2(P0, P0r, P0i);
+            up2(P1, P1r, P1i);
+            up2(P2, P2r, P2i);
+            up2(G2, Gr, Gi);
+            up2(NW, Wr, Wi);
+            Wr = -Wr;
+            Wi = -Wi;
             const T Ur = -Gr + eta * Wi, Ui = -Gi - eta * Wr;
             cr += Gr;
             ci += Gi;
