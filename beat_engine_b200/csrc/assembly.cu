@@ -170,6 +170,16 @@ __device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
                  : "memory");
 }
+// the same for one 4- or 8-byte element
+template <typename E> __device__ __forceinline__ void cp_async_el(E *smem, const E *gmem) {
+    static_assert(sizeof(E) == 4 || sizeof(E) == 8, "cp.async element of 4 or 8 bytes");
+    if constexpr (sizeof(E) == 4)
+        cp_async4(smem, gmem);
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+                     "l"(gmem)
+                     : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
@@ -271,35 +281,45 @@ __global__ void __launch_bounds__(REG_THREADS, sizeof(T) == 4 ? 3 : 2) regular_p
 
     for (int i = tid; i < VT * REG_S; i += REG_THREADS) sC[i] = Cx<T>{T(0), T(0)};
     for (int i = tid; i < VT * TS; i += REG_THREADS) sB[i] = Cx<T>{T(0), T(0)};
-    for (int i = tid; i < nt * Q * 3; i += REG_THREADS) tq[i] = g.qpts[(size_t)t0 * Q * 3 + i];
+    // the tile arrays: every copy in flight at once, one wait
+    for (int i = tid; i < nt * Q * 3; i += REG_THREADS) cp_async_el(&tq[i], &g.qpts[(size_t)t0 * Q * 3 + i]);
     for (int i = tid; i < nt * 3; i += REG_THREADS) {
-        tn[i] = g.normal[(size_t)t0 * 3 + i];
-        tgv[i] = g.gvert[(size_t)t0 * 3 + i];
-        tlv[i] = g.t_local[(size_t)t0 * 3 + i];
+        cp_async_el(&tn[i], &g.normal[(size_t)t0 * 3 + i]);
+        cp_async_el(&tgv[i], &g.gvert[(size_t)t0 * 3 + i]);
+        cp_async_el(&tlv[i], &g.t_local[(size_t)t0 * 3 + i]);
     }
-    for (int i = tid; i < nt * 9; i += REG_THREADS) tc[i] = g.curl[(size_t)t0 * 9 + i];
-    for (int i = tid; i < nt; i += REG_THREADS) ta[i] = g.area[t0 + i];
+    for (int i = tid; i < nt * 9; i += REG_THREADS) cp_async_el(&tc[i], &g.curl[(size_t)t0 * 9 + i]);
+    for (int i = tid; i < nt; i += REG_THREADS) cp_async_el(&ta[i], &g.area[t0 + i]);
     for (int i = tid; i < ns * Q * 3; i += REG_THREADS) {
         int s = i / (Q * 3), j = i % (Q * 3);
-        sq[j * TS + s] = g.xs[j % 3] * g.qpts[(size_t)s0 * Q * 3 + i];
+        cp_async_el(&sq[j * TS + s], &g.qpts[(size_t)s0 * Q * 3 + i]);
     }
     for (int i = tid; i < ns * 3; i += REG_THREADS) {
         int s = i / 3, j = i % 3;
-        sn[j * TS + s] = g.xs[j] * g.normal[(size_t)s0 * 3 + i];
-        sgv[j * TS + s] = g.gvert[(size_t)s0 * 3 + i];
+        cp_async_el(&sn[j * TS + s], &g.normal[(size_t)s0 * 3 + i]);
+        cp_async_el(&sgv[j * TS + s], &g.gvert[(size_t)s0 * 3 + i]);
     }
     for (int i = tid; i < ns * 9; i += REG_THREADS) {
         int s = i / 9, j = i % 9;
-        sc[j * TS + s] = g.xdet * g.xs[j % 3] * g.curl[(size_t)s0 * 9 + i];
+        cp_async_el(&sc[j * TS + s], &g.curl[(size_t)s0 * 9 + i]);
     }
-    for (int i = tid; i < ns; i += REG_THREADS) sa[i] = g.area[s0 + i];
-    for (int i = tid; i < REG_INC; i += REG_THREADS) inc_start[i] = g.s_inc[(size_t)blockIdx.x * REG_INC + i];
+    for (int i = tid; i < ns; i += REG_THREADS) cp_async_el(&sa[i], &g.area[s0 + i]);
+    for (int i = tid; i < REG_INC; i += REG_THREADS)
+        cp_async_el(&inc_start[i], &g.s_inc[(size_t)blockIdx.x * REG_INC + i]);
+    cp_async_wait_all();
     __syncthreads();
     // every point y of a flat face has the same y . n
     for (int i = tid; i < nt; i += REG_THREADS)
         tpl[i] = tq[i * Q * 3] * tn[3 * i] + tq[i * Q * 3 + 1] * tn[3 * i + 1] + tq[i * Q * 3 + 2] * tn[3 * i + 2];
-    for (int i = tid; i < ns; i += REG_THREADS)
-        spl[i] = sq[i] * sn[i] + sq[TS + i] * sn[TS + i] + sq[2 * TS + i] * sn[2 * TS + i];
+    if (tid < ns) {  // one thread per trial face: its image reflection, then its plane offset
+        if (g.image) {
+            // an image pass reflects the trial tile (signs xs, curls also by det)
+            for (int j = 0; j < Q * 3; ++j) sq[j * TS + tid] *= g.xs[j % 3];
+            for (int j = 0; j < 3; ++j) sn[j * TS + tid] *= g.xs[j];
+            for (int j = 0; j < 9; ++j) sc[j * TS + tid] *= g.xdet * g.xs[j % 3];
+        }
+        spl[tid] = sq[tid] * sn[tid] + sq[TS + tid] * sn[TS + tid] + sq[2 * TS + tid] * sn[2 * TS + tid];
+    }
     __syncthreads();
 
     const T k = g.k, eta = g.eta;
