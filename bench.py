@@ -392,7 +392,7 @@ def measured_peaks():
 # and the algorithmic output of that launch (A: N^2 c64, B: N x F c64).  Traffic grows with the
 # output written (the zeroed A and B are read back by the red.global.add flush), so a launch on
 # another mesh is scaled by its output bytes.
-SYM_TRAFFIC_F5120 = {"bytes": 159.081728e6 + 121.277952e6, "output_bytes": 2562 * 2562 * 8 + 2562 * 5120 * 8}
+SYM_TRAFFIC_F5120 = {"bytes": 158.986496e6 + 119.639296e6, "output_bytes": 2562 * 2562 * 8 + 2562 * 5120 * 8}
 
 
 def roofline(args, mesh, stages, peaks):
