@@ -229,7 +229,7 @@ template <typename T> struct RegArgs {
     const int *gvert;   // F x 3
     const int *face_id; // F
     const int *t_fstart, *t_vstart, *t_verts, *t_local;
-    const int *s_fstart, *s_vstart, *s_verts, *s_local;
+    const int *s_fstart, *s_vstart, *s_verts;
     const int *t_inc = nullptr, *s_inc = nullptr;  // per-tile vertex incidences (Tiling::incidence)
     Cx<T> *A;
     Cx<T> *B;
@@ -1167,7 +1167,6 @@ static void launch_regular(beat_b200_ctx *c, double k, double eta, int img, int 
     g.s_fstart = c->trial_tiles.face_start.as<int>();
     g.s_vstart = c->trial_tiles.vert_start.as<int>();
     g.s_verts = c->trial_tiles.verts.as<int>();
-    g.s_local = c->trial_tiles.local_vert.as<int>();
     g.s_inc = c->trial_tiles.incidence.as<int>();
     BB_REQUIRE(c->trial_tiles.inc_stride() == REG_INC, BEAT_B200_STATE, "assembly: trial tile shape mismatch");
     g.A = c->ws.A.as<Cx<T>>();
@@ -1212,7 +1211,7 @@ static void launch_sym(beat_b200_ctx *c, double k, double eta, int img, int R, c
     g.t_local = c->sym_tiles.local_vert.as<int>();
     g.t_inc = c->sym_tiles.incidence.as<int>();
     BB_REQUIRE(c->sym_tiles.inc_stride() == SYM_INC, BEAT_B200_STATE, "assembly: square tile shape mismatch");
-    g.s_fstart = g.s_vstart = g.s_verts = g.s_local = nullptr;
+    g.s_fstart = g.s_vstart = g.s_verts = nullptr;
     g.A = c->ws.A.as<Cx<float>>();
     g.B = c->ws.rhs_cached ? c->ws.B.as<Cx<float>>() : nullptr;
     g.q = q;
