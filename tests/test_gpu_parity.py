@@ -102,6 +102,25 @@ def test_other_quadrature_orders(order, sorder):
     assert rel(A, Ao) <= 1e-12 and rel(b, bo) <= 1e-12
 
 
+@pytest.mark.parametrize("order", [1, 2])
+def test_fp32_assembly_other_quadrature_orders(order):
+    """The FP32 element-pair kernel at its 1- and 3-point rules (the 6-point
+    rule is the test above), cached and matrix-free right-hand sides, at the
+    FP32 tolerance."""
+    mesh = M.reference_sphere(0.1, 2)
+    k = 15.0
+    q = random_q(mesh.num_faces, 2, 15)
+    Ao, bo = oracle.assemble(mesh, k, 1.0 / k, q, quad_order=order, sing_order=2)
+    with _lib.Context(0) as c:
+        c.set_mesh(mesh.vertices, mesh.faces, order, 2)
+        A, b = c.assemble(k, 1.0 / k, q, precision=_lib.MIXED_FP32_IR)
+        assert rel(A, Ao) <= 2e-6 and rel(b, bo) <= 2e-6
+        po = oracle.lu_solve(Ao, bo)
+        for flags in (_lib.FLAG_RHS_CACHED, _lib.FLAG_RHS_MATRIX_FREE):
+            p, d = c.solve(k, 1.0 / k, q, _lib.Context.opts(_lib.MIXED_FP32_IR, flags=flags))
+            assert d["ir_converged"] == 1 and np.all(col_rel(p, po) <= 1e-6), (flags, col_rel(p, po))
+
+
 def test_tiny_tetrahedron_all_pairs_touch():
     mesh = tetrahedron()
     q = random_q(4, 2, 15)
