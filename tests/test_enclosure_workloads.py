@@ -1,5 +1,5 @@
-"""The batched-sweep and adjoint-gradient workloads on the rounded-box
-enclosure (BASELINE configs 3 and 4), at sizes the FP64 oracle runs in
+"""The batched-sweep and adjoint-gradient workloads on a rounded-box
+loudspeaker enclosure with a front piston, at sizes the FP64 oracle runs in
 seconds:
 
 * sweep: a 2k-face enclosure, log-spaced frequencies from 100 Hz to 8 kHz, the
