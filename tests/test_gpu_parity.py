@@ -174,7 +174,7 @@ def test_field_and_farfield_match_oracle(ctx3, sphere3):
 
 @pytest.mark.parametrize("precision", ["float64", "mixed_fp32_ir"])
 def test_analytic_pulsating_sphere_through_reference_interface(sphere3, precision):
-    """Config 0: pulsating sphere, exp(+i omega t), 181 points on a 2 m arc,
+    """The analytic gate: pulsating sphere, exp(+i omega t), 181 points on a 2 m arc,
     against p = rho c u (a/r) (ika/(1+ika)) exp(-ik(r-a)) at 0.05 dB / 0.5 deg."""
     f, a, rho, c = 1000.0, 0.1, 1.21, 343.0
     om = 2 * math.pi * f
