@@ -33,11 +33,25 @@ namespace bb {
 // Bound: FP64 FMA issue (4 DFMA per complex multiply-add).
 // ---------------------------------------------------------------------------
 constexpr int TG_THREADS = 256, TG_RC = 16;
+
+// one 8- or 16-byte element global -> shared through the asynchronous copy
+// unit, or zeros (nothing is read) when `in` is false
+template <typename E> __device__ __forceinline__ void cp_async_zfill(E *smem, const E *gmem, bool in) {
+    static_assert(sizeof(E) == 8 || sizeof(E) == 16, "8- or 16-byte elements");
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = in ? (int)sizeof(E) : 0;
+    if constexpr (sizeof(E) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(gmem), "r"(n) : "memory");
+    else
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(gmem), "r"(n) : "memory");
+}
 template <typename T> struct TgChunk {
     static constexpr int KC = 32;  // K entries per shared-memory chunk (c64 M)
+    static constexpr int STAGE_UNROLL = 1;  // unrolling of the chunk's copy loop (no spills at 128 registers)
 };
 template <> struct TgChunk<double> {
     static constexpr int KC = 16;
+    static constexpr int STAGE_UNROLL = 4;
 };
 
 template <typename T>
@@ -56,20 +70,20 @@ __global__ void __launch_bounds__(TG_THREADS, 2) tall_gemm_kernel(const Cx<T> *M
     for (int e = 0; e < TG_RC; ++e) ar[e] = ai[e] = 0.0;
     for (int k0 = kb; k0 < ke; k0 += KC) {
         const int kn = min(KC, ke - k0);
-        batched_copy<TG_THREADS, 4, Cx<T>>(
-            TG_THREADS * KC,
-            [&](int i) {
-                const int r = i / KC, k = i % KC;  // consecutive threads: consecutive k of one row
-                return (row0 + r < rows && k < kn) ? M[(int64_t)(row0 + r) * ld + k0 + k] : Cx<T>{T(0), T(0)};
-            },
-            [&](int i, Cx<T> v) { sM[(i / KC) * (KC + 1) + i % KC] = v; });
-        batched_copy<TG_THREADS, 2, double2>(
-            KC * TG_RC,
-            [&](int i) {
-                const int c = i / KC, k = i % KC;
-                return (c < rc && k < kn) ? X[(size_t)(r0 + c) * K + k0 + k] : make_double2(0, 0);
-            },
-            [&](int i, double2 v) { sX[(i % KC) * TG_RC + i / KC] = v; });
+        // the chunk of M and of X by asynchronous copies, all in flight at
+        // once; entries past the matrix are zero-filled
+#pragma unroll TgChunk<T>::STAGE_UNROLL
+        for (int i = threadIdx.x; i < TG_THREADS * KC; i += TG_THREADS) {
+            const int r = i / KC, k = i % KC;  // consecutive threads: consecutive k of one row
+            const bool in = row0 + r < rows && k < kn;
+            cp_async_zfill(&sM[r * (KC + 1) + k], in ? &M[(int64_t)(row0 + r) * ld + k0 + k] : M, in);
+        }
+        for (int i = threadIdx.x; i < KC * TG_RC; i += TG_THREADS) {
+            const int c = i / KC, k = i % KC;
+            const bool in = c < rc && k < kn;
+            cp_async_zfill(&sX[k * TG_RC + c], in ? &X[(size_t)(r0 + c) * K + k0 + k] : X, in);
+        }
+        asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
         __syncthreads();
 #pragma unroll 2
         for (int k = 0; k < KC; ++k) {
