@@ -145,6 +145,18 @@ def test_fp64_solve_matches_oracle(ctx3, sphere3, R):
     assert d["precision"] == _lib.FP64
 
 
+@pytest.mark.parametrize("precision,nb,tol", [(_lib.FP64, 32, 1e-10), (_lib.FP64, 64, 1e-10),
+                                               (_lib.FP64, 256, 1e-10), (_lib.MIXED_FP32_IR, 32, 1e-6),
+                                               (_lib.MIXED_FP32_IR, 64, 1e-6), (_lib.MIXED_FP32_IR, 256, 1e-6)])
+def test_panel_widths(ctx3, sphere3, precision, nb, tol):
+    # the LU's panel width (opts.lu_block) other than the default 128
+    k = 36.6
+    q = random_q(sphere3.num_faces, 3, 50)
+    p, d = ctx3.solve(k, 1 / k, q, _lib.Context.opts(precision, lu_block=nb))
+    Ao, bo = oracle.assemble(sphere3, k, 1 / k, q)
+    assert np.all(col_rel(p, oracle.lu_solve(Ao, bo)) <= tol)
+
+
 @pytest.mark.parametrize("split", [1, 3])
 def test_mixed_solve_within_1e6_of_fp64_oracle(ctx3, sphere3, split):
     k = 110.0

@@ -1,9 +1,9 @@
 """Frequency sweep (beat_b200_sweep / beat_b200_sweep_device) against one
 solve per frequency on the same context, through the C ABI.
 
-A sweep runs the same kernels as beat_b200_solve, pipelined over two solve
-lanes; only the order of the floating-point atomic sums in the assembly can
-differ between the two runs.  Tolerances: mixed form relative L2 per column
+A sweep runs the same kernels as beat_b200_solve, pipelined over up to six
+solve lanes (four in FP64); only the order of the floating-point atomic sums
+in the assembly can differ between the two runs.  Tolerances: mixed form relative L2 per column
 <= 1e-6 (the target of the form), FP64 <= 1e-10, far field the same.
 """
 import numpy as np
@@ -55,6 +55,19 @@ def test_sweep_matches_one_solve_per_frequency(ctx, sphere3, precision, tol):
         assert diags[f]["precision"] == precision and diags[f]["lu_ms"] > 0
         if precision == _lib.MIXED_FP32_IR:
             assert diags[f]["ir_converged"] == 1
+
+
+def test_lanes_reused_across_frequencies(ctx, sphere3):
+    # more frequencies than lanes in both forms: each lane solves several in turn
+    ks = [7.0, 20.0, 36.6, -52.0, 64.0, 80.0, 95.0, 110.0, 12.0, 44.0]
+    k, eta, q = sweep_inputs(sphere3.num_faces, 2, ks, 7)
+    for precision, tol in ((_lib.MIXED_FP32_IR, 1e-6), (_lib.FP64, 1e-10)):
+        opts = _lib.Context.opts(precision)
+        p, _, diags = ctx.sweep(k, eta, q, opts)
+        for f in range(len(ks)):
+            pf, _ = ctx.solve(k[f], eta[f], q[:, :, f], opts)
+            assert np.all(col_rel(p[:, :, f], pf) <= tol), (precision, f, col_rel(p[:, :, f], pf))
+            assert diags[f]["precision"] == precision
 
 
 def test_sweep_device_matches_host_sweep(ctx, sphere3):
