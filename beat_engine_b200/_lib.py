@@ -176,6 +176,9 @@ def _c128_f(a, rows: int) -> np.ndarray:
 class Context:
     """One device context per mesh (``beat_b200_create`` .. ``beat_b200_destroy``)."""
 
+    generation = 0  # library calls made through this object (see _check)
+    quad_order = singular_order = 4
+
     def __init__(self, device: int = 0):
         self.lib = load()
         h = ctypes.c_void_p()
@@ -203,6 +206,10 @@ class Context:
         self.close()
 
     def _check(self, st: int):
+        # every library call on this context counts: a caller that must know
+        # whether the context still holds the state it left (autodiff's
+        # backward) compares this counter
+        self.generation += 1
         if st != OK:
             raise BeatB200Error(st, self.lib.beat_b200_last_error(self.handle).decode(errors="replace"))
 
@@ -213,6 +220,7 @@ class Context:
                                                 f.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
                                                 quad_order, singular_order))
         self.V, self.F = v.shape[0], f.shape[0]
+        self.quad_order, self.singular_order = quad_order, singular_order
 
     @staticmethod
     def opts(precision: int = MIXED_FP32_IR, **kw) -> Opts:

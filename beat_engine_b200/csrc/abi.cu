@@ -10,6 +10,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <atomic>
 #include <new>
 #include <thread>
 
@@ -95,6 +96,10 @@ void solve_core(beat_b200_ctx *c, double k, double eta, int R, const double *d_q
     BB_REQUIRE(R >= 1, BEAT_B200_INVALID_ARG, "R must be >= 1");
     BB_REQUIRE(std::isfinite(k) && k != 0.0 && std::isfinite(eta), BEAT_B200_INVALID_ARG,
                "wavenumber must be finite and nonzero");
+    // the factors are overwritten from here on (a workspace change may free
+    // them): they count as current again only once this factorisation has
+    // finished without a timeout or a zero pivot
+    c->ws.lu_valid = 0;
     ensure_workspace(c, o.precision, R, rhs_request(o));
     Workspace &w = c->ws;
     const int n = c->V;
@@ -111,6 +116,7 @@ void solve_core(beat_b200_ctx *c, double k, double eta, int R, const double *d_q
     c->last_eta = eta;
     BB_REQUIRE(!(st & DEV_BARRIER_TIMEOUT), BEAT_B200_TIMEOUT, "LU panel: grid barrier ran out of its wait budget");
     BB_REQUIRE(!(st & DEV_ZERO_PIVOT), BEAT_B200_SINGULAR, "LU: exact zero pivot (singular system)");
+    w.lu_valid = 1;
     IrResult ir{0, 1, 0.0};
     if (o.precision == BEAT_B200_FP64) {
         BB_CUDA(cudaMemcpyAsync(d_x, w.b.p, (size_t)n * R * 16, cudaMemcpyDeviceToDevice, c->stream));
@@ -228,9 +234,12 @@ static int sweep_lane_count(beat_b200_ctx *c, int nfreq, const beat_b200_opts &o
     return lanes;
 }
 
-// Runs work(lane_ctx, f) for f = 0..nfreq-1, frequency f on lane f % L, one
-// host thread per lane (lane 0 on the calling thread).  The first error (by
-// frequency) is rethrown after every lane has stopped.
+// Runs work(lane_ctx, f) for f = 0..nfreq-1, one host thread per lane (lane 0
+// on the calling thread).  Each lane takes the next unclaimed frequency from a
+// shared counter when it finishes one, so a lane that drew cheap frequencies
+// does not idle while another still holds a queue.  After a failure no lane
+// starts another frequency; the first error (by frequency) is rethrown after
+// every lane has stopped.
 template <typename W> void run_sweep(beat_b200_ctx *c, int nfreq, int lanes, W &&work) {
     const int L = std::max(1, std::min(lanes, nfreq));
     std::vector<beat_b200_ctx *> lane(L);
@@ -245,10 +254,12 @@ template <typename W> void run_sweep(beat_b200_ctx *c, int nfreq, int lanes, W &
     }
     std::vector<Error> err(L);
     std::vector<int> err_f(L, -1);
+    std::atomic<int> next{0};
+    std::atomic<bool> failed{false};
     auto body = [&](int i) {
         try {
             BB_CUDA(cudaSetDevice(c->device));
-            for (int f = i; f < nfreq; f += L) {
+            for (int f = next.fetch_add(1); f < nfreq && !failed.load(); f = next.fetch_add(1)) {
                 err_f[i] = f;
                 work(lane[i], f);
             }
@@ -260,12 +271,19 @@ template <typename W> void run_sweep(beat_b200_ctx *c, int nfreq, int lanes, W &
         } catch (...) {
             err[i] = Error{BEAT_B200_CUDA_ERROR, "unexpected exception"};
         }
-        if (err_f[i] >= 0 && lane[i]->stream) cudaStreamSynchronize(lane[i]->stream);
+        if (err_f[i] >= 0) {
+            failed.store(true);
+            if (lane[i]->stream) cudaStreamSynchronize(lane[i]->stream);
+        }
     };
     std::vector<std::thread> th;
     for (int i = 1; i < L; ++i) th.emplace_back(body, i);
     body(0);
     for (auto &t : th) t.join();
+    // lane 0 is this context: its factors now belong to whichever frequency it
+    // solved last, which the caller cannot name, so they are not offered to
+    // beat_b200_resolve_noalloc or beat_b200_adjoint
+    for (int i = 0; i < L; ++i) lane[i]->ws.lu_valid = 0;
     int first = -1;
     for (int i = 0; i < L; ++i)
         if (err_f[i] >= 0 && (first < 0 || err_f[i] < err_f[first])) first = i;
@@ -309,7 +327,14 @@ int32_t beat_b200_create(int32_t device, beat_b200_ctx **out) {
         BB_REQUIRE(prop.major >= 10, BEAT_B200_NO_DEVICE,
                    std::string("libbeatb200 is built for sm_100a; device is ") + prop.name);
         c->sm_count = prop.multiProcessorCount;
-        BB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        // the context's stream carries the LU's critical path (its panels) at the
+        // highest priority; the look-ahead trailing updates run on the side stream
+        int prio_least = 0, prio_greatest = 0;
+        BB_CUDA(cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest));
+        BB_CUDA(cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, prio_greatest));
+        BB_CUDA(cudaStreamCreateWithPriority(&c->side_stream, cudaStreamNonBlocking, prio_least));
+        BB_CUDA(cudaEventCreateWithFlags(&c->la_fork, cudaEventDisableTiming));
+        BB_CUDA(cudaEventCreateWithFlags(&c->la_join, cudaEventDisableTiming));
         for (auto &e : c->ev) BB_CUDA(cudaEventCreate(&e));
         c->status.alloc(256);
         BB_CUDA(cudaMemset(c->status.p, 0, 256));
@@ -347,6 +372,10 @@ int32_t beat_b200_destroy(beat_b200_ctx *c) {
     }
     for (auto &e : c->ev)
         if (e) cudaEventDestroy(e);
+    if (c->side_stream) cudaStreamSynchronize(c->side_stream);
+    for (cudaEvent_t e : {c->la_fork, c->la_join})
+        if (e) cudaEventDestroy(e);
+    if (c->side_stream) cudaStreamDestroy(c->side_stream);
     if (c->stream) cudaStreamDestroy(c->stream);
     cudaGetLastError();
     delete c;
@@ -379,6 +408,7 @@ int32_t beat_b200_solve(beat_b200_ctx *c, double k, double eta, int32_t R, const
         BB_REQUIRE(q && p_out && R >= 1, BEAT_B200_INVALID_ARG, "null pointer or R < 1");
         BB_REQUIRE(c->F > 0, BEAT_B200_STATE, "no mesh: call beat_b200_set_mesh first");
         const beat_b200_opts o = resolve_opts(opts);
+        c->ws.lu_valid = 0;  // the workspace may change below; solve_core sets it once the factors are good
         ensure_workspace(c, o.precision, R, rhs_request(o));
         Workspace &w = c->ws;
         BB_CUDA(cudaMemcpyAsync(w.q.p, q, (size_t)c->F * R * 16, cudaMemcpyHostToDevice, c->stream));

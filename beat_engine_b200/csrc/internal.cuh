@@ -210,6 +210,10 @@ struct beat_b200_ctx {
     bb::Workspace ws;
 
     cudaEvent_t ev[10] = {};
+    // the LU's look-ahead: the trailing update of panel k runs on side_stream
+    // (lower priority) while panel k + 1 is factored on `stream`
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t la_fork = nullptr, la_join = nullptr;
     float last_regular_ms = 0.f;
     bool cluster_checked = false;  // can a 16-CTA cluster of the panel kernel be scheduled?
     bool cluster_ok = false;

@@ -277,6 +277,41 @@ __global__ void laswp_kernel(Cx<T> *A, int64_t ld, int n, int k, int nb, const i
     }
 }
 
+// Row interchanges ipiv[k .. k+nsw) on the columns [c_lo, c_hi) outside
+// [x_lo, x_hi); with perm non-null, one extra thread applies them to the
+// running permutation.  (The look-ahead LU swaps a sub-panel's rows inside its
+// panel first and on the other columns once per panel.)
+template <typename T>
+__global__ void laswp_range_kernel(Cx<T> *A, int64_t ld, int n, int k, int nsw, const int *ipiv, int c_lo, int c_hi,
+                                   int x_lo, int x_hi, int *perm) {
+    __shared__ int sp[256];
+    for (int j = threadIdx.x; j < nsw; j += blockDim.x) sp[j] = ipiv[k + j];
+    __syncthreads();
+    const int jmax = min(nsw, n - k);
+    const int c = c_lo - 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (c == c_lo - 1) {
+        if (!perm) return;
+        for (int j = 0; j < jmax; ++j) {
+            const int p = sp[j];
+            if (p > k + j && p < n) {
+                const int t = perm[k + j];
+                perm[k + j] = perm[p];
+                perm[p] = t;
+            }
+        }
+        return;
+    }
+    if (c >= c_hi || (c >= x_lo && c < x_hi)) return;
+    for (int j = 0; j < jmax; ++j) {
+        const int p = sp[j];
+        if (p > k + j && p < n) {  // an interchange always names a later row
+            const Cx<T> t = A[(int64_t)(k + j) * ld + c];
+            A[(int64_t)(k + j) * ld + c] = A[(int64_t)p * ld + c];
+            A[(int64_t)p * ld + c] = t;
+        }
+    }
+}
+
 __global__ void iota_kernel(int *perm, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) perm[i] = i;
@@ -523,14 +558,19 @@ __device__ __forceinline__ void dmma884(double (&c)[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
+// Persistent over the output tiles (tiles_x per row of tiles, ntiles in all):
+// CTA b takes tiles b, b + gridDim.x, ... so a capped grid leaves SMs free
+// for the kernels running beside it (the LU's panel on the other stream).
 __global__ void __launch_bounds__(256, 2) dmma_update_kernel(Cx<double> *A, int64_t ld, int n, int k, int kk,
-                                                            int row0, int col0, int col_end) {
+                                                            int row0, int col0, int col_end, int tiles_x,
+                                                            int ntiles) {
     __shared__ double sLr[GT][DM_LP], sLi[GT][DM_LP];  // L chunk: 64 rows x 16
     __shared__ double sUr[DM_KC][DM_UP], sUi[DM_KC][DM_UP];  // U chunk: 16 x 64 columns
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wr = warp >> 2, wc = warp & 3;  // warp tile: rows 32 wr .., columns 16 wc ..
     const int g = lane >> 2, t = lane & 3;
-    const int r0 = row0 + blockIdx.y * GT, c0 = col0 + blockIdx.x * GT;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int r0 = row0 + (tile / tiles_x) * GT, c0 = col0 + (tile % tiles_x) * GT;
     double cr[4][2][2], ci[4][2][2];  // [row block][column block][fragment]
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -590,16 +630,23 @@ __global__ void __launch_bounds__(256, 2) dmma_update_kernel(Cx<double> *A, int6
                     d.im -= ci[i][j][e];
                 }
             }
+    }
 }
 
-// the trailing / in-panel update C -= L U: tensor cores (DMMA) in FP64, SIMT in FP32
+// the trailing / in-panel update C -= L U over rows row0.. and columns
+// [col0, col_end): tensor cores (DMMA) in FP64, SIMT in FP32.  max_ctas
+// (0: no cap) bounds the persistent DMMA grid.
 template <typename T>
 static void launch_update(cudaStream_t st, dim3 grid, Cx<T> *A, int64_t ld, int n, int k, int kk, int row0, int col0,
-                          int col_end) {
-    if constexpr (sizeof(T) == 8)
-        dmma_update_kernel<<<grid, 256, 0, st>>>(A, ld, n, k, kk, row0, col0, col_end);
-    else
+                          int col_end, int max_ctas = 0) {
+    if constexpr (sizeof(T) == 8) {
+        const int ntiles = (int)(grid.x * grid.y);
+        const int g = max_ctas > 0 ? std::min(ntiles, max_ctas) : ntiles;
+        if (g > 0)
+            dmma_update_kernel<<<g, 256, 0, st>>>(A, ld, n, k, kk, row0, col0, col_end, (int)grid.x, ntiles);
+    } else {
         gemm_update_kernel<T><<<grid, 256, 0, st>>>(A, ld, n, k, kk, row0, col0, col_end);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1072,9 +1119,12 @@ static bool cluster_panel(beat_b200_ctx *c, Cx<T> *A, int64_t ld, int n, int k, 
     return true;
 }
 
-// FP32 form trailing update on the tensor cores (tc_gemm.cu); returns false
-// when the shape is not supported, in which case the SIMT kernel runs.
-bool tc_trailing_update(beat_b200_ctx *c, int k, int nb, int split_terms);
+// FP32 form trailing update on the tensor cores (tc_gemm.cu)
+bool tc_update_supported(int nb);
+void tc_stage_l(beat_b200_ctx *c, int k, int nb, int split_terms, cudaStream_t st);
+void tc_stage_u(beat_b200_ctx *c, int k, int nb, int split_terms, int col_lo, int col_hi, cudaStream_t st);
+void tc_update_cols(beat_b200_ctx *c, int k, int nb, int split_terms, int col_lo, int col_hi, cudaStream_t st,
+                    int max_ctas);
 
 // ---------------------------------------------------------------------------
 // host driver
@@ -1122,12 +1172,55 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
     iota_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(w.perm.as<int>(), n);
     BB_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream));
     const size_t trsm_w_smem = sizeof(Cx<T>) * ((size_t)W * W + (size_t)W * TRSM_COLS);
+    int *ipiv = w.ipiv.as<int>();
+    int *perm = w.perm.as<int>();
+    cudaStream_t s0 = c->stream, s1 = c->side_stream;
+    const bool tc = sizeof(T) == 4 && tc_update_supported(nb);
+    // SMs the look-ahead update leaves to the panel factorisation beside it (one
+    // 16-CTA cluster); the grid-wide panel fallback waits for its own SMs
+    const int side_cap = std::max(1, G - CP_CTAS);
+    // U12 = L11^-1 A12 of panel k for the columns [c_lo, c_hi), on stream st
+    auto u_solve = [&](int k, int c_lo, int c_hi, cudaStream_t st) {
+        const int cols = c_hi - c_lo;
+        if (cols <= 0) return;
+        if (blocked)
+            trsm_blocked_kernel<T, WF><<<(cols + TB_COLS - 1) / TB_COLS, 256, tb_smem, st>>>(
+                A, ld, k, nb / W, dinv + (size_t)(k / W) * W * W, c_lo, c_hi);
+        else
+            trsm_kernel<T><<<(cols + TRSM_COLS - 1) / TRSM_COLS, 256, trsm_smem, st>>>(A, ld, n, k, nb, c_lo, c_hi);
+        BB_CUDA(cudaGetLastError());
+    };
+    // A[k+nb.., c_lo..c_hi) -= L21 U12 of panel k, on stream st
+    auto update = [&](int k, int c_lo, int c_hi, cudaStream_t st, int cap) {
+        if (c_hi <= c_lo || k + nb >= n) return;
+        if (tc) {
+            tc_stage_u(c, k, nb, split_terms, c_lo, c_hi, st);
+            tc_update_cols(c, k, nb, split_terms, c_lo, c_hi, st, cap);
+        } else {
+            dim3 grid((c_hi - c_lo + GT - 1) / GT, (n - k - nb + GT - 1) / GT);
+            launch_update<T>(st, grid, A, ld, n, k, nb, k + nb, c_lo, c_hi, cap > 0 ? 2 * cap : 0);
+            BB_CUDA(cudaGetLastError());
+        }
+    };
+    // Right-looking LU with a look-ahead of one panel.  For panel k (columns
+    // [k, pe)):
+    //   1. factor its sub-panels on s0, swapping rows inside the panel only;
+    //   2. wait for the side stream (the previous panel's update of the
+    //      columns right of this panel);
+    //   3. the panel's interchanges on every other column and the permutation;
+    //   4. U12 and the update of the next panel's columns on s0 (they are all
+    //      the next panel needs);
+    //   5. U12 and the update of the remaining columns on s1, which then runs
+    //      beside the next panel's factorisation (step 1 of panel k + nb).
+    // The next panel touches only its own columns and rows >= pe until its
+    // step 3, which follows the join: the streams never touch the same entries.
+    bool side_pending = false;
     for (int k = 0; k < n; k += nb) {
         const int pe = std::min(k + nb, n);  // end of this panel
         for (int ks = k; ks < pe; ks += W) {
             const int m = n - ks;
             Cx<T> *dinv_s = blocked ? dinv + (size_t)(ks / W) * W * W : nullptr;
-            const bool on_cluster = cluster_panel<T>(c, A, ld, n, ks, W, w.ipiv.as<int>(), dinv_s);
+            const bool on_cluster = cluster_panel<T>(c, A, ld, n, ks, W, ipiv, dinv_s);
             if (!on_cluster) {
                 // grid-wide panel kernel on the sub-panel
                 int g = std::min(G, std::max(1, (m + 15) / 16));
@@ -1139,7 +1232,7 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
                 a.k = ks;
                 a.nb = W;
                 a.rpc = rows;
-                a.ipiv = w.ipiv.as<int>();
+                a.ipiv = ipiv;
                 a.pub_rows = pub_rows;
                 a.pub_diag = pub_diag;
                 a.recs = recs;
@@ -1147,48 +1240,57 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
                 a.status = c->status.as<int>();
                 a.spin_limit = 1u << 22;
                 const size_t ps = sizeof(Cx<T>) * ((size_t)rows * W + 2 * W + rows);
-                BB_CUDA(cudaMemsetAsync(c->barrier.p, 0, sizeof(unsigned), c->stream));
+                BB_CUDA(cudaMemsetAsync(c->barrier.p, 0, sizeof(unsigned), s0));
                 void *args[] = {&a};
                 BB_CUDA(cudaLaunchCooperativeKernel((void *)panel_kernel<T>, dim3(g), dim3(PANEL_THREADS), args, ps,
-                                                    c->stream));
+                                                    s0));
             }
-            laswp_kernel<T><<<(n + 1 + 255) / 256, 256, 0, c->stream>>>(A, ld, n, ks, W, w.ipiv.as<int>(),
-                                                                        w.perm.as<int>());
-            BB_CUDA(cudaGetLastError());
+            // this sub-panel's interchanges on the rest of the panel
+            if (pe - k > W) {
+                laswp_range_kernel<T><<<(pe - k + 1 + 255) / 256, 256, 0, s0>>>(A, ld, n, ks, W, ipiv, k, pe, ks,
+                                                                                ks + W, nullptr);
+                BB_CUDA(cudaGetLastError());
+            }
             if (blocked && !on_cluster) {
-                diag_block_inverse_kernel<T><<<1, 32, 0, c->stream>>>(A, ld, n, ks, W, dinv_s);
+                diag_block_inverse_kernel<T><<<1, 32, 0, s0>>>(A, ld, n, ks, W, dinv_s);
                 BB_CUDA(cudaGetLastError());
             }
             if (ks + W < pe) {
                 // rest of this panel: U row block, then the panel's own trailing update
                 const int cols = pe - ks - W;
                 if (blocked)
-                    trsm_blocked_kernel<T, WF><<<(cols + TB_COLS - 1) / TB_COLS, 256, tb_smem, c->stream>>>(
+                    trsm_blocked_kernel<T, WF><<<(cols + TB_COLS - 1) / TB_COLS, 256, tb_smem, s0>>>(
                         A, ld, ks, 1, dinv + (size_t)(ks / W) * W * W, ks + W, pe);
                 else
-                    trsm_kernel<T><<<(cols + TRSM_COLS - 1) / TRSM_COLS, 256, trsm_w_smem, c->stream>>>(
+                    trsm_kernel<T><<<(cols + TRSM_COLS - 1) / TRSM_COLS, 256, trsm_w_smem, s0>>>(
                         A, ld, n, ks, W, ks + W, pe);
                 dim3 grid((cols + GT - 1) / GT, (n - ks - W + GT - 1) / GT);
-                launch_update<T>(c->stream, grid, A, ld, n, ks, W, ks + W, ks + W, pe);
+                launch_update<T>(s0, grid, A, ld, n, ks, W, ks + W, ks + W, pe);
                 BB_CUDA(cudaGetLastError());
             }
         }
-        const int rest = n - k - nb;
-        if (rest > 0) {
-            if (blocked)
-                trsm_blocked_kernel<T, WF><<<(rest + TB_COLS - 1) / TB_COLS, 256, tb_smem, c->stream>>>(
-                    A, ld, k, nb / W, dinv + (size_t)(k / W) * W * W, k + nb, n);
-            else
-                trsm_kernel<T><<<(rest + TRSM_COLS - 1) / TRSM_COLS, 256, trsm_smem, c->stream>>>(A, ld, n, k, nb,
-                                                                                               k + nb, n);
-            BB_CUDA(cudaGetLastError());
-            if (!(sizeof(T) == 4 && tc_trailing_update(c, k, nb, split_terms))) {
-                dim3 grid((rest + GT - 1) / GT, (rest + GT - 1) / GT);
-                launch_update<T>(c->stream, grid, A, ld, n, k, nb, k + nb, k + nb, n);
-                BB_CUDA(cudaGetLastError());
-            }
+        if (side_pending) {
+            BB_CUDA(cudaStreamWaitEvent(s0, c->la_join, 0));
+            side_pending = false;
+        }
+        // the panel's interchanges on every column outside it, and on perm
+        laswp_range_kernel<T><<<(n + 1 + 255) / 256, 256, 0, s0>>>(A, ld, n, k, pe - k, ipiv, 0, n, k, pe, perm);
+        BB_CUDA(cudaGetLastError());
+        if (pe >= n) break;
+        const int ne = std::min(pe + nb, n);  // end of the next panel
+        if (tc) tc_stage_l(c, k, nb, split_terms, s0);
+        u_solve(k, pe, ne, s0);
+        update(k, pe, ne, s0, 0);
+        if (ne < n) {
+            BB_CUDA(cudaEventRecord(c->la_fork, s0));
+            BB_CUDA(cudaStreamWaitEvent(s1, c->la_fork, 0));
+            u_solve(k, ne, n, s1);
+            update(k, ne, n, s1, side_cap);
+            BB_CUDA(cudaEventRecord(c->la_join, s1));
+            side_pending = true;
         }
     }
+    if (side_pending) BB_CUDA(cudaStreamWaitEvent(s0, c->la_join, 0));
 }
 
 
@@ -1634,7 +1736,6 @@ void lu_factor(beat_b200_ctx *c, int precision, int nb, int split_terms) {
         lu_factor_t<float>(c, nb, split_terms);
         diag_inverses<float>(c);
     }
-    c->ws.lu_valid = 1;
 }
 
 void lu_solve_fp64(beat_b200_ctx *c, int R, double *x_dev) {

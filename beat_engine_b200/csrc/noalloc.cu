@@ -15,7 +15,10 @@
 // Host code must not use the symbol's host-side name as a device pointer; the
 // device address is looked up once per device with cudaGetSymbolAddress (on
 // the first call on that device, with that device current) and passed to the
-// kernels.  All calls on a device share the one array: the entry point clears
+// kernels.  The looked-up address is kept for the life of the process; a
+// cudaDeviceReset of the device would invalidate it, and callers are told not
+// to call this entry point on a device after resetting it.
+// All calls on a device share the one array: the entry point clears
 // it at the start of every call, and calls whose work overlaps on the GPU
 // (other threads, other streams or other contexts on the same device) race on
 // it, so they must be serialised by the caller.
@@ -67,8 +70,13 @@ extern "C" int32_t beat_b200_resolve_noalloc(beat_b200_ctx *c, int32_t R, const 
         BB_REQUIRE(c->ws.lu_valid, BEAT_B200_STATE,
                    "no current factorisation: call beat_b200_solve (or beat_b200_solve_device) first");
         BB_REQUIRE(R >= 1, BEAT_B200_INVALID_ARG, "R must be >= 1");
-        BB_REQUIRE(d_b && d_x && d_b != d_x, BEAT_B200_INVALID_ARG,
-                   "d_b and d_x must be distinct non-null device buffers of N x R complex doubles");
+        BB_REQUIRE(d_b && d_x, BEAT_B200_INVALID_ARG,
+                   "d_b and d_x must be non-null device buffers of N x R complex doubles");
+        // the row permutation reads b while it writes x: the ranges must not overlap
+        const uintptr_t span = (uintptr_t)c->V * (uintptr_t)R * 16u;
+        const uintptr_t ub = (uintptr_t)d_b, ux = (uintptr_t)d_x;
+        BB_REQUIRE(ub + span <= ux || ux + span <= ub, BEAT_B200_INVALID_ARG,
+                   "d_b and d_x overlap: they must be separate N x R complex-double buffers");
         const int nblk = (c->V + 63) / 64;
         BB_REQUIRE(nblk <= RESOLVE_MAX_BLOCKS, BEAT_B200_INVALID_ARG,
                    "beat_b200_resolve_noalloc supports at most 262144 unknowns (its static scratch holds "

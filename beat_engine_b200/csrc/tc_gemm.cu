@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 
 #include "internal.cuh"
@@ -116,6 +117,7 @@ struct TcArgs {
     int m;             // rows of the trailing block
     int ncr;           // real columns of the trailing block (2 x complex columns)
     int cx0, cy0;      // coordinates of the block origin in the C tensor map (real col, row)
+    int brow0;         // first row of the staged B operand that this block's columns use
     int kchunks;       // K / 32
     int split;         // 1 or 3
     int tiles_n;       // column tiles
@@ -200,10 +202,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     mbar_expect_tx(&full_bar[s], stage_tx);
                     const int kx = kc * TC_BK;
                     tma_load_2d(st, &mA_hi, kx, row0, &full_bar[s]);
-                    tma_load_2d(st + 2 * A_BYTES, &mB_hi, kx, col0, &full_bar[s]);
+                    tma_load_2d(st + 2 * A_BYTES, &mB_hi, kx, g.brow0 + col0, &full_bar[s]);
                     if (split3) {
                         tma_load_2d(st + A_BYTES, &mA_lo, kx, row0, &full_bar[s]);
-                        tma_load_2d(st + 2 * A_BYTES + B_BYTES, &mB_lo, kx, col0, &full_bar[s]);
+                        tma_load_2d(st + 2 * A_BYTES + B_BYTES, &mB_lo, kx, g.brow0 + col0, &full_bar[s]);
                     }
                 }
             }
@@ -329,12 +331,13 @@ __global__ void stage_a_kernel(const float2 *A, int64_t ld, int k, int nb, int m
     }
 }
 
-__global__ void stage_b_kernel(const float2 *A, int64_t ld, int k, int nb, int ncols, float *bhi, float *blo,
+__global__ void stage_b_kernel(const float2 *A, int64_t ld, int k, int nb, int j0, int ncols, float *bhi, float *blo,
                                int split) {
-    // U12[kk][j] = A[k+kk][k+nb+j]; rows 2j and 2j+1 of B_s get (Ur, -Ui) and (Ui, Ur) at K = 2kk
+    // U12[kk][j] = A[k+kk][k+nb+j], j = j0 .. j0+ncols; rows 2j and 2j+1 of B_s get (Ur, -Ui) and
+    // (Ui, Ur) at K = 2kk
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (int64_t)ncols * nb) return;
-    const int j = (int)(idx / nb), kk = (int)(idx % nb);
+    const int j = j0 + (int)(idx / nb), kk = (int)(idx % nb);
     const float2 u = A[(int64_t)(k + kk) * ld + k + nb + j];
     const float2 e = make_float2(u.x, -u.y), o = make_float2(u.y, u.x);
     float2 *h0 = reinterpret_cast<float2 *>(bhi + (int64_t)(2 * j) * 2 * nb) + kk;
@@ -407,52 +410,93 @@ static CUtensorMap make_c_map(const float *ptr, int n, int64_t ld) {
     return m;
 }
 
-bool tc_trailing_update(beat_b200_ctx *c, int k, int nb, int split_terms) {
+// Staging of panel k's operands for the trailing update A22 -= L21 U12 (rows
+// and columns k + nb .. n): A_hi/A_lo (m x 2nb) and B_hi/B_lo (2m x 2nb),
+// m = n - k - nb, in the workspace's staging buffer.
+struct TcStage {
+    float *ahi, *alo, *bhi, *blo;
+    int m, kdim;
+};
+
+static TcStage tc_stage_buffers(beat_b200_ctx *c, int k, int nb) {
     Workspace &w = c->ws;
     const int n = c->V;
-    const int m = n - k - nb;
-    if (m <= 0) return true;
-    if (nb % 16 != 0) return false;  // K = 2 nb must be a multiple of 32
-    const int kdim = 2 * nb;
-    // staging: A_hi, A_lo (m x kdim), B_hi, B_lo (2m x kdim), padded to whole tiles
-    const int64_t mpad = ((int64_t)m + TC_BM - 1) / TC_BM * TC_BM;
-    const int64_t npad = ((int64_t)2 * m + TC_BN - 1) / TC_BN * TC_BN;
-    const size_t need = sizeof(float) * (size_t)kdim * (2 * (size_t)mpad + 2 * (size_t)npad) + 1024;
+    TcStage s;
+    s.m = n - k - nb;
+    s.kdim = 2 * nb;
+    const int64_t mpad = ((int64_t)s.m + TC_BM - 1) / TC_BM * TC_BM;
+    const int64_t npad = ((int64_t)2 * s.m + TC_BN - 1) / TC_BN * TC_BN;
+    const size_t need = sizeof(float) * (size_t)s.kdim * (2 * (size_t)mpad + 2 * (size_t)npad) + 1024;
     if (w.stage.bytes < need) {
         // size for the first (largest) panel
         const int64_t m0 = n, mp0 = (m0 + TC_BM - 1) / TC_BM * TC_BM, np0 = (2 * m0 + TC_BN - 1) / TC_BN * TC_BN;
-        w.stage.alloc(sizeof(float) * (size_t)kdim * (2 * (size_t)mp0 + 2 * (size_t)np0) + 1024);
+        w.stage.alloc(sizeof(float) * (size_t)s.kdim * (2 * (size_t)mp0 + 2 * (size_t)np0) + 1024);
     }
-    float *ahi = w.stage.as<float>();
-    float *alo = ahi + (size_t)mpad * kdim;
-    float *bhi = alo + (size_t)mpad * kdim;
-    float *blo = bhi + (size_t)npad * kdim;
-    const float2 *A = w.A.as<float2>();
-    {
-        const int64_t na = (int64_t)m * nb;
-        stage_a_kernel<<<(unsigned)((na + 255) / 256), 256, 0, c->stream>>>(A, w.ld, k, nb, m, ahi, alo, split_terms);
-        stage_b_kernel<<<(unsigned)((na + 255) / 256), 256, 0, c->stream>>>(A, w.ld, k, nb, m, bhi, blo, split_terms);
-        BB_CUDA(cudaGetLastError());
-    }
-    const CUtensorMap mah = make_map(ahi, m, kdim, TC_BM), mal = make_map(alo, m, kdim, TC_BM);
-    const CUtensorMap mbh = make_map(bhi, 2 * (int64_t)m, kdim, TC_BN), mbl = make_map(blo, 2 * (int64_t)m, kdim, TC_BN);
-    const CUtensorMap mc = make_c_map(w.A.as<float>(), n, w.ld);
+    s.ahi = w.stage.as<float>();
+    s.alo = s.ahi + (size_t)mpad * s.kdim;
+    s.bhi = s.alo + (size_t)mpad * s.kdim;
+    s.blo = s.bhi + (size_t)npad * s.kdim;
+    return s;
+}
+
+bool tc_update_supported(int nb) { return nb % 16 == 0; }  // K = 2 nb must be a multiple of 32
+
+// Stages L21 of panel k (every row below the panel).
+void tc_stage_l(beat_b200_ctx *c, int k, int nb, int split_terms, cudaStream_t st) {
+    const TcStage s = tc_stage_buffers(c, k, nb);
+    if (s.m <= 0) return;
+    const int64_t na = (int64_t)s.m * nb;
+    stage_a_kernel<<<(unsigned)((na + 255) / 256), 256, 0, st>>>(c->ws.A.as<float2>(), c->ws.ld, k, nb, s.m, s.ahi,
+                                                                 s.alo, split_terms);
+    BB_CUDA(cudaGetLastError());
+}
+
+// Stages U12 of panel k for the columns [col_lo, col_hi) (absolute, >= k + nb),
+// which must already hold U12 = L11^-1 A12.
+void tc_stage_u(beat_b200_ctx *c, int k, int nb, int split_terms, int col_lo, int col_hi, cudaStream_t st) {
+    const TcStage s = tc_stage_buffers(c, k, nb);
+    const int nc = col_hi - col_lo;
+    if (s.m <= 0 || nc <= 0) return;
+    const int64_t nbk = (int64_t)nc * nb;
+    stage_b_kernel<<<(unsigned)((nbk + 255) / 256), 256, 0, st>>>(c->ws.A.as<float2>(), c->ws.ld, k, nb,
+                                                                  col_lo - (k + nb), nc, s.bhi, s.blo, split_terms);
+    BB_CUDA(cudaGetLastError());
+}
+
+// A[k+nb.., col_lo..col_hi) -= L21 U12 from the staged operands, on `st`,
+// with at most max_ctas persistent CTAs (0: one per SM).
+void tc_update_cols(beat_b200_ctx *c, int k, int nb, int split_terms, int col_lo, int col_hi, cudaStream_t st,
+                    int max_ctas) {
+    const int n = c->V;
+    const TcStage s = tc_stage_buffers(c, k, nb);
+    const int nc = col_hi - col_lo;
+    if (s.m <= 0 || nc <= 0) return;
+    const CUtensorMap mah = make_map(s.ahi, s.m, s.kdim, TC_BM), mal = make_map(s.alo, s.m, s.kdim, TC_BM);
+    const CUtensorMap mbh = make_map(s.bhi, 2 * (int64_t)s.m, s.kdim, TC_BN),
+                      mbl = make_map(s.blo, 2 * (int64_t)s.m, s.kdim, TC_BN);
+    const CUtensorMap mc = make_c_map(c->ws.A.as<float>(), n, c->ws.ld);
     TcArgs g;
-    g.m = m;
-    g.ncr = 2 * m;
-    g.cx0 = 2 * (k + nb);
+    g.m = s.m;
+    g.ncr = 2 * nc;
+    g.cx0 = 2 * col_lo;
     g.cy0 = k + nb;
-    g.kchunks = kdim / TC_BK;
+    g.brow0 = 2 * (col_lo - (k + nb));
+    g.kchunks = s.kdim / TC_BK;
     g.split = split_terms;
-    g.tiles_n = (2 * m + TC_BN - 1) / TC_BN;
-    g.ntiles = g.tiles_n * ((m + TC_BM - 1) / TC_BM);
+    g.tiles_n = (2 * nc + TC_BN - 1) / TC_BN;
+    g.ntiles = g.tiles_n * ((s.m + TC_BM - 1) / TC_BM);
     g.status = c->status.as<int>();
     const size_t smem = (size_t)TC_STAGES * (2 * TC_BM * TC_BK * 4 + 2 * TC_BN * TC_BK * 4) + 4 * TC_EPI_BYTES + 1024;
-    BB_CUDA(cudaFuncSetAttribute(tc_update_kernel<TC_STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int grid = std::min(g.ntiles, c->sm_count);
-    tc_update_kernel<TC_STAGES><<<grid, TC_THREADS, smem, c->stream>>>(mah, mal, mbh, mbl, mc, g);
+    static std::atomic<bool> attr_done{false};  // sweep lanes call this from several threads
+    if (!attr_done) {
+        BB_CUDA(cudaFuncSetAttribute(tc_update_kernel<TC_STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+        attr_done = true;
+    }
+    const int cap = max_ctas > 0 ? std::min(max_ctas, c->sm_count) : c->sm_count;
+    const int grid = std::min(g.ntiles, cap);
+    tc_update_kernel<TC_STAGES><<<grid, TC_THREADS, smem, st>>>(mah, mal, mbh, mbl, mc, g);
     BB_CUDA(cudaGetLastError());
-    return true;
 }
 
 }  // namespace bb

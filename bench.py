@@ -12,16 +12,24 @@ assembly + one LU + R-column solve (+ FP64 GMRES refinement in the mixed
 form) + the far-field pattern at 541 directions (360 equator + 181 meridian)
 for all R.
 
-``value``: device-timed throughput with q already in HBM: the K timed steps
-(frequencies) run as one beat_b200_sweep_device call, which pipelines them over
-up to six solve lanes, four in the FP64 form (one frequency's assembly beside
+``value``: device-timed throughput of the mixed form (FP32 assembly, TF32
+split tensor-core LU, FP64 GMRES refinement) with q already in HBM: the K
+timed steps (frequencies) run as one beat_b200_sweep_device call, which
+pipelines them over up to six solve lanes (one frequency's assembly beside
 another's factorisation).
-``e2e``: the same through the host C-ABI sweep (beat_b200_sweep) from pinned
-host buffers.  ``stages_ms`` are one frequency solved alone.
+``e2e``: the same K frequencies through the host C-ABI sweep (beat_b200_sweep)
+from pinned host buffers, results copied back to the host.
+``fp64_value`` / ``fp64_e2e``: the same for the plain FP64 form (four lanes),
+on its own context; ``speedup_vs_fp64`` = value / fp64_value.
+``accuracy``: per-RHS relative L2 error of the timed mixed solutions against
+the timed FP64 solutions of the same frequencies, and of both forms against
+the FP64 oracle's solution of this workload (tests/golden/headline_F20480.npz),
+at 0.5, 2 and 6 kHz; computed after the timed regions.
+``stages_ms`` are one frequency solved alone.
 
 ``--impl reference`` times the CPU restatement of the reference's FP64 path
-(oracle/, OpenMP on all host cores + LAPACK LU) on a bounded sample and
-extrapolates to freq-solves/s.
+(oracle/, OpenMP on all host cores + LAPACK LU) piece by piece (CpuRecipe) and
+reports the freq-solves/s it accounts for.
 """
 from __future__ import annotations
 
@@ -120,60 +128,146 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------------
-# CPU baseline: the oracle on a bounded sample
+# CPU baseline: the oracle on a bounded sample (one recipe for both CPU legs)
 # --------------------------------------------------------------------------
-def cpu_sample(mesh, vel, dirs, sample_faces: int, lu_n: int, threads: int):
-    """Time the FP64 CPU restatement on a sample and extrapolate one full
-    frequency solve: regular+singular assembly of `sample_faces` test faces
-    (scaled by F / sample_faces), LAPACK LU + solve at order `lu_n` (scaled by
-    (N / lu_n)^3) and the far field of 8 directions (scaled by 541 / 8)."""
-    import scipy.linalg as sl
+CPU_SLICES = 16   # a frequency's assembly is cut into 16 equal slices of test faces
+CPU_FREQ = 2000.0
 
-    import oracle
-    F, N = mesh.num_faces, mesh.num_vertices
-    R = vel.shape[1]
-    f = 2000.0
-    k = 2 * math.pi * f / C0
-    q = neumann(vel, f)
-    t0 = time.perf_counter()
-    oracle.assemble(mesh, k, 1.0 / k, q, test_range=(0, sample_faces), threads=threads)
-    t_asm = (time.perf_counter() - t0) * F / sample_faces
-    rng = np.random.default_rng(5)
-    A = rng.standard_normal((lu_n, lu_n)) + 1j * rng.standard_normal((lu_n, lu_n)) + lu_n * np.eye(lu_n)
-    B = rng.standard_normal((lu_n, R)) + 1j * rng.standard_normal((lu_n, R))
-    t0 = time.perf_counter()
-    sl.lu_solve(sl.lu_factor(A, overwrite_a=True, check_finite=False), B, check_finite=False)
-    t_lu = (time.perf_counter() - t0) * (N / lu_n) ** 3
-    p = rng.standard_normal((N, R)) + 1j * rng.standard_normal((N, R))
-    t0 = time.perf_counter()
-    oracle.farfield(mesh, k, dirs[:8], p, q, threads=threads)
-    t_ff = (time.perf_counter() - t0) * dirs.shape[0] / 8
-    total = t_asm + t_lu + t_ff
-    return 1.0 / total, {"assembly_s": t_asm, "lu_solve_s": t_lu, "farfield_s": t_ff, "total_s": total}
+
+class CpuRecipe:
+    """The FP64 CPU restatement of the reference path (oracle/: assembly in
+    C/OpenMP, LAPACK LU), timed piece by piece on the host so that one
+    frequency solve of the full workload is accounted for without running all
+    of it:
+
+    * assembly: the test faces are cut into CPU_SLICES equal slices; each
+      timed slice assembles its test faces against every trial face (regular
+      and touching pairs) into one shared A and b without clearing them.
+      ``fixed`` is the rest of an assembly (clearing A and b, the identity
+      term, set-up), timed once; ``overhead`` is the per-call set-up that a
+      slice call repeats (timed once with an empty slice) and is taken out of
+      every slice.  One frequency's assembly = fixed + sum over all slices of
+      (slice - overhead), unmeasured slices at the measured mean;
+    * LU: one full LAPACK zgetrf + zgetrs of the N x N system with R columns,
+      timed in full;
+    * far field: the full 541-direction far field of all R columns, timed.
+
+    Nothing is scaled by a power law: every piece is timed at the full size."""
+
+    def __init__(self, mesh, vel, dirs, threads):
+        import oracle
+        self.oracle = oracle
+        self.mesh, self.vel, self.dirs, self.threads = mesh, vel, dirs, threads
+        self.F, self.N, self.R = mesh.num_faces, mesh.num_vertices, vel.shape[1]
+        self.k = 2 * math.pi * CPU_FREQ / C0
+        self.q = neumann(vel, CPU_FREQ)
+        self.A = np.zeros((self.N, self.N), dtype=np.complex128, order="F")
+        self.b = np.zeros((self.N, self.R), dtype=np.complex128, order="F")
+        self.bounds = np.linspace(0, self.F, CPU_SLICES + 1).astype(int)
+        self.slice_s = {}
+        self.fixed_s = self.overhead_s = self.lu_s = self.ff_s = None
+
+    def _assemble(self, lo, hi, flags):
+        t0 = time.perf_counter()
+        self.oracle.assemble(self.mesh, self.k, 1.0 / self.k, self.q, threads=self.threads, flags=flags,
+                             test_range=(lo, hi), out=(self.A, self.b))
+        return time.perf_counter() - t0
+
+    def time_fixed(self):
+        o = self.oracle
+        self.fixed_s = self._assemble(0, 0, 0)  # clear + identity + set-up
+        self.overhead_s = self._assemble(0, 0, o.NO_CLEAR | o.SKIP_IDENTITY)
+        return self.fixed_s + self.overhead_s
+
+    def time_slice(self, i):
+        o = self.oracle
+        j = i % CPU_SLICES
+        t = self._assemble(int(self.bounds[j]), int(self.bounds[j + 1]), o.NO_CLEAR | o.SKIP_IDENTITY)
+        self.slice_s.setdefault(j, []).append(t)
+        return t
+
+    def time_lu(self):
+        import scipy.linalg as sl
+        rng = np.random.default_rng(5)
+        # the system's own values do not change LAPACK's work; a diagonally
+        # weighted random matrix keeps the pivots well away from zero
+        A = np.asfortranarray(rng.standard_normal((self.N, self.N)) + 1j * rng.standard_normal((self.N, self.N)))
+        A[np.diag_indices(self.N)] += self.N
+        B = rng.standard_normal((self.N, self.R)) + 1j * rng.standard_normal((self.N, self.R))
+        t0 = time.perf_counter()
+        sl.lu_solve(sl.lu_factor(A, overwrite_a=True, check_finite=False), B, check_finite=False)
+        self.lu_s = time.perf_counter() - t0
+        return self.lu_s
+
+    def time_farfield(self):
+        rng = np.random.default_rng(6)
+        p = rng.standard_normal((self.N, self.R)) + 1j * rng.standard_normal((self.N, self.R))
+        t0 = time.perf_counter()
+        self.oracle.farfield(self.mesh, self.k, self.dirs, p, self.q, threads=self.threads)
+        self.ff_s = time.perf_counter() - t0
+        return self.ff_s
+
+    def estimate(self):
+        per = {j: statistics.median(v) - self.overhead_s for j, v in self.slice_s.items()}
+        mean = statistics.mean(per.values())
+        asm = self.fixed_s + sum(per.get(j, mean) for j in range(CPU_SLICES))
+        total = asm + self.lu_s + self.ff_s
+        parts = {"assembly_s": asm, "lu_solve_s": self.lu_s, "farfield_s": self.ff_s, "total_s": total,
+                 "slices_timed": len(per), "slices": CPU_SLICES}
+        return 1.0 / total, parts
+
+    def describe(self):
+        return (f"FP64 C/OpenMP restatement of the reference CPU path (oracle/) on {self.threads} host threads, "
+                f"one frequency solve of this workload ({CPU_FREQ:.0f} Hz) accounted piece by piece: assembly as "
+                f"{CPU_SLICES} slices of {self.F // CPU_SLICES} test faces x all {self.F} trial faces, "
+                f"{len(self.slice_s)} of them timed (the rest at their mean), plus the clear/identity/set-up "
+                f"part timed once; one full LAPACK zgetrf+zgetrs at N={self.N} with {self.R} RHS; the full "
+                f"{self.dirs.shape[0]}-direction far field")
+
+
+def cpu_baseline(mesh, vel, dirs, threads, n_slices):
+    r = CpuRecipe(mesh, vel, dirs, threads)
+    r.time_fixed()
+    for i in range(n_slices):
+        r.time_slice(i)
+    r.time_lu()
+    r.time_farfield()
+    v, parts = r.estimate()
+    return v, parts, r.describe()
 
 
 def run_reference(args):
-    """--impl reference: the CPU restatement of the reference path on the host."""
+    """--impl reference: the CPU restatement of the reference path on the host.
+    A step is one slice of a frequency's assembly (1/CPU_SLICES of its test
+    faces); the LU and the far field are timed once, in full, after the
+    steps.  value = one over the accounted seconds of one frequency solve."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
     mesh, vel, dirs = workload(args.sub, args.rhs)
-    vals, parts = [], None
-    for i in range(args.warmup + args.steps):
-        v, parts = cpu_sample(mesh, vel, dirs, args.ref_sample_faces, args.ref_lu_n, threads)
-        if i >= args.warmup:
-            vals.append(v)
-    value = statistics.median(vals)
-    sample = (f"per step: oracle assembly of {args.ref_sample_faces}/{mesh.num_faces} test faces x all trial faces "
-              f"(scaled by F/{args.ref_sample_faces}), LAPACK zgetrf+zgetrs at N={args.ref_lu_n} with {args.rhs} RHS "
-              f"(scaled by (N/{args.ref_lu_n})^3), far field of 8/541 directions (scaled); extrapolated "
-              f"seconds {json.dumps({k: round(v, 2) for k, v in parts.items()})}")
+    t_start = time.perf_counter()
+    r = CpuRecipe(mesh, vel, dirs, threads)
+    r.time_fixed()
+    for i in range(args.warmup):  # untimed: first touches of A and the oracle's caches
+        r._assemble(int(r.bounds[i % CPU_SLICES]), int(r.bounds[i % CPU_SLICES + 1]),
+                    r.oracle.NO_CLEAR | r.oracle.SKIP_IDENTITY)
+    step_s = [r.time_slice(i) for i in range(args.steps)]
+    r.time_lu()
+    r.time_farfield()
+    value, parts = r.estimate()
+    timed_s = sum(step_s) + r.lu_s + r.ff_s + r.fixed_s + r.overhead_s
+    sample = (r.describe() + f"; a step is one assembly slice ({args.steps} timed after {args.warmup} warm-up); "
+              f"accounted seconds per frequency solve {json.dumps({k: round(v, 2) for k, v in parts.items()})}; "
+              f"measured seconds in this run {timed_s:.1f} (wall {time.perf_counter() - t_start:.1f})")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(step_s), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
             "config": config_dict(args, mesh), "impl": "reference",
+            "step_basis": f"one of {CPU_SLICES} assembly slices of a frequency solve; value accounts a whole "
+                          "frequency solve (all slices, LU and far field, each timed)",
+            "timed_region_s": timed_s,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -185,16 +279,18 @@ def config_dict(args, mesh):
                         f"(F={mesh.num_faces} faces, N={mesh.num_vertices} P1 dofs), R={args.rhs} RHS, "
                         "f cycling 0.5/2/6 kHz, order 4/4, far field at 541 directions",
             "faces": mesh.num_faces, "dofs": mesh.num_vertices, "rhs": args.rhs,
-            "precision_form": args.precision, "lu_split_terms": args.split,
+            "precision_form": "mixed (FP32 assembly, TF32 split tensor-core LU, FP64 GMRES refinement); "
+                              "the FP64 form timed beside it", "lu_split_terms": args.split,
             "l2": "inputs larger than L2: every step rewrites A (N^2 complex) and the N x F RHS operator",
             "parallelism": f"frequency replicas x{args.gpus} (no collective); "
-                           "up to 6 solve lanes per GPU, 4 in the FP64 form (pipelined frequency sweep)"}
+                           "up to 6 solve lanes per GPU, 4 in the FP64 form (pipelined frequency sweep, "
+                           "each lane takes the next frequency when it finishes one)"}
 
 
 # --------------------------------------------------------------------------
 # GPU arm
 # --------------------------------------------------------------------------
-def count_launches(ctx, fn):
+def count_launches(fn):
     """Kernels of libbeatb200 launched by fn(), counted by the CUDA profiler."""
     import torch
     from torch.profiler import ProfilerActivity, profile
@@ -206,6 +302,72 @@ def count_launches(ctx, fn):
         if ev.device_type is not None and "cuda" in str(ev.device_type).lower() and "bb::" in ev.name:
             n += 1
     return n
+
+
+class Form:
+    """One precision form on its own context: the sweep lanes of each form
+    stay allocated, so neither form's timed sweep pays for the other's."""
+
+    def __init__(self, lib, mesh, device, precision, split):
+        import torch
+        self.lib = lib
+        self.precision = precision
+        self.ctx = lib.Context(device)
+        self.ctx.set_mesh(mesh.vertices, mesh.faces, 4, 4)
+        self.opts = lib.Context.opts(precision, lu_split_terms=split)
+        self.stream = torch.cuda.ExternalStream(self.ctx.stream_handle(), device=torch.device("cuda", device))
+
+    def sweep(self, ks, qs, ps, dirs, ffs):
+        return self.ctx.sweep_device(ks, 1.0 / ks, qs.data_ptr(), qs.shape[1], ps.data_ptr(), self.opts, dirs,
+                                     ffs.data_ptr())
+
+
+def timed(stream, fn, clocks_device=None):
+    """CUDA-event milliseconds of fn() on `stream` (the library's stream: the
+    sweep returns after every lane finished, so its end event follows all of
+    its work), with the SM clocks sampled meanwhile when clocks_device is set."""
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(clocks_device) if clocks_device is not None else None
+    if sampler:
+        sampler.__enter__()
+    try:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    finally:
+        if sampler:
+            sampler.__exit__(None, None, None)
+    return e0.elapsed_time(e1), out, (sampler.summary() if sampler else None)
+
+
+def oracle_gold(args):
+    """The oracle's FP64 solution of this workload (tests/golden/headline_F20480.npz,
+    made by tests/golden/make_headline_fixtures.py), when the workload is that one."""
+    path = os.path.join(ROOT, "tests", "golden", "headline_F20480.npz")
+    if args.sub != 5 or args.rhs != 16 or not os.path.exists(path):
+        return None
+    g = dict(np.load(path))
+    rng = np.random.default_rng(77)
+    n = 10242
+    g["W"] = rng.standard_normal((n, 8)) + 1j * rng.standard_normal((n, 8))
+    return g
+
+
+def errors_vs_oracle(gold, f, p, ff):
+    """Per-column relative errors of one frequency's solution p (N x R) and far
+    field ff (M x R) against the oracle: the stored full columns, the probe
+    sketch of every column and the far field of every column (max of each)."""
+    tag = f"_{int(f)}"
+    keep = list(gold["keep"])
+    ref = gold["p_cols" + tag]
+    e_cols = np.linalg.norm(p[:, keep] - ref, axis=0) / np.linalg.norm(ref, axis=0)
+    e_proj = np.sqrt(np.mean(np.abs(gold["W"].T @ p - gold["proj" + tag]) ** 2, axis=0)) / gold["pnorm" + tag]
+    fref = gold["ff" + tag]
+    e_ff = np.linalg.norm(ff - fref, axis=0) / np.linalg.norm(fref, axis=0)
+    return float(max(e_cols.max(), e_proj.max())), float(e_ff.max())
 
 
 def run_gpu(args):
@@ -222,155 +384,171 @@ def run_gpu(args):
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
     mesh, vel, dirs = workload(args.sub, args.rhs)
     F, N, R, M = mesh.num_faces, mesh.num_vertices, args.rhs, dirs.shape[0]
-    prec = _lib.FP64 if args.precision == "fp64" else _lib.MIXED_FP32_IR
-    opts = _lib.Context.opts(prec, lu_split_terms=args.split)
-
-    ctx = _lib.Context(local)
-    ctx.set_mesh(mesh.vertices, mesh.faces, 4, 4)
-    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=torch.device("cuda", local))
-    dev = torch.device("cuda", local)
-    # device-resident inputs: q per frequency (F x R column-major = R x F row-major)
-    q_dev = {f: torch.from_numpy(np.ascontiguousarray(neumann(vel, f).T)).to(dev) for f in FREQS}
-    p_dev = torch.empty((R, N), dtype=torch.complex128, device=dev)
-    ff_dev = torch.empty((R, M), dtype=torch.complex128, device=dev)
+    K = args.steps
 
     # this rank's share of the job's frequency list (round-robin, as
     # beat_engine_b200.sharding splits a multi-GPU sweep); each rank solves
     # its own frequencies, nothing crosses between ranks
-    share = sharding.partition(world * (args.steps + args.warmup + args.e2e_steps + 16), world)[rank]
+    share = sharding.partition(world * (K + args.warmup + 16), world)[rank]
 
     def freq(i):
         return FREQS[share[i] % len(FREQS)]
 
-    def step(i, diags=None):
-        # one frequency on its own (launch count, isolated stage times)
-        f = freq(i)
-        k = 2 * math.pi * f / C0
-        d = ctx.solve_device(k, 1.0 / k, q_dev[f].data_ptr(), R, p_dev.data_ptr(), opts)
-        ctx.farfield_device(k, dirs, R, p_dev.data_ptr(), q_dev[f].data_ptr(), ff_dev.data_ptr())
-        if diags is not None:
-            diags.append(d)
+    # device-resident inputs: q per frequency (F x R column-major = R x F row-major)
+    q_dev = {f: torch.from_numpy(np.ascontiguousarray(neumann(vel, f).T)).to(dev) for f in FREQS}
 
-    def sweep_buffers(i0, n):
+    def sweep_inputs(i0, n):
         fs = [freq(i0 + j) for j in range(n)]
         ks = np.array([2 * math.pi * f / C0 for f in fs])
         qs = torch.stack([q_dev[f] for f in fs])  # n x R x F: frequency-major F x R column-major slices
         ps = torch.empty((n, R, N), dtype=torch.complex128, device=dev)
         ffs = torch.empty((n, R, M), dtype=torch.complex128, device=dev)
-        return ks, qs, ps, ffs
+        return fs, ks, qs, ps, ffs
 
-    def sweep(bufs):
-        ks, qs, ps, ffs = bufs
-        return ctx.sweep_device(ks, 1.0 / ks, qs.data_ptr(), R, ps.data_ptr(), opts, dirs, ffs.data_ptr())
-
-    # a step is one frequency solve + far field; the K timed steps run as one
-    # pipelined sweep (beat_b200_sweep_device) with their inputs resident
-    warm = sweep_buffers(0, max(args.warmup, 2))
-    sweep(warm)
-    timed = sweep_buffers(args.warmup, args.steps)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        torch.cuda.synchronize()
-        e0.record(stream)
-        sweep_diags = sweep(timed)
-        # the sweep returns after every lane finished: this event follows all of its work
-        e1.record(stream)
-        torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    clocks = clk.summary()
-    if world > 1:
+    def max_over_ranks(ms):
+        if world == 1:
+            return ms
         t = torch.tensor([ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        return float(t.item())
+
+    def run_form(form, n_steps):
+        # warm-up: at least one frequency per lane, so every lane exists and
+        # holds its workspace before the timed sweep
+        _, ks, qs, ps, ffs = sweep_inputs(0, max(args.warmup, 6))
+        form.sweep(ks, qs, ps, dirs, ffs)
+        fs, ks, qs, ps, ffs = sweep_inputs(args.warmup, n_steps)
+        torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
-    value = world * args.steps / (ms / 1e3)
-    del warm, timed
+        ms, diags, clk = timed(form.stream, lambda: form.sweep(ks, qs, ps, dirs, ffs), clocks_device=local)
+        ms = max_over_ranks(ms)
+        return ms, diags, clk, fs, ps, ffs
+
+    def run_e2e(form, n_steps):
+        """The same K frequencies through the host C-ABI sweep (beat_b200_sweep):
+        q from pinned host memory in, p and the far field back to the host."""
+        fs = [freq(args.warmup + i) for i in range(n_steps)]
+        ks = np.array([2 * math.pi * f / C0 for f in fs])
+        q_pin = torch.stack([torch.from_numpy(np.ascontiguousarray(neumann(vel, f).T)) for f in fs]).pin_memory()
+        qh = q_pin.numpy().transpose(2, 1, 0)  # F x R x n, column-major view of pinned memory
+        form.ctx.sweep(ks[:2], 1.0 / ks[:2], qh[:, :, :2], form.opts, dirs)  # sizes the lanes' staging (untimed)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ms, _, _ = timed(form.stream, lambda: form.ctx.sweep(ks, 1.0 / ks, qh, form.opts, dirs))
+        return max_over_ranks(ms)
+
+    mixed = Form(_lib, mesh, local, _lib.MIXED_FP32_IR, args.split)
+    ms, sweep_diags, clocks, fs, ps_mixed, ff_mixed = run_form(mixed, K)
+    value = world * K / (ms / 1e3)
+    e2e_ms = run_e2e(mixed, K)
+    e2e_value = world * K / (e2e_ms / 1e3)
+
+    fp64 = None
+    if not args.no_fp64:
+        fp64 = Form(_lib, mesh, local, _lib.FP64, args.split)
+        ms64, diags64, clocks64, fs64, ps_64, ff_64 = run_form(fp64, K)
+        fp64_value = world * K / (ms64 / 1e3)
+        fp64_e2e = world * K / (run_e2e(fp64, K) / 1e3)
+
+    # accuracy of the timed mixed solutions against the timed FP64 solutions of
+    # the same frequencies, and of both against the oracle (outside the timed regions)
+    acc = None
+    if rank == 0:
+        pm = ps_mixed.cpu().numpy()
+        fm = ff_mixed.cpu().numpy()
+        acc = {"basis": "per-RHS relative L2 error of the timed sweeps' solutions (N x 16 per frequency)",
+               "by_frequency_hz": {}}
+        gold = oracle_gold(args)
+        p64 = ps_64.cpu().numpy() if fp64 else None
+        f64 = ff_64.cpu().numpy() if fp64 else None
+        for f in FREQS:
+            idx = [i for i, x in enumerate(fs) if x == f]
+            if not idx:
+                continue
+            row = {}
+            if fp64:
+                e = [np.linalg.norm(pm[i] - p64[i], axis=1) / np.linalg.norm(p64[i], axis=1) for i in idx]
+                row["mixed_vs_fp64_form_max"] = float(np.max(e))
+            if gold is not None:
+                i = idx[0]
+                row["mixed_vs_oracle_max"], row["mixed_farfield_vs_oracle_max"] = errors_vs_oracle(
+                    gold, f, pm[i].T, fm[i].T)
+                if fp64:
+                    row["fp64_vs_oracle_max"], row["fp64_farfield_vs_oracle_max"] = errors_vs_oracle(
+                        gold, f, p64[i].T, f64[i].T)
+            acc["by_frequency_hz"][str(int(f))] = row
+        vals = [v for r in acc["by_frequency_hz"].values() for k2, v in r.items() if k2.startswith("mixed_vs")]
+        acc["max_rel_err"] = float(max(vals)) if vals else None
+        acc["within_1e-6"] = bool(vals) and max(vals) <= 1e-6
+        acc["oracle"] = ("FP64 oracle (oracle/ assembly + LAPACK) solutions stored in "
+                         "tests/golden/headline_F20480.npz" if gold is not None else "unavailable for this workload")
+    del ps_mixed, ff_mixed
+    if fp64:
+        del ps_64, ff_64
 
     # stage times of one frequency solved alone (not timed into value)
-    diags = []
-    for i in range(3):
-        step(i, diags)
+    def stages_of(form):
+        p_dev = torch.empty((R, N), dtype=torch.complex128, device=dev)
+        ff_dev = torch.empty((R, M), dtype=torch.complex128, device=dev)
+        diags = []
+        for f in FREQS:
+            k = 2 * math.pi * f / C0
+            diags.append(form.ctx.solve_device(k, 1.0 / k, q_dev[f].data_ptr(), R, p_dev.data_ptr(), form.opts))
+            form.ctx.farfield_device(k, dirs, R, p_dev.data_ptr(), q_dev[f].data_ptr(), ff_dev.data_ptr())
+        torch.cuda.synchronize()
+        st = {k2: round(float(np.mean([d[k2] for d in diags])), 3)
+              for k2 in ("assembly_ms", "regular_ms", "singular_ms", "lu_ms", "solve_ms", "ir_ms")}
+        st["ir_iterations"] = float(np.mean([d["ir_iterations"] for d in diags]))
+        return st, (lambda: (form.ctx.solve_device(2 * math.pi * FREQS[0] / C0, C0 / (2 * math.pi * FREQS[0]),
+                                                   q_dev[FREQS[0]].data_ptr(), R, p_dev.data_ptr(), form.opts),
+                             form.ctx.farfield_device(2 * math.pi * FREQS[0] / C0, dirs, R, p_dev.data_ptr(),
+                                                      q_dev[FREQS[0]].data_ptr(), ff_dev.data_ptr())))
 
-    # e2e through the host C-ABI sweep with pinned buffers
-    ke = max(2, min(args.steps, args.e2e_steps))
-    fs = [freq(i) for i in range(ke)]
-    ks = np.array([2 * math.pi * f / C0 for f in fs])
-    q_pin = torch.stack([torch.from_numpy(np.ascontiguousarray(neumann(vel, f).T)) for f in fs]).pin_memory()
-    qh = q_pin.numpy().transpose(2, 1, 0)  # F x R x ke, column-major view of pinned memory
-    ctx.sweep(ks, 1.0 / ks, qh, opts, dirs)  # sizes the lanes' host-staging buffers (untimed)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    ctx.sweep(ks, 1.0 / ks, qh, opts, dirs)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * ke / (e2e_ms / 1e3)
-    h2d = F * R * 16 + M * 24
-    d2h = N * R * 16 + M * R * 16
-
-    # accuracy of this form against the FP64 form on the same step (not timed)
-    acc = None
-    if args.check_accuracy and prec != _lib.FP64 and rank == 0:
-        f = freq(0)
-        k = 2 * math.pi * f / C0
-        qh = neumann(vel, f)
-        p_mixed, _ = ctx.solve(k, 1.0 / k, qh, opts)
-        p64, _ = ctx.solve(k, 1.0 / k, qh, _lib.Context.opts(_lib.FP64))
-        err = np.linalg.norm(p_mixed - p64, axis=0) / np.linalg.norm(p64, axis=0)
-        acc = {"frequency_hz": f, "max_rel_err_vs_fp64_gpu": float(err.max()),
-               "median_rel_err_vs_fp64_gpu": float(np.median(err))}
+    stages, one_step = stages_of(mixed)
+    stages64 = stages_of(fp64)[0] if fp64 else None
 
     launches = None
     if rank == 0:
         try:
-            launches = count_launches(ctx, lambda: step(0)) * args.steps
+            launches = count_launches(one_step) * K
         except Exception as exc:  # profiler unavailable: report the failure, not a guess
             launches = f"unavailable: {exc}"
 
     if rank == 0:
-        def mean(key):
-            return float(np.mean([d[key] for d in diags]))
-        stages = {k: round(mean(k), 3) for k in ("assembly_ms", "regular_ms", "singular_ms", "lu_ms", "solve_ms",
-                                                   "ir_ms")}
-        stages["ir_iterations"] = float(np.mean([d["ir_iterations"] for d in diags]))
         peaks = measured_peaks()
         roof = roofline(args, mesh, stages, peaks)
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+                "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
-                "dtype": "c64 (tf32 tensor LU) + c128 refinement" if prec != _lib.FP64 else "c128",
+                "dtype": "c64 (tf32 tensor LU) + c128 refinement",
                 "data": "synthetic (seeded velocities on a generated icosphere)",
                 "config": config_dict(args, mesh), "stages_ms": stages,
                 "stages_basis": "one frequency solved alone (stage times inside the sweep overlap)",
-                "sweep_ir_converged": all(d["ir_converged"] == 1 for d in sweep_diags) if prec != _lib.FP64 else None,
-                "roofline": roof,
-                "clocks": clocks, "gpu_launches": launches,
-                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                        "steps": ke}}
-        if acc:
-            line["accuracy"] = acc
+                "sweep_ir_converged": all(d["ir_converged"] == 1 for d in sweep_diags),
+                "roofline": roof, "clocks": clocks, "gpu_launches": launches,
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": F * R * 16 + M * 24,
+                        "d2h_bytes_per_step": N * R * 16 + M * R * 16, "steps": K}}
+        if fp64:
+            line.update({"fp64_value": fp64_value, "fp64_e2e": fp64_e2e, "fp64_ms_per_step": ms64 / K,
+                         "fp64_steps": K, "speedup_vs_fp64": value / fp64_value,
+                         "speedup_vs_fp64_e2e": e2e_value / fp64_e2e, "fp64_clocks": clocks64,
+                         "fp64_stages_ms": stages64})
+        line["accuracy"] = acc
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
-            v, parts = cpu_sample(mesh, vel, dirs, args.cpu_sample_faces, args.cpu_lu_n, threads)
-            line["cpu_baseline"] = {
-                "value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                "sample": (f"oracle (FP64 C/OpenMP restatement) assembly of {args.cpu_sample_faces}/{F} test faces, "
-                           f"LAPACK LU at N={args.cpu_lu_n} scaled by (N/{args.cpu_lu_n})^3, far field of 8/541 "
-                           f"directions; extrapolated seconds "
-                           f"{json.dumps({k: round(x, 2) for k, x in parts.items()})}")}
+            v, parts, desc = cpu_baseline(mesh, vel, dirs, threads, args.cpu_slices)
+            line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                                    "sample": desc + "; accounted seconds " +
+                                    json.dumps({k2: round(x, 2) for k2, x in parts.items()})}
         print(json.dumps(line), flush=True)
-    ctx.close()
+    mixed.ctx.close()
+    if fp64:
+        fp64.ctx.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -388,49 +566,48 @@ def measured_peaks():
 
 
 # DRAM traffic of sym_pairs_kernel<6> (the mixed form's element-pair kernel) measured by ncu on
-# the F = 5,120 icosphere (profiles/sym_pairs_kernel_F5120.md): dram read + write bytes per launch
-# and the algorithmic output of that launch (A: N^2 c64, B: N x F c64).  Traffic grows with the
-# output written (the zeroed A and B are read back by the red.global.add flush), so a launch on
-# another mesh is scaled by its output bytes.
+# the F = 5,120 icosphere: 158.99 MB read + 119.64 MB written per launch, against an algorithmic
+# output of A (N^2 c64) + B (N x F c64) = 157.4 MB at N = 2,562.  Traffic grows with the output
+# written (the zeroed A and B are read back by the red.global.add flush), so a launch on another
+# mesh is scaled by its output bytes.
 SYM_TRAFFIC_F5120 = {"bytes": 158.986496e6 + 119.639296e6, "output_bytes": 2562 * 2562 * 8 + 2562 * 5120 * 8}
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # FP32 FMA lanes x 2 flops x max SM clock
 
 
 def roofline(args, mesh, stages, peaks):
-    """Roofline of the element-pair assembly kernel (the dominant kernel of
-    the step: sym_pairs_kernel in the mixed form, regular_pairs_kernel in
-    FP64).  achieved = algorithmic bytes per launch / its CUDA-event
-    duration; algorithmic bytes = the output it produces, A (N^2) and the RHS
-    operator B (N x F), c64 entries in the mixed form, c128 in FP64.  The
-    kernel is bound by FP32 FMA/SFU issue, not HBM: the compute fraction
-    (72 flops per ordered point pair, the algorithmic count) is reported
-    beside it."""
+    """Roofline of the element-pair assembly kernel (sym_pairs_kernel<6>, the
+    largest SM-filling kernel of the mixed form; its time is the CUDA-event
+    time of its launch, stages_ms.regular_ms).
+
+    The kernel is bound by FP32 instruction issue (FMA + MUFU), not by HBM:
+    about 1,300 flops per byte it writes.  So the binding fraction is the
+    compute one: achieved = 72 flops per ordered regular point pair (the
+    algorithmic count of the combined Burton-Miller integrand) x the point
+    pairs of one launch / its duration, against the nominal FP32 FMA rate
+    (MEASURED_PEAKS.json holds no FP32 SIMT peak).  The HBM figures beside it:
+    algorithmic bytes = A (N^2) + the RHS operator B (N x F), c64; traffic =
+    ncu DRAM bytes of the F = 5,120 launch scaled by output bytes."""
     F, N = mesh.num_faces, mesh.num_vertices
-    esz = 16 if args.precision == "fp64" else 8
     regular_pairs = F * F - (13 * F - 60)
     point_pairs = 36 * regular_pairs
-    alg_bytes = N * N * esz + N * F * esz
+    alg_bytes = N * N * 8 + N * F * 8
     t = stages["regular_ms"] / 1e3
-    achieved = alg_bytes / t / 1e9 if t > 0 else None
-    peak = peaks["hbm_gbs"]
-    traffic = None
-    if esz == 8:
-        traffic = SYM_TRAFFIC_F5120["bytes"] * alg_bytes / SYM_TRAFFIC_F5120["output_bytes"]
     flops = point_pairs * 72.0
-    fp_peak = 148 * 128 * 2 * 1.965e9 / (2 if args.precision == "fp64" else 1)
-    kernel = ("regular_pairs_kernel<double, 6> (element-pair Galerkin assembly)" if esz == 16 else
-              "sym_pairs_kernel<6> (element-pair Galerkin assembly, both orders per unordered pair)")
-    return {"kernel": kernel, "bound": "hbm",
-            "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-            "traffic_basis": "ncu dram read+write of the F=5,120 launch scaled by output bytes" if traffic else None,
-            "peak_source": f"{peaks['source']} hbm_gbs (MEASURED_PEAKS.json)" if peaks["source"] == "measured"
-            else "fallback 6.65 TB/s",
-            "algorithmic_bytes_per_launch": alg_bytes,
-            "compute": {"point_pairs_per_launch": point_pairs, "flops_per_point_pair": 72,
-                        "achieved_tflops": flops / t / 1e12 if t > 0 else None,
-                        "peak_tflops": fp_peak / 1e12,
-                        "peak_basis": "nominal FP32 (FP64 for the fp64 form) FMA issue, 148 SMs at 1965 MHz",
-                        "frac": (flops / t / fp_peak) if t > 0 else None}}
+    achieved = flops / t / 1e12 if t > 0 else None
+    gbs = alg_bytes / t / 1e9 if t > 0 else None
+    traffic = SYM_TRAFFIC_F5120["bytes"] * alg_bytes / SYM_TRAFFIC_F5120["output_bytes"]
+    return {"kernel": "sym_pairs_kernel<6> (element-pair Galerkin assembly, both orders per unordered pair)",
+            "bound": "fp32_issue", "achieved": achieved, "peak": FP32_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+            "frac": (achieved / FP32_NOMINAL_TFLOPS) if achieved else None,
+            "peak_source": "nominal FP32 FMA issue: 148 SMs x 128 lanes x 2 flops x 1965 MHz",
+            "flops_per_launch": flops, "point_pairs_per_launch": point_pairs, "flops_per_point_pair": 72,
+            "traffic": traffic,
+            "traffic_basis": "ncu dram read+write of the F=5,120 launch scaled by output bytes",
+            "hbm": {"achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                    "frac": (gbs / peaks["hbm_gbs"]) if gbs else None,
+                    "algorithmic_bytes_per_launch": alg_bytes,
+                    "peak_source": "measured hbm_gbs (MEASURED_PEAKS.json)" if peaks["source"] == "measured"
+                    else "fallback 6.65 TB/s"}}
 
 
 def main():
@@ -439,17 +616,13 @@ def main():
     ap.add_argument("--steps", type=int, default=24)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
-    ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
     ap.add_argument("--split", type=int, default=3, choices=(1, 3))
     ap.add_argument("--sub", type=int, default=5)
     ap.add_argument("--rhs", type=int, default=16)
-    ap.add_argument("--e2e-steps", type=int, default=6)
-    ap.add_argument("--cpu-sample-faces", type=int, default=640)
-    ap.add_argument("--cpu-lu-n", type=int, default=4096)
-    ap.add_argument("--ref-sample-faces", type=int, default=160)
-    ap.add_argument("--ref-lu-n", type=int, default=2048)
+    ap.add_argument("--cpu-slices", type=int, default=2,
+                    help="assembly slices timed by the cpu_baseline leg (of %d per frequency)" % CPU_SLICES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--check-accuracy", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 arm")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         ap.error("--warmup must be >= 3")

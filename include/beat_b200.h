@@ -238,14 +238,21 @@ int64_t beat_b200_device_bytes(const beat_b200_ctx *ctx);
  * for callers whose device memory belongs to their own pool (so a
  * library-side cudaMalloc would bypass its accounting) or that cannot afford
  * cudaMalloc/cudaFree on their thread.  d_b (input) and d_x (output) are
- * distinct device buffers of N x R complex doubles, column-major.  The FP64
+ * non-overlapping device buffers of N x R complex doubles, column-major.
+ * The factors must come from beat_b200_solve or beat_b200_solve_device:
+ * after a sweep (whose lanes leave no factors the caller can name), a failed
+ * solve or a change of mesh, symmetry or admittance the call returns
+ * BEAT_B200_STATE.  The FP64
  * form gives the exact LU solution; the mixed form gives its FP32-LU
  * solution without the GMRES refinement.  Limit: N <= 262144.  Its scratch
  * is a 16 KB static device array that every GPU loading the library holds
  * until exit, shared by all calls on that device: calls whose work overlaps
  * on the GPU race and must be serialised by the caller.  The first call on a
- * device looks up that array's address; make that first call before any
- * stream capture.  Synchronises the context's stream before returning. */
+ * device looks up that array's address and keeps it for the life of the
+ * process; a cudaDeviceReset of that device invalidates it, so do not call
+ * this entry point on a device after resetting it.  Make the first call on a
+ * device before any stream capture.  Synchronises the context's stream
+ * before returning. */
 int32_t beat_b200_resolve_noalloc(beat_b200_ctx *ctx, int32_t R, const void *d_b, void *d_x);
 
 /* Frequency sweep: nfreq independent solves of this mesh, each followed by

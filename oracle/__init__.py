@@ -20,7 +20,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libbemoracle.so")
 _lib = None
 
-SKIP_REGULAR, SKIP_SINGULAR, SKIP_IDENTITY = 1, 2, 4
+SKIP_REGULAR, SKIP_SINGULAR, SKIP_IDENTITY, NO_CLEAR = 1, 2, 4, 8
 
 
 def build(force: bool = False) -> str:
@@ -75,11 +75,14 @@ def _mesh_args(mesh):
 
 
 def assemble(mesh, k_signed, eta, q=None, quad_order=4, sing_order=4, threads=0, flags=0,
-             test_range=None):
+             test_range=None, out=None):
     """Fused Burton-Miller system ``(A, b)``: ``A`` is ``N x N`` complex128,
     ``b`` ``N x R``.  ``q`` is ``F x R`` (or ``F``) complex Neumann data,
     ``k_signed`` the outgoing wavenumber, ``eta`` the imaginary part of the
-    coupling (``burton_miller_coupling``)."""
+    coupling (``burton_miller_coupling``).  ``test_range`` restricts the
+    element pairs to test faces [t0, t1); ``out = (A, b)`` (Fortran-ordered
+    complex128, ``b`` with max(R, 1) columns) reuses buffers, and with
+    ``flags & NO_CLEAR`` the slice accumulates into them."""
     v, f = _mesh_args(mesh)
     N, F = mesh.num_vertices, mesh.num_faces
     if q is None:
@@ -89,8 +92,14 @@ def assemble(mesh, k_signed, eta, q=None, quad_order=4, sing_order=4, threads=0,
         q = q[:, None]
     R = q.shape[1]
     qf = np.asfortranarray(q)
-    A = np.zeros((N, N), dtype=np.complex128, order="F")
-    b = np.zeros((N, max(R, 1)), dtype=np.complex128, order="F")
+    if out is None:
+        A = np.zeros((N, N), dtype=np.complex128, order="F")
+        b = np.zeros((N, max(R, 1)), dtype=np.complex128, order="F")
+    else:
+        A, b = out
+        if (A.shape != (N, N) or b.shape != (N, max(R, 1)) or A.dtype != np.complex128 or b.dtype != np.complex128
+                or not A.flags.f_contiguous or not b.flags.f_contiguous):
+            raise ValueError("out must be Fortran-ordered complex128 (N x N, N x max(R, 1)) buffers")
     t0, t1 = (0, F) if test_range is None else test_range
     st = lib().bo_assemble_range(N, _dp(v), F, _ip(f), quad_order, sing_order, float(k_signed), float(eta),
                                  R, qf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),

@@ -43,6 +43,7 @@
 #define BO_SKIP_REGULAR 1
 #define BO_SKIP_SINGULAR 2
 #define BO_SKIP_IDENTITY 4
+#define BO_NO_CLEAR 8 /* accumulate into A and b as given (a slice of a larger assembly) */
 
 static const double BO_PI = 3.14159265358979323846;
 
@@ -652,8 +653,10 @@ int bo_assemble_range(int V, const double *verts, int F, const int *faces,
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #endif
-    memset(A, 0, sizeof(double) * 2 * (size_t)N * N);
-    if (R > 0) memset(b, 0, sizeof(double) * 2 * (size_t)N * R);
+    if (!(flags & BO_NO_CLEAR)) {
+        memset(A, 0, sizeof(double) * 2 * (size_t)N * N);
+        if (R > 0) memset(b, 0, sizeof(double) * 2 * (size_t)N * R);
+    }
     if (test_begin < 0) test_begin = 0;
     if (test_end > F) test_end = F;
 
