@@ -28,6 +28,7 @@ EXPORTS = (
     "beat_b200_last_error", "beat_b200_set_mesh", "beat_b200_solve", "beat_b200_solve_device",
     "beat_b200_field", "beat_b200_farfield", "beat_b200_farfield_device", "beat_b200_assemble",
     "beat_b200_release_workspace", "beat_b200_device_bytes", "beat_b200_stream", "beat_b200_resolve_noalloc",
+    "beat_b200_sweep_batch", "beat_b200_sweep_batch_device",
     "beat_b200_sweep", "beat_b200_sweep_device", "beat_b200_set_admittance", "beat_b200_adjoint",
     "beat_b200_set_symmetry", "beat_b200_field_gradient", "beat_b200_field_gradient_device",
     "beat_b200_rhs_use_operator", "beat_b200_assemble_coupled_device", "beat_b200_coupled_blocks_device",
@@ -40,7 +41,7 @@ SYMMETRY_MODES = {"off": 0, "x": 1, "xy": 2, "ground": 3}
 class Opts(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("ir_restart", ctypes.c_int32), ("ir_max_iters", ctypes.c_int32),
                 ("lu_split_terms", ctypes.c_int32), ("ir_rtol", ctypes.c_double), ("lu_block", ctypes.c_int32),
-                ("flags", ctypes.c_int32)]
+                ("flags", ctypes.c_int32), ("sweep_lanes", ctypes.c_int32)]
 
 
 class Diag(ctypes.Structure):
@@ -149,6 +150,12 @@ def load(path: str = LIB_PATH):
     L.beat_b200_sweep_device.argtypes = [vp, i32, dp, dp, i32, vp, ctypes.POINTER(Opts), vp, i32, dp, vp,
                                          ctypes.POINTER(Diag)]
     L.beat_b200_sweep_device.restype = i32
+    pp = ctypes.POINTER(vp)
+    L.beat_b200_sweep_batch.argtypes = [i32, pp, ip, pp, pp, ip, pp, ctypes.POINTER(Opts), pp, i32, dp, pp, pp]
+    L.beat_b200_sweep_batch.restype = i32
+    L.beat_b200_sweep_batch_device.argtypes = [i32, pp, ip, pp, pp, ip, pp, ctypes.POINTER(Opts), pp, i32, dp, pp,
+                                               pp]
+    L.beat_b200_sweep_batch_device.restype = i32
     L.beat_b200_set_symmetry.argtypes = [vp, i32]
     L.beat_b200_set_symmetry.restype = i32
     L.beat_b200_set_admittance.argtypes = [vp, dp]
@@ -423,3 +430,77 @@ class Context:
     def stream_handle(self) -> int:
         """cudaStream_t of this context as an integer (for torch.cuda.ExternalStream)."""
         return int(self.lib.beat_b200_stream(self.handle) or 0)
+
+
+def _ptrs(arrays):
+    """ctypes array of the data pointers of `arrays` (None -> NULL)."""
+    return (ctypes.c_void_p * len(arrays))(*[None if a is None else a.ctypes.data for a in arrays])
+
+
+def _handles(ctxs):
+    return (ctypes.c_void_p * len(ctxs))(*[c.handle.value for c in ctxs])
+
+
+def sweep_batch(ctxs, k_signed, eta, q, opts=None, dirs=None):
+    """Several meshes' frequency sweeps as one job list (beat_b200_sweep_batch):
+    ``ctxs[m]`` is mesh m's context, ``k_signed[m]`` / ``eta[m]`` its
+    frequencies' wavenumbers and couplings, ``q[m]`` its F x R x nfreq Neumann
+    data, ``opts[m]`` (or None) its options.  The lanes take the jobs in
+    decreasing order of cost.  Returns per mesh (p: N x R x nfreq, far field:
+    M x R x nfreq or None, diagnostics)."""
+    nm = len(ctxs)
+    L = ctxs[0].lib
+    ks = [np.ascontiguousarray(k, dtype=np.float64).ravel() for k in k_signed]
+    es = [np.ascontiguousarray(e, dtype=np.float64).ravel() for e in eta]
+    qs, ps, ffs, diags = [], [], [], []
+    dd = None if dirs is None else np.ascontiguousarray(dirs, dtype=np.float64).reshape(-1, 3)
+    M = 0 if dd is None else dd.shape[0]
+    for m, c in enumerate(ctxs):
+        nf = ks[m].size
+        if es[m].size != nf:
+            raise ValueError("k_signed and eta must have one entry per frequency")
+        qm = np.asfortranarray(np.asarray(q[m], dtype=np.complex128).reshape(c.F, -1, nf))
+        qs.append(qm)
+        R = qm.shape[1]
+        ps.append(np.zeros((c.V, R, nf), dtype=np.complex128, order="F"))
+        ffs.append(np.zeros((M, R, nf), dtype=np.complex128, order="F") if M else None)
+        diags.append((Diag * max(nf, 1))())
+    nfreq = (ctypes.c_int32 * nm)(*[k.size for k in ks])
+    Rs = (ctypes.c_int32 * nm)(*[qm.shape[1] for qm in qs])
+    optarr = None
+    if opts is not None:
+        optarr = (Opts * nm)(*[o if o is not None else Context.opts() for o in opts])
+    dg = (ctypes.c_void_p * nm)(*[ctypes.addressof(d) for d in diags])
+    st = L.beat_b200_sweep_batch(nm, _handles(ctxs), nfreq, _ptrs(ks), _ptrs(es), Rs, _ptrs(qs), optarr, _ptrs(ps),
+                                 M, _dp(dd) if dd is not None else None, _ptrs(ffs) if M else None, dg)
+    for c in ctxs[1:]:
+        c.generation += 1
+    ctxs[0]._check(st)
+    return [(ps[m], ffs[m], [diags[m][i].as_dict() for i in range(ks[m].size)]) for m in range(nm)]
+
+
+def sweep_batch_device(ctxs, k_signed, eta, d_q, R, d_p, opts=None, dirs=None, d_ff=None):
+    """beat_b200_sweep_batch_device: per mesh m, d_q[m], d_p[m] and d_ff[m] are
+    device pointers (F x R, N x R, M x R complex128 slices, one per frequency).
+    Returns each mesh's per-frequency diagnostics."""
+    nm = len(ctxs)
+    L = ctxs[0].lib
+    ks = [np.ascontiguousarray(k, dtype=np.float64).ravel() for k in k_signed]
+    es = [np.ascontiguousarray(e, dtype=np.float64).ravel() for e in eta]
+    dd = None if dirs is None else np.ascontiguousarray(dirs, dtype=np.float64).reshape(-1, 3)
+    M = 0 if dd is None else dd.shape[0]
+    diags = [(Diag * max(k.size, 1))() for k in ks]
+    nfreq = (ctypes.c_int32 * nm)(*[k.size for k in ks])
+    Rs = (ctypes.c_int32 * nm)(*R)
+    optarr = None
+    if opts is not None:
+        optarr = (Opts * nm)(*[o if o is not None else Context.opts() for o in opts])
+    vpa = ctypes.c_void_p * nm
+    dg = vpa(*[ctypes.addressof(d) for d in diags])
+    st = L.beat_b200_sweep_batch_device(nm, _handles(ctxs), nfreq, _ptrs(ks), _ptrs(es), Rs, vpa(*d_q), optarr,
+                                        vpa(*d_p), M, _dp(dd) if dd is not None else None,
+                                        vpa(*d_ff) if M else None, dg)
+    for c in ctxs[1:]:
+        c.generation += 1
+    ctxs[0]._check(st)
+    return [[diags[m][i].as_dict() for i in range(ks[m].size)] for m in range(nm)]

@@ -10,6 +10,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <algorithm>
 #include <atomic>
 #include <new>
 #include <thread>
@@ -40,6 +41,8 @@ template <typename F> int32_t guarded(beat_b200_ctx *c, F &&fn) {
     }
 }
 
+constexpr int MAX_SWEEP_LANES = 16;
+
 beat_b200_opts resolve_opts(const beat_b200_opts *o) {
     beat_b200_opts r;
     beat_b200_default_opts(&r);
@@ -50,6 +53,8 @@ beat_b200_opts resolve_opts(const beat_b200_opts *o) {
     if (r.lu_split_terms != 1 && r.lu_split_terms != 3) r.lu_split_terms = 3;
     BB_REQUIRE(r.precision == BEAT_B200_FP64 || r.precision == BEAT_B200_MIXED_FP32_IR, BEAT_B200_INVALID_ARG,
                "unknown precision form");
+    BB_REQUIRE(r.sweep_lanes >= 0 && r.sweep_lanes <= MAX_SWEEP_LANES, BEAT_B200_INVALID_ARG,
+               "sweep_lanes must be 0 (default) or 1.." + std::to_string(MAX_SWEEP_LANES));
     if (r.lu_block <= 0) r.lu_block = 128;  // measured best for both forms at N = 10,242
     BB_REQUIRE(r.lu_block == 32 || r.lu_block == 64 || r.lu_block == 128 || r.lu_block == 256,
                BEAT_B200_INVALID_ARG, "lu_block must be 32, 64, 128 or 256");
@@ -203,30 +208,45 @@ static int64_t held_matrix_bytes(const beat_b200_ctx *l) {
     return (int64_t)(l->ws.A.bytes + l->ws.Aop.bytes + l->ws.B.bytes);
 }
 
-// How many lanes to run: up to SWEEP_LANES (SWEEP_LANES_FP64 in the FP64
-// form), as many as there are frequencies,
-// and only as many as can hold a system matrix (with the FP32 operator copy in
-// the mixed form, and the N x F mapping when the right-hand sides may be
-// cached) beside a 512 MiB margin in the free device memory; buffers a lane
-// already holds count as available.  Lane 0 always runs.
-static int sweep_lane_count(beat_b200_ctx *c, int nfreq, const beat_b200_opts &o, int R) {
+// device bytes one lane of context c needs for a solve with these options
+static int64_t lane_bytes(const beat_b200_ctx *c, const beat_b200_opts &o, int R) {
     const bool fp64 = o.precision == BEAT_B200_FP64;
-    const int want = std::min(fp64 ? SWEEP_LANES_FP64 : SWEEP_LANES, nfreq);
-    if (want <= 1) return 1;
     const int64_t ld = ((int64_t)c->V + 127) / 128 * 128;
     const int64_t csz = fp64 ? 16 : 8;
     const int req = rhs_request(o);
-    const bool may_cache =
-        c->adm_set || req == BEAT_B200_RHS_CACHED || (req == BEAT_B200_RHS_AUTO && R >= 2);
-    const int64_t per_lane = (int64_t)c->V * ld * csz * (fp64 ? 1 : 2) +
-                             (may_cache ? (int64_t)c->V * c->F * csz : 0) + (512ll << 20);
+    const bool may_cache = c->adm_set || req == BEAT_B200_RHS_CACHED || (req == BEAT_B200_RHS_AUTO && R >= 2);
+    return (int64_t)c->V * ld * csz * (fp64 ? 1 : 2) + (may_cache ? (int64_t)c->V * c->F * csz : 0);
+}
+
+static int default_lanes(const beat_b200_opts &o) {
+    if (o.sweep_lanes > 0) return o.sweep_lanes;
+    return o.precision == BEAT_B200_FP64 ? SWEEP_LANES_FP64 : SWEEP_LANES;
+}
+
+// How many lanes a sweep over the contexts cs (one per mesh) runs: the
+// requested count (default_lanes of the first mesh's options), no more than
+// there are jobs, and only as many as can hold every mesh's system matrix
+// (with the FP32 operator copy in the mixed form, and the N x F mapping when
+// the right-hand sides may be cached) beside a 512 MiB margin in the free
+// device memory; buffers a lane already holds count as available.  Lane 0
+// always runs.
+static int lane_count(const std::vector<beat_b200_ctx *> &cs, const std::vector<int> &R, int njobs,
+                      const beat_b200_opts *o) {
+    const int want = std::min(default_lanes(o[0]), njobs);
+    if (want <= 1) return 1;
     size_t free_b = 0, total_b = 0;
     BB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    int64_t avail = (int64_t)free_b - std::max<int64_t>(0, per_lane - held_matrix_bytes(c));
+    const int64_t margin = 512ll << 20;
+    int64_t avail = (int64_t)free_b;
+    for (size_t m = 0; m < cs.size(); ++m)  // lane 0 is the contexts themselves
+        avail -= std::max<int64_t>(0, lane_bytes(cs[m], o[m], R[m]) - held_matrix_bytes(cs[m]));
     int lanes = 1;
     for (int i = 1; i < want; ++i) {
-        const beat_b200_ctx *l = i - 1 < (int)c->lanes.size() ? c->lanes[i - 1] : nullptr;
-        const int64_t need = std::max<int64_t>(0, per_lane - (l ? held_matrix_bytes(l) : 0));
+        int64_t need = margin;
+        for (size_t m = 0; m < cs.size(); ++m) {
+            const beat_b200_ctx *l = i - 1 < (int)cs[m]->lanes.size() ? cs[m]->lanes[i - 1] : nullptr;
+            need += std::max<int64_t>(0, lane_bytes(cs[m], o[m], R[m]) - (l ? held_matrix_bytes(l) : 0));
+        }
         if (need > avail) break;
         avail -= need;
         ++lanes;
@@ -234,14 +254,59 @@ static int sweep_lane_count(beat_b200_ctx *c, int nfreq, const beat_b200_opts &o
     return lanes;
 }
 
-// Runs work(lane_ctx, f) for f = 0..nfreq-1, one host thread per lane (lane 0
-// on the calling thread).  Each lane takes the next unclaimed frequency from a
-// shared counter when it finishes one, so a lane that drew cheap frequencies
-// does not idle while another still holds a queue.  After a failure no lane
-// starts another frequency; the first error (by frequency) is rethrown after
-// every lane has stopped.
-template <typename W> void run_sweep(beat_b200_ctx *c, int nfreq, int lanes, W &&work) {
-    const int L = std::max(1, std::min(lanes, nfreq));
+static int sweep_lane_count(beat_b200_ctx *c, int nfreq, const beat_b200_opts &o, int R) {
+    return lane_count({c}, {R}, nfreq, &o);
+}
+
+// Runs work(lane, job) for the jobs in `order`, one host thread per lane (lane
+// 0 on the calling thread).  Each lane takes the next unclaimed job from a
+// shared counter when it finishes one, so a lane that drew cheap jobs does
+// not idle while another still holds a queue.  After a failure no lane starts
+// another job; the first error (by job number, named `what` in the message)
+// is rethrown after every lane has stopped, with stream_of(lane, job)
+// synchronised for the failed job.
+template <typename W, typename S>
+void run_jobs(beat_b200_ctx *c, int L, const std::vector<int> &order, const char *what, W &&work, S &&stream_of) {
+    const int njobs = (int)order.size();
+    std::vector<Error> err(L);
+    std::vector<int> err_job(L, -1);
+    std::atomic<int> next{0};
+    std::atomic<bool> failed{false};
+    auto body = [&](int i) {
+        try {
+            BB_CUDA(cudaSetDevice(c->device));
+            for (int t = next.fetch_add(1); t < njobs && !failed.load(); t = next.fetch_add(1)) {
+                err_job[i] = order[t];
+                work(i, order[t]);
+            }
+            err_job[i] = -1;
+        } catch (const Error &e) {
+            err[i] = e;
+        } catch (const std::bad_alloc &) {
+            err[i] = Error{BEAT_B200_OOM, "host allocation failed"};
+        } catch (...) {
+            err[i] = Error{BEAT_B200_CUDA_ERROR, "unexpected exception"};
+        }
+        if (err_job[i] >= 0) {
+            failed.store(true);
+            cudaStream_t st = stream_of(i, err_job[i]);
+            if (st) cudaStreamSynchronize(st);
+        }
+    };
+    std::vector<std::thread> th;
+    for (int i = 1; i < L; ++i) th.emplace_back(body, i);
+    body(0);
+    for (auto &t : th) t.join();
+    int first = -1;
+    for (int i = 0; i < L; ++i)
+        if (err_job[i] >= 0 && (first < 0 || err_job[i] < err_job[first])) first = i;
+    if (first >= 0)
+        throw Error{err[first].code, std::string(what) + " " + std::to_string(err_job[first]) + ": " + err[first].msg};
+}
+
+// The lanes of context c for a sweep of L lanes (lane 0 is c itself), with
+// c's admittance copied to the others.
+static std::vector<beat_b200_ctx *> prepare_lanes(beat_b200_ctx *c, int L) {
     std::vector<beat_b200_ctx *> lane(L);
     for (int i = 0; i < L; ++i) lane[i] = sweep_lane(c, i);
     for (int i = 1; i < L; ++i) {  // the lanes solve with this context's admittance
@@ -252,43 +317,68 @@ template <typename W> void run_sweep(beat_b200_ctx *c, int nfreq, int lanes, W &
         }
         lane[i]->ws.lu_valid = 0;
     }
-    std::vector<Error> err(L);
-    std::vector<int> err_f(L, -1);
-    std::atomic<int> next{0};
-    std::atomic<bool> failed{false};
-    auto body = [&](int i) {
-        try {
-            BB_CUDA(cudaSetDevice(c->device));
-            for (int f = next.fetch_add(1); f < nfreq && !failed.load(); f = next.fetch_add(1)) {
-                err_f[i] = f;
-                work(lane[i], f);
-            }
-            err_f[i] = -1;
-        } catch (const Error &e) {
-            err[i] = e;
-        } catch (const std::bad_alloc &) {
-            err[i] = Error{BEAT_B200_OOM, "host allocation failed"};
-        } catch (...) {
-            err[i] = Error{BEAT_B200_CUDA_ERROR, "unexpected exception"};
-        }
-        if (err_f[i] >= 0) {
-            failed.store(true);
-            if (lane[i]->stream) cudaStreamSynchronize(lane[i]->stream);
-        }
+    return lane;
+}
+
+// Runs work(lane_ctx, f) for f = 0..nfreq-1 over L lanes of c.  Afterwards no
+// lane offers its factors: lane 0 is this context, and its factors belong to
+// whichever frequency it solved last, which the caller cannot name, so
+// beat_b200_resolve_noalloc and beat_b200_adjoint refuse them.
+template <typename W> void run_sweep(beat_b200_ctx *c, int nfreq, int lanes, W &&work) {
+    const int L = std::max(1, std::min(lanes, nfreq));
+    std::vector<beat_b200_ctx *> lane = prepare_lanes(c, L);
+    std::vector<int> order(nfreq);
+    for (int f = 0; f < nfreq; ++f) order[f] = f;
+    try {
+        run_jobs(
+            c, L, order, "frequency", [&](int i, int f) { work(lane[i], f); },
+            [&](int i, int) { return lane[i]->stream; });
+    } catch (...) {
+        for (beat_b200_ctx *l : lane) l->ws.lu_valid = 0;
+        throw;
+    }
+    for (beat_b200_ctx *l : lane) l->ws.lu_valid = 0;
+}
+
+// Several meshes' sweeps as one job list over L lanes: job (m, f) is mesh m
+// at its frequency f, on lane i's context of mesh m.  Jobs are taken in
+// decreasing order of cost (N^3, the factorisation), so the lanes finish
+// together instead of one lane ending on the largest mesh alone.
+template <typename W>
+void run_batch(const std::vector<beat_b200_ctx *> &cs, const std::vector<int> &nfreq, int lanes, W &&work) {
+    const int nm = (int)cs.size();
+    std::vector<int> base(nm + 1, 0);
+    for (int m = 0; m < nm; ++m) base[m + 1] = base[m] + nfreq[m];
+    const int njobs = base[nm];
+    if (njobs == 0) return;
+    const int L = std::max(1, std::min(lanes, njobs));
+    std::vector<std::vector<beat_b200_ctx *>> lane(nm);
+    for (int m = 0; m < nm; ++m) lane[m] = prepare_lanes(cs[m], L);
+    std::vector<int> order(njobs), mesh_of(njobs);
+    for (int m = 0; m < nm; ++m)
+        for (int f = 0; f < nfreq[m]; ++f) mesh_of[base[m] + f] = m;
+    for (int j = 0; j < njobs; ++j) order[j] = j;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        const double na = cs[mesh_of[a]]->V, nb = cs[mesh_of[b]]->V;
+        return na * na * na > nb * nb * nb;
+    });
+    auto clear = [&] {
+        for (auto &v : lane)
+            for (beat_b200_ctx *l : v) l->ws.lu_valid = 0;
     };
-    std::vector<std::thread> th;
-    for (int i = 1; i < L; ++i) th.emplace_back(body, i);
-    body(0);
-    for (auto &t : th) t.join();
-    // lane 0 is this context: its factors now belong to whichever frequency it
-    // solved last, which the caller cannot name, so they are not offered to
-    // beat_b200_resolve_noalloc or beat_b200_adjoint
-    for (int i = 0; i < L; ++i) lane[i]->ws.lu_valid = 0;
-    int first = -1;
-    for (int i = 0; i < L; ++i)
-        if (err_f[i] >= 0 && (first < 0 || err_f[i] < err_f[first])) first = i;
-    if (first >= 0)
-        throw Error{err[first].code, "frequency " + std::to_string(err_f[first]) + ": " + err[first].msg};
+    try {
+        run_jobs(
+            cs[0], L, order, "job (mesh-major numbering)",
+            [&](int i, int j) {
+                const int m = mesh_of[j];
+                work(lane[m][i], m, j - base[m]);
+            },
+            [&](int i, int j) { return lane[mesh_of[j]][i]->stream; });
+    } catch (...) {
+        clear();
+        throw;
+    }
+    clear();
 }
 
 }  // namespace
@@ -617,6 +707,96 @@ int32_t beat_b200_sweep(beat_b200_ctx *c, int32_t nfreq, const double *k_signed,
             if (M > 0)
                 BB_CUDA(cudaMemcpyAsync(ff_out + f * fs, dff, fs * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
             BB_CUDA(cudaStreamSynchronize(l->stream));
+        });
+    });
+}
+
+// the contexts, options and column counts of a batched sweep, checked
+static void batch_inputs(int32_t nmesh, beat_b200_ctx *const *ctxs, const int32_t *nfreq, const int32_t *R,
+                         const beat_b200_opts *opts, std::vector<beat_b200_ctx *> &cs, std::vector<int> &nf,
+                         std::vector<int> &rr, std::vector<beat_b200_opts> &o) {
+    BB_REQUIRE(nmesh >= 1 && ctxs && nfreq && R, BEAT_B200_INVALID_ARG, "batched sweep: bad arguments");
+    for (int m = 0; m < nmesh; ++m) {
+        beat_b200_ctx *c = ctxs[m];
+        BB_REQUIRE(c, BEAT_B200_INVALID_ARG, "batched sweep: null context");
+        BB_REQUIRE(c->device == ctxs[0]->device, BEAT_B200_INVALID_ARG,
+                   "batched sweep: every context must be on the same device");
+        for (int j = 0; j < m; ++j)
+            BB_REQUIRE(ctxs[j] != c, BEAT_B200_INVALID_ARG, "batched sweep: a context appears twice");
+        BB_REQUIRE(c->F > 0, BEAT_B200_STATE, "batched sweep: a context has no mesh");
+        BB_REQUIRE(nfreq[m] >= 0 && R[m] >= 1, BEAT_B200_INVALID_ARG, "batched sweep: nfreq >= 0 and R >= 1");
+        cs.push_back(c);
+        nf.push_back(nfreq[m]);
+        rr.push_back(R[m]);
+        o.push_back(resolve_opts(opts ? opts + m : nullptr));
+    }
+}
+
+int32_t beat_b200_sweep_batch(int32_t nmesh, beat_b200_ctx *const *ctxs, const int32_t *nfreq,
+                              const double *const *k_signed, const double *const *eta_im, const int32_t *R,
+                              const double *const *q, const beat_b200_opts *opts, double *const *p_out, int32_t M,
+                              const double *dirs, double *const *ff_out, beat_b200_diag *const *diags) {
+    if (nmesh < 1 || !ctxs || !ctxs[0]) return BEAT_B200_INVALID_ARG;
+    return guarded(ctxs[0], [&] {
+        std::vector<beat_b200_ctx *> cs;
+        std::vector<int> nf, rr;
+        std::vector<beat_b200_opts> o;
+        batch_inputs(nmesh, ctxs, nfreq, R, opts, cs, nf, rr, o);
+        BB_REQUIRE(k_signed && eta_im && q && p_out, BEAT_B200_INVALID_ARG, "batched sweep: null pointer");
+        BB_REQUIRE(M >= 0 && (M == 0 || (dirs && ff_out)), BEAT_B200_INVALID_ARG,
+                   "batched sweep: bad far-field arguments");
+        int njobs = 0;
+        for (int m = 0; m < nmesh; ++m) {
+            BB_REQUIRE(nf[m] == 0 || (k_signed[m] && eta_im[m] && q[m] && p_out[m] && (M == 0 || ff_out[m])),
+                       BEAT_B200_INVALID_ARG, "batched sweep: null pointer for mesh " + std::to_string(m));
+            njobs += nf[m];
+        }
+        run_batch(cs, nf, lane_count(cs, rr, njobs, o.data()), [&](beat_b200_ctx *l, int m, int f) {
+            const int Rm = rr[m];
+            const size_t qs = (size_t)cs[m]->F * Rm * 2, ps = (size_t)cs[m]->V * Rm * 2, fs = (size_t)M * Rm * 2;
+            ensure_workspace(l, o[m].precision, Rm, rhs_request(o[m]));
+            Workspace &w = l->ws;
+            BB_CUDA(cudaMemcpyAsync(w.q.p, q[m] + f * qs, qs * sizeof(double), cudaMemcpyHostToDevice, l->stream));
+            w.io.alloc((ps + fs) * sizeof(double));
+            double *dp = w.io.as<double>(), *dff = dp + ps;
+            solve_core(l, k_signed[m][f], eta_im[m][f], Rm, w.q.as<double>(), o[m], dp,
+                       diags && diags[m] ? diags[m] + f : nullptr);
+            if (M > 0) farfield(l, k_signed[m][f], M, dirs, Rm, dp, w.q.as<double>(), dff, true);
+            BB_CUDA(cudaMemcpyAsync(p_out[m] + f * ps, dp, ps * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
+            if (M > 0)
+                BB_CUDA(cudaMemcpyAsync(ff_out[m] + f * fs, dff, fs * sizeof(double), cudaMemcpyDeviceToHost,
+                                        l->stream));
+            BB_CUDA(cudaStreamSynchronize(l->stream));
+        });
+    });
+}
+
+int32_t beat_b200_sweep_batch_device(int32_t nmesh, beat_b200_ctx *const *ctxs, const int32_t *nfreq,
+                                     const double *const *k_signed, const double *const *eta_im, const int32_t *R,
+                                     const void *const *d_q, const beat_b200_opts *opts, void *const *d_p, int32_t M,
+                                     const double *dirs, void *const *d_ff, beat_b200_diag *const *diags) {
+    if (nmesh < 1 || !ctxs || !ctxs[0]) return BEAT_B200_INVALID_ARG;
+    return guarded(ctxs[0], [&] {
+        std::vector<beat_b200_ctx *> cs;
+        std::vector<int> nf, rr;
+        std::vector<beat_b200_opts> o;
+        batch_inputs(nmesh, ctxs, nfreq, R, opts, cs, nf, rr, o);
+        BB_REQUIRE(k_signed && eta_im && d_q && d_p, BEAT_B200_INVALID_ARG, "batched sweep: null pointer");
+        BB_REQUIRE(M >= 0 && (M == 0 || (dirs && d_ff)), BEAT_B200_INVALID_ARG,
+                   "batched sweep: bad far-field arguments");
+        int njobs = 0;
+        for (int m = 0; m < nmesh; ++m) {
+            BB_REQUIRE(nf[m] == 0 || (k_signed[m] && eta_im[m] && d_q[m] && d_p[m] && (M == 0 || d_ff[m])),
+                       BEAT_B200_INVALID_ARG, "batched sweep: null pointer for mesh " + std::to_string(m));
+            njobs += nf[m];
+        }
+        run_batch(cs, nf, lane_count(cs, rr, njobs, o.data()), [&](beat_b200_ctx *l, int m, int f) {
+            const int Rm = rr[m];
+            const size_t qs = (size_t)cs[m]->F * Rm * 2, ps = (size_t)cs[m]->V * Rm * 2, fs = (size_t)M * Rm * 2;
+            const double *qd = (const double *)d_q[m] + f * qs;
+            double *pd = (double *)d_p[m] + f * ps;
+            solve_core(l, k_signed[m][f], eta_im[m][f], Rm, qd, o[m], pd, diags && diags[m] ? diags[m] + f : nullptr);
+            if (M > 0) farfield(l, k_signed[m][f], M, dirs, Rm, pd, qd, (double *)d_ff[m] + f * fs, true);
         });
     });
 }

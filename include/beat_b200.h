@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define BEAT_B200_ABI_VERSION 1
+#define BEAT_B200_ABI_VERSION 2 /* 2: beat_b200_opts.sweep_lanes, beat_b200_sweep_batch */
 
 /* status codes */
 #define BEAT_B200_OK 0
@@ -63,6 +63,8 @@ typedef struct {
     double ir_rtol;         /* relative residual target of the refinement (1e-10) */
     int32_t lu_block;       /* LU panel width; 0 = tuned default */
     int32_t flags;          /* BEAT_B200_FLAG_* bits, 0 by default */
+    int32_t sweep_lanes;    /* solve lanes of a sweep (1..16); 0 = default: 6 in the mixed
+                               form, 4 in FP64 (always capped by free device memory) */
 } beat_b200_opts;
 
 /* opts.flags: return the mixed form's direct FP32-LU solution without the
@@ -282,6 +284,37 @@ int32_t beat_b200_sweep_device(beat_b200_ctx *ctx, int32_t nfreq, const double *
                                const double *eta_im, int32_t R, const void *d_q,
                                const beat_b200_opts *opts, void *d_p, int32_t M,
                                const double *dirs, void *d_ff, beat_b200_diag *diags);
+
+/* Batched sweep: the frequency sweeps of nmesh meshes (meshes of uneven
+ * size, e.g. the variants of a design) as one job list over one set of solve
+ * lanes.  The reference runs its meshes' sweeps one after another, each
+ * overlapping assembly and solve only on Metal (start_sweep_assembly_pipeline
+ * / take_sweep_assembly!, src/BeatEngineCore.jl:1451-1599, called from
+ * BeatEngineCompiledDriver.jl:1222-1268).  Here mesh m (context ctxs[m], on
+ * one device, each with its mesh set) has nfreq[m] frequencies with
+ * k_signed[m][f], eta_im[m][f], R[m] columns, q[m] + f F_m R_m, p_out[m] +
+ * f N_m R_m and ff_out[m] + f M R_m (layouts as in beat_b200_sweep), options
+ * opts[m] (opts NULL: defaults), diagnostics diags[m][f] (diags or diags[m]
+ * may be NULL).  Every (mesh, frequency) is one job; the lanes (opts[0]'s
+ * sweep_lanes, capped by the free memory for every mesh) take the jobs in
+ * decreasing order of N^3, the factorisation's cost, each the next one when
+ * it finishes one.  Errors are reported on ctxs[0]; the first failing job in
+ * mesh-major numbering gives the status. */
+int32_t beat_b200_sweep_batch(int32_t nmesh, beat_b200_ctx *const *ctxs, const int32_t *nfreq,
+                              const double *const *k_signed, const double *const *eta_im,
+                              const int32_t *R, const double *const *q,
+                              const beat_b200_opts *opts, double *const *p_out, int32_t M,
+                              const double *dirs, double *const *ff_out,
+                              beat_b200_diag *const *diags);
+
+/* As beat_b200_sweep_batch with every mesh's q, p and far field in device
+ * memory. */
+int32_t beat_b200_sweep_batch_device(int32_t nmesh, beat_b200_ctx *const *ctxs,
+                                     const int32_t *nfreq, const double *const *k_signed,
+                                     const double *const *eta_im, const int32_t *R,
+                                     const void *const *d_q, const beat_b200_opts *opts,
+                                     void *const *d_p, int32_t M, const double *dirs,
+                                     void *const *d_ff, beat_b200_diag *const *diags);
 
 /* Symmetry images (the reference's symmetry_mode: normalized_symmetry_mode,
  * symmetry_transforms, BeatEngineCore.jl:448-482; image passes and

@@ -29,7 +29,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_defaults():
     L = _lib.load()
-    assert L.beat_b200_abi_version() == 1
+    assert L.beat_b200_abi_version() == 2
     o = _lib.Opts()
     L.beat_b200_default_opts(ctypes.byref(o))
     assert o.precision == _lib.MIXED_FP32_IR and o.ir_restart == 20 and abs(o.ir_rtol - 1e-10) < 1e-20
