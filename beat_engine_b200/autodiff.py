@@ -33,6 +33,7 @@ import numpy as np
 
 from . import _lib
 
+
 def _numpy(t):
     return t.detach().cpu().numpy()
 
@@ -69,7 +70,9 @@ def _function():
                 p, _ = _forward(ctx, faces, k_signed, eta, dirs, qn, an, xn, opts)
             g = np.asfortranarray(_numpy(grad).astype(np.complex128))
             gx = None
-            if fctx.needs_input_grad[9] and fctx.has_x:
+            # needs_input_grad follows forward's inputs: ctx, faces, k, eta, dirs, precision, q0 (6), a (7),
+            # vertices (8)
+            if fctx.has_x and fctx.needs_input_grad[8]:
                 w, ga, gx = ctx.adjoint_shape(k_signed, dirs, p, qn, g, opts)
                 gx = 0.5 * gx  # real input: dL/dX, not 2 dL/dX
             else:
