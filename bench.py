@@ -555,6 +555,126 @@ def run_gpu(args):
     return 0
 
 
+# --------------------------------------------------------------------------
+# --config sweep: six uneven enclosures x 64 frequencies, batched
+# --------------------------------------------------------------------------
+SWEEP_MESHES = (2000, 4000, 6000, 8000, 10000, 12000)
+SWEEP_FREQS = 64
+
+
+def sweep_workload():
+    """Rounded-box enclosures 0.2 x 0.3 x 0.25 m with a 0.05 m piston on the
+    front face, jittered 5 % of the edge length (seeded), at targets of 2k-12k
+    triangles; 64 log-spaced frequencies 100 Hz-8 kHz; the piston at 1 m/s
+    plus 4 seeded random-velocity columns (R = 5)."""
+    from beat_engine_b200 import mesh as M
+    meshes, vels = [], []
+    for i, nf in enumerate(SWEEP_MESHES):
+        m = M.rounded_box_enclosure(nf, seed=60 + i)
+        rng = np.random.default_rng(70 + i)
+        v = np.zeros((m.num_faces, 5), complex)
+        v[m.physical_tags == 2, 0] = 1.0
+        v[:, 1:] = rng.standard_normal((m.num_faces, 4)) + 1j * rng.standard_normal((m.num_faces, 4))
+        meshes.append(m)
+        vels.append(v)
+    return meshes, vels, np.geomspace(100.0, 8000.0, SWEEP_FREQS)
+
+
+def run_sweep_config(args):
+    """The batched sweep (beat_b200_sweep_batch_device, mixed form with
+    refinement, lu_block per mesh and the lane count from the autotuner)
+    against the per-frequency plain FP64 loop (beat_b200_solve_device, one
+    (mesh, frequency) after another), both with inputs resident in HBM and
+    timed with CUDA events; plus the batch end to end from host buffers, and
+    the mixed results' per-column error against the FP64 loop's over all
+    jobs."""
+    import torch
+
+    from beat_engine_b200 import _lib, autotune
+    dev = torch.device("cuda", 0)
+    meshes, vels, freqs = sweep_workload()
+    ks = 2 * math.pi * freqs / C0
+    ctxs, d_q, d_p, R = [], [], [], []
+    for m, v in zip(meshes, vels):
+        c = _lib.Context(0)
+        c.set_mesh(m.vertices, m.faces, 4, 4)
+        ctxs.append(c)
+        q = np.stack([neumann(v, f) for f in freqs], axis=2)  # F x R x nf
+        d_q.append(torch.from_numpy(np.ascontiguousarray(q.transpose(2, 1, 0))).to(dev))
+        d_p.append(torch.empty((len(freqs), v.shape[1], m.num_vertices), dtype=torch.complex128, device=dev))
+        R.append(v.shape[1])
+    # autotuner: panel width per mesh, lane count on the largest mesh (cached in JSON)
+    t0 = time.perf_counter()
+    tuned = []
+    for i, (c, v) in enumerate(zip(ctxs, vels)):
+        fm = float(np.sqrt(freqs[0] * freqs[-1]))
+        k = 2 * math.pi * fm / C0
+        lanes = autotune.LANES if i == len(ctxs) - 1 else (6,)
+        tuned.append(autotune.tune(c, k, 1 / k, neumann(v, fm), _lib.MIXED_FP32_IR, cache=args.tune_cache,
+                                   lanes=lanes))
+    tune_s = time.perf_counter() - t0
+    lanes = tuned[-1]["sweep_lanes"]
+    opts = [_lib.Context.opts(_lib.MIXED_FP32_IR, lu_block=t["lu_block"], sweep_lanes=lanes) for t in tuned]
+    kl, el = [ks] * len(ctxs), [1 / ks] * len(ctxs)
+
+    def batch():
+        return _lib.sweep_batch_device(ctxs, kl, el, [t.data_ptr() for t in d_q], R,
+                                       [t.data_ptr() for t in d_p], opts)
+
+    stream = torch.cuda.ExternalStream(ctxs[0].stream_handle(), device=dev)
+    for _ in range(max(1, args.warmup - 2)):
+        batch()
+    with ClockSampler(0) as clk:
+        ms, diags, _ = timed(stream, batch)
+    clocks = clk.summary()
+    n_jobs = len(ctxs) * len(freqs)
+    p_mixed = [t.cpu().numpy() for t in d_p]
+    # end to end from host buffers (pinned inputs)
+    q_host = [torch.from_numpy(np.ascontiguousarray(t.cpu().numpy())).pin_memory() for t in d_q]
+    qh = [x.numpy().transpose(2, 1, 0) for x in q_host]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _lib.sweep_batch(ctxs, kl, el, qh, opts)
+    e2e_s = time.perf_counter() - t0
+    # the per-frequency plain FP64 loop
+    o64 = _lib.Context.opts(_lib.FP64)
+    for c, q, p, r in zip(ctxs, d_q, d_p, R):  # warm: the FP64 workspaces
+        c.solve_device(ks[0], 1 / ks[0], q[0].data_ptr(), r, p[0].data_ptr(), o64)
+
+    def loop():
+        for c, q, p, r in zip(ctxs, d_q, d_p, R):
+            for f in range(len(freqs)):
+                c.solve_device(ks[f], 1 / ks[f], q[f].data_ptr(), r, p[f].data_ptr(), o64)
+
+    ms64, _, clocks64 = timed(stream, loop, clocks_device=0)
+    err = 0.0
+    for pm, t in zip(p_mixed, d_p):
+        p64 = t.cpu().numpy()
+        err = max(err, float(np.max(np.linalg.norm(pm - p64, axis=2) / np.linalg.norm(p64, axis=2))))
+    line = {"metric": "batched sweep: freq-solves/s over 6 enclosures x 64 frequencies, mixed FP32+IR, 1 B200",
+            "value": n_jobs / (ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": args.warmup,
+            "sweep_wall_s": ms / 1e3, "higher_is_better": True, "dtype": "c64 (tf32 tensor LU) + c128 refinement",
+            "data": "synthetic (seeded jittered enclosures and velocities)",
+            "config": {"workload": "rounded-box enclosures 0.2x0.3x0.25 m + 0.05 m piston, targets "
+                                   f"{list(SWEEP_MESHES)} triangles (F = {[m.num_faces for m in meshes]}, "
+                                   f"N = {[m.num_vertices for m in meshes]}), {SWEEP_FREQS} log-spaced "
+                                   "frequencies 100 Hz-8 kHz, piston 1 m/s + 4 random RHS (R = 5), order 4/4",
+                       "jobs": n_jobs, "lanes": lanes, "lu_block": [t["lu_block"] for t in tuned],
+                       "autotune_s": tune_s, "autotune_cached": [t["cached"] for t in tuned]},
+            "fp64_loop_value": n_jobs / (ms64 / 1e3), "fp64_loop_wall_s": ms64 / 1e3,
+            "speedup_vs_fp64_loop": ms64 / ms,
+            "e2e": {"value": n_jobs / e2e_s, "unit": UNIT, "wall_s": e2e_s,
+                    "h2d_bytes_per_step": int(sum(t.numel() * 16 for t in d_q)),
+                    "d2h_bytes_per_step": int(sum(t.numel() * 16 for t in d_p))},
+            "accuracy": {"max_rel_err_mixed_vs_fp64_loop": err, "jobs": n_jobs,
+                         "ir_converged": all(d["ir_converged"] == 1 for dm in diags for d in dm)},
+            "clocks": clocks, "fp64_clocks": clocks64}
+    print(json.dumps(line), flush=True)
+    for c in ctxs:
+        c.close()
+    return 0
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -623,11 +743,16 @@ def main():
                     help="assembly slices timed by the cpu_baseline leg (of %d per frequency)" % CPU_SLICES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 arm")
+    ap.add_argument("--config", choices=("headline", "sweep"), default="headline",
+                    help="sweep: the batched 6-enclosure x 64-frequency sweep against the FP64 loop")
+    ap.add_argument("--tune-cache", default=None, help="autotuner JSON cache (default ~/.cache/beat_b200)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.config == "sweep":
+        return run_sweep_config(args)
     return run_gpu(args)
 
 

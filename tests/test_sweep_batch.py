@@ -112,3 +112,28 @@ def test_batch_errors_are_status_codes(batch):
     assert e.value.status == _lib.INVALID_ARG
     p, _, _ = _lib.sweep_batch(ctxs[1:2], ks[1:2], [1 / ks[1]], qs[1:2])[0]
     assert np.all(np.isfinite(p))
+
+
+def test_sweep_config_subset_against_oracle():
+    """The benchmark's batched-sweep workload (bench.py --config sweep): its two
+    smallest enclosures at the first, middle and last of the 64 frequencies,
+    as one batch in the mixed form, against the FP64 oracle (1e-6)."""
+    from bench import neumann, sweep_workload
+    meshes, vels, freqs = sweep_workload()
+    sel = freqs[[0, 32, 63]]
+    ks = 2 * math.pi * sel / C0
+    ctxs = []
+    try:
+        for m in meshes[:2]:
+            c = _lib.Context(0)
+            c.set_mesh(m.vertices, m.faces, 4, 4)
+            ctxs.append(c)
+        qs = [np.stack([neumann(v, f) for f in sel], axis=2) for v in vels[:2]]
+        out = _lib.sweep_batch(ctxs, [ks, ks], [1 / ks, 1 / ks], qs)
+        for m, f in ((0, 0), (0, 1), (0, 2), (1, 2)):
+            A, b = oracle.assemble(meshes[m], ks[f], 1 / ks[f], qs[m][:, :, f])
+            assert rel(out[m][0][:, :, f], np.linalg.solve(A, b)) <= 1e-6, (m, f)
+            assert out[m][2][f]["ir_converged"] == 1
+    finally:
+        for c in ctxs:
+            c.close()
