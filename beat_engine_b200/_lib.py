@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "libbeatb200.so")
 
 OK, INVALID_ARG, OOM, CUDA_ERROR, NOT_CONVERGED, TIMEOUT, NO_DEVICE, STATE, SINGULAR = range(9)
 FP64, MIXED_FP32_IR = 0, 1
-FLAG_NO_REFINE, FLAG_RHS_MATRIX_FREE, FLAG_RHS_CACHED, FLAG_NO_FALLBACK, FLAG_PARTIAL_PIVOT = 1, 2, 4, 8, 16
+FLAG_NO_REFINE, FLAG_RHS_MATRIX_FREE, FLAG_RHS_CACHED, FLAG_NO_FALLBACK = 1, 2, 4, 8
 RHS_AUTO, RHS_MATRIX_FREE, RHS_CACHED = 0, 1, 2
 RHS_MODES = {"auto": RHS_AUTO, "matrix_free": RHS_MATRIX_FREE, "cached_operator": RHS_CACHED}
 STATUS_NAMES = {OK: "OK", INVALID_ARG: "INVALID_ARG", OOM: "OOM", CUDA_ERROR: "CUDA_ERROR",

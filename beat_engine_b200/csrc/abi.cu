@@ -114,7 +114,7 @@ void solve_core(beat_b200_ctx *c, double k, double eta, int R, const double *d_q
     if (o.precision != BEAT_B200_FP64)
         BB_CUDA(cudaMemcpyAsync(w.Aop.p, w.A.p, (size_t)n * w.ld * 8, cudaMemcpyDeviceToDevice, c->stream));
     BB_CUDA(cudaEventRecord(c->ev[4], c->stream));
-    lu_factor(c, o.precision, o.lu_block, o.lu_split_terms, !(o.flags & BEAT_B200_FLAG_PARTIAL_PIVOT));
+    lu_factor(c, o.precision, o.lu_block, o.lu_split_terms);
     BB_CUDA(cudaEventRecord(c->ev[5], c->stream));
     const int st = read_status(c);
     c->last_k = k;

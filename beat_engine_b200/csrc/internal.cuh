@@ -217,8 +217,6 @@ struct beat_b200_ctx {
     float last_regular_ms = 0.f;
     bool cluster_checked = false;  // can a 16-CTA cluster of the panel kernel be scheduled?
     bool cluster_ok = false;
-    bool tournament_checked = false;  // the same for the tournament-pivoted panel kernel
-    bool tournament_ok = false;
 
     // extra solve lanes of a frequency sweep: each a full context (own stream,
     // workspace and status words) over a copy of this mesh
@@ -250,9 +248,7 @@ void assemble(beat_b200_ctx *c, double k, double eta, int precision, int R, cons
               float *ms_total, float *ms_singular);
 
 // lu.cu
-// tournament: the mixed form's panels by tournament pivoting (else partial
-// pivoting, as LAPACK); the FP64 form always pivots partially
-void lu_factor(beat_b200_ctx *c, int precision, int nb, int split_terms, bool tournament);
+void lu_factor(beat_b200_ctx *c, int precision, int nb, int split_terms);
 void lu_solve_fp64(beat_b200_ctx *c, int R, double *x_dev);          // in place, N x R col-major
 void lu_precond_fp32(beat_b200_ctx *c, int R, const double *in, double *out);
 

@@ -43,9 +43,6 @@ template <typename T> __device__ __forceinline__ T cabs1(Cx<T> v) { return fabs(
 template <typename T> __device__ __forceinline__ Cx<T> cms(Cx<T> x, Cx<T> l, Cx<T> u) {  // x - l u
     return Cx<T>{x.re - (l.re * u.re - l.im * u.im), x.im - (l.re * u.im + l.im * u.re)};
 }
-template <typename T> __device__ __forceinline__ Cx<T> cfma(Cx<T> a, Cx<T> b, Cx<T> c) {  // c + a b
-    return Cx<T>{fma(a.re, b.re, fma(-a.im, b.im, c.re)), fma(a.re, b.im, fma(a.im, b.re, c.im))};
-}
 
 // L2-coherent loads of values other CTAs published before a grid barrier
 __device__ __forceinline__ Cx<double> ldcg(const Cx<double> *p) {
@@ -1122,391 +1119,6 @@ static bool cluster_panel(beat_b200_ctx *c, Cx<T> *A, int64_t ld, int n, int k, 
     return true;
 }
 
-// ---------------------------------------------------------------------------
-// Tournament-pivoted sub-panel (the mixed form's LU).
-//
-// The mixed form's LU is the preconditioner of an FP64 refinement, so its
-// pivots need to keep the factorisation stable, not to repeat LAPACK's.  The
-// partial-pivoting cluster kernel above exchanges candidates between its 16
-// CTAs once per pivot column (2.9 us per column at N = 10,242); tournament
-// pivoting (communication-avoiding LU: Grigori, Demmel and Xiang, SIAM J.
-// Matrix Anal. Appl. 32 (2011) 1317-1350) exchanges once per 32-column
-// sub-panel:
-//   1. every CTA factors its own rows of the sub-panel with partial pivoting
-//      (no exchange) and keeps the rows it pivoted on, at most 32;
-//   2. the candidates' row numbers go to CTA 0 (one cluster barrier);
-//   3. CTA 0 loads the candidates' original rows and factors them with
-//      partial pivoting: its pivot rows are the sub-panel's winners, and the
-//      factored winners are [L11 \ U11] of the sub-panel;
-//   4. CTA 0 writes the interchanges that bring the winners to the top (in
-//      LAPACK's ipiv form), [L11 \ U11], L11^-1 and U11^-1.
-// The kernel writes nothing else of A: laswp_range_kernel then moves the rows,
-// trsm_blocked_kernel forms U12 = L11^-1 A12 of the panel's remaining
-// columns, and calu_tail_kernel writes [L11 \ U11], L21 = A21 U11^-1 and the
-// panel's own trailing update.  Ties of |re| + |im| go to the smaller row
-// number, so the result does not depend on the scheduling.
-// ---------------------------------------------------------------------------
-constexpr int TP_W = 32;                    // sub-panel width (c64: 256-byte rows)
-constexpr int TP_CAND = CP_CTAS * TP_W;     // candidates of the final round
-constexpr int TP_SCRATCH_ROWS = 4 * TP_W;   // rows of P that CTA 0 uses for the triangles
-
-template <typename T> struct TournamentArgs {
-    const Cx<T> *A;
-    int64_t ld;
-    int n, k, rpc;  // sub-panel: rows [k, n), columns [k, k + TP_W); rows per CTA
-    int *ipiv;
-    int *status;
-    Cx<T> *lu11;    // TP_W x TP_W, row-major: [L11 \ U11]
-    Cx<T> *uinv;    // TP_W x TP_W: U11^-1 (identity past the sub-panel's width)
-    Cx<T> *dinv;    // TP_W x TP_W: L11^-1
-    uint64_t timeout_ns;
-};
-
-__device__ __forceinline__ void st_cluster_u32(uint32_t addr, uint32_t v) {
-    asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
-}
-
-// bounded wait on a CTA-local mbarrier phase; false (status bit set) on expiry
-__device__ __forceinline__ bool tp_wait(uint64_t *bar, unsigned parity, uint64_t timeout_ns, int *status) {
-    if (mb_try(bar, parity)) return true;
-    const uint64_t t0 = global_ns();
-    while (!mb_try(bar, parity))
-        if (global_ns() - t0 > timeout_ns) {
-            atomicOr(status, (int)DEV_BARRIER_TIMEOUT);
-            return false;
-        }
-    return true;
-}
-
-// One round of partial-pivoting elimination on the rows this thread owns
-// (row i = tid + r * CP_THREADS, live[r]): the CTA-wide winner of column j
-// by |re| + |im| (ties: the smaller position pos[r]), then every other live
-// row eliminated; with keep_l the multiplier stays in column j.  Returns the
-// winner's local row (-1: no live row left); red_* are the double-buffered
-// per-warp candidates, indexed by pb = j & 1.
-template <typename T>
-__device__ __forceinline__ int tp_round(Cx<T> *P, int j, bool (&live)[CP_RMAX], const int (&pos)[CP_RMAX],
-                                        bool keep_l, uint64_t (*red_m)[CP_WARPS], int (*red_pos)[CP_WARPS],
-                                        int (*red_li)[CP_WARPS], int *status, int *win_pos) {
-    constexpr int RS = CP_ROW_BYTES / sizeof(Cx<T>);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, pb = j & 1;
-    uint64_t m = 0;
-    int bp = CP_NONE, li = -1;
-#pragma unroll
-    for (int r = 0; r < CP_RMAX; ++r)
-        if (live[r]) {
-            const int i = tid + r * CP_THREADS;
-            const uint64_t mr = mag_bits(cabs1(P[(size_t)i * RS + j]));
-            if (bp == CP_NONE || mr > m || (mr == m && pos[r] < bp)) {
-                m = mr;
-                bp = pos[r];
-                li = i;
-            }
-        }
-    const int wl = warp_argbest<T>(m, bp);
-    const uint64_t wm = __shfl_sync(0xffffffffu, m, wl);
-    const int wp = __shfl_sync(0xffffffffu, bp, wl), wi = __shfl_sync(0xffffffffu, li, wl);
-    if (lane == 0) {
-        red_m[pb][warp] = wm;
-        red_pos[pb][warp] = wp;
-        red_li[pb][warp] = wi;
-    }
-    __syncthreads();
-    const uint64_t cm = lane < CP_WARPS ? red_m[pb][lane] : 0ull;
-    const int cp = lane < CP_WARPS ? red_pos[pb][lane] : CP_NONE;
-    const int bw = warp_argbest<T>(cm, cp) & (CP_WARPS - 1);
-    const int gp = __shfl_sync(0xffffffffu, cp, bw);
-    if (gp == CP_NONE) return -1;  // uniform: the same smem values in every warp
-    const int gi = red_li[pb][bw];
-    const T gm = mag_value<T>(__shfl_sync(0xffffffffu, cm, bw));
-    if (tid == 0) {
-        if (win_pos) win_pos[j] = gp;
-        if (!(gm > T(0)) && status) atomicOr(status, (int)DEV_ZERO_PIVOT);
-    }
-    const Cx<T> *prow = P + (size_t)gi * RS;
-    const Cx<T> pv = prow[j];
-    const T den = pv.re * pv.re + pv.im * pv.im;
-    const T rd = den > T(0) ? T(1) / den : T(0);
-    const Cx<T> inv{pv.re * rd, -pv.im * rd};
-#pragma unroll
-    for (int r = 0; r < CP_RMAX; ++r)
-        if (live[r] && tid + r * CP_THREADS == gi) live[r] = false;
-#pragma unroll
-    for (int r = 0; r < CP_RMAX; ++r)
-        if (live[r]) {
-            Cx<T> *row = P + (size_t)(tid + r * CP_THREADS) * RS;
-            const Cx<T> l = cmul(row[j], inv);
-            if (keep_l) row[j] = l;
-            row_update(row, prow, l, j + 1, TP_W);
-        }
-    return gi;
-}
-
-template <typename T>
-__global__ void __launch_bounds__(CP_THREADS) tournament_panel_kernel(TournamentArgs<T> a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int RS = CP_ROW_BYTES / sizeof(Cx<T>);
-    Cx<T> *P = reinterpret_cast<Cx<T> *>(smem_raw);  // max(rpc, TP_CAND + TP_SCRATCH_ROWS) rows of RS
-    __shared__ uint64_t ldbar;
-    __shared__ uint64_t red_m[2][CP_WARPS];
-    __shared__ int red_pos[2][CP_WARPS], red_li[2][CP_WARPS];
-    __shared__ int cand_pos[TP_CAND];  // CTA 0: row numbers of every CTA's candidates (slot rank * TP_W + j)
-    __shared__ int cand_cnt[CP_CTAS], cstart[CP_CTAS + 1];
-    __shared__ int sel_pos[TP_W], win_pos[TP_W], win_t[TP_W];
-    const uint32_t rank = cl_rank();
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int gr0 = a.k + (int)rank * a.rpc;
-    const int nrows = max(0, min(a.rpc, a.n - gr0));
-    const int jmax = min(TP_W, a.n - a.k);
-    const uint32_t row_bytes = (uint32_t)(TP_W * sizeof(Cx<T>));
-    if (tid == 0) {
-        mb_init(&ldbar, 1);
-        mb_init_fence();
-        mb_arrive_expect(&ldbar, (unsigned)nrows * row_bytes);
-    }
-    __syncthreads();
-    // every CTA of the cluster has started before anyone stores into CTA 0's
-    // shared memory (phase 2): arrive now, wait just before those stores
-    asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
-    for (int i = tid; i < nrows; i += CP_THREADS)
-        bulk_g2s(sm_addr(P + (size_t)i * RS), a.A + (int64_t)(gr0 + i) * a.ld + a.k, row_bytes, sm_addr(&ldbar));
-    tp_wait(&ldbar, 0u, a.timeout_ns, a.status);
-
-    // 1. local partial pivoting: this CTA's candidates
-    bool live[CP_RMAX];
-    int pos[CP_RMAX];
-#pragma unroll
-    for (int r = 0; r < CP_RMAX; ++r) {
-        const int i = tid + r * CP_THREADS;
-        live[r] = i < nrows;
-        pos[r] = gr0 + i;
-    }
-    int nsel = 0;
-    for (int j = 0; j < jmax; ++j) {
-        if (tp_round<T>(P, j, live, pos, false, red_m, red_pos, red_li, nullptr, sel_pos) < 0) break;
-        ++nsel;
-    }
-    __syncthreads();
-    asm volatile("barrier.cluster.wait.aligned;" ::: "memory");
-    // 2. candidates to CTA 0, then one cluster barrier (release / acquire)
-    if (tid < nsel) st_cluster_u32(cl_map(sm_addr(&cand_pos[rank * TP_W + tid]), 0), (uint32_t)sel_pos[tid]);
-    if (tid == 0) st_cluster_u32(cl_map(sm_addr(&cand_cnt[rank]), 0), (uint32_t)nsel);
-    cl_sync();
-    if (rank != 0) return;  // nothing reads or writes another CTA's shared memory from here on
-
-    // 3. the final round on CTA 0: the candidates' original rows
-    if (tid == 0) {
-        int sum = 0;
-        for (int q = 0; q < CP_CTAS; ++q) {
-            cstart[q] = sum;
-            sum += cand_cnt[q];
-        }
-        cstart[CP_CTAS] = sum;
-    }
-    fence_proxy_async_smem();  // the local round's generic writes of P before the bulk loads into it
-    __syncthreads();
-    const int C = cstart[CP_CTAS];
-    int myq = 0;
-    while (myq + 1 < CP_CTAS && cstart[myq + 1] <= tid) ++myq;
-    const int mypos = tid < C ? cand_pos[myq * TP_W + (tid - cstart[myq])] : CP_NONE;
-    if (tid == 0) mb_arrive_expect(&ldbar, (unsigned)C * row_bytes);
-    __syncthreads();  // the expectation precedes every completion
-    if (tid < C) bulk_g2s(sm_addr(P + (size_t)tid * RS), a.A + (int64_t)mypos * a.ld + a.k, row_bytes, sm_addr(&ldbar));
-    tp_wait(&ldbar, 1u, a.timeout_ns, a.status);
-    bool live2[CP_RMAX] = {};
-    int pos2[CP_RMAX];
-    live2[0] = tid < C;
-    pos2[0] = mypos;
-#pragma unroll
-    for (int r = 1; r < CP_RMAX; ++r) pos2[r] = CP_NONE;
-    for (int j = 0; j < jmax; ++j) {
-        const int gi = tp_round<T>(P, j, live2, pos2, true, red_m, red_pos, red_li, a.status, win_pos);
-        if (tid == 0) win_t[j] = gi;
-    }
-    __syncthreads();
-
-    // 4. outputs: [L11 \ U11], the interchanges, L11^-1 and U11^-1
-    Cx<T> *LU = P + (size_t)TP_CAND * RS;  // TP_W x (TP_W + 1) each: the triangles,
-    Cx<T> *Y = LU + TP_W * (TP_W + 1);     // the lower inverse's scratch,
-    Cx<T> *X = Y + TP_W * (TP_W + 1);      // the upper inverse
-    for (int e = tid; e < TP_W * TP_W; e += CP_THREADS) {
-        const int i = e / TP_W, c = e % TP_W;
-        Cx<T> v{T(i == c), T(0)};
-        if (i < jmax && c < jmax) v = P[(size_t)win_t[i] * RS + c];
-        LU[i * (TP_W + 1) + c] = v;
-        a.lu11[e] = v;
-    }
-    __syncthreads();
-    if (warp == 0) {
-        // interchanges (LAPACK form): winner i moves to row k + i, the row there
-        // to where the winner was.  Lane t holds one displaced row: its
-        // original number and where it sits now.
-        int orig = -1, loc = -1;
-        for (int i = 0; i < jmax; ++i) {
-            const int p = win_pos[i], target = a.k + i;
-            const unsigned hp = __ballot_sync(0xffffffffu, orig == p);
-            const int cur = hp ? __shfl_sync(0xffffffffu, loc, __ffs(hp) - 1) : p;
-            const unsigned ht = __ballot_sync(0xffffffffu, orig >= 0 && loc == target);
-            const int occ = ht ? __shfl_sync(0xffffffffu, orig, __ffs(ht) - 1) : target;
-            if (lane == 0) a.ipiv[target] = cur;
-            if (hp && lane == __ffs(hp) - 1) orig = -1;  // the winner is in place for good
-            if (cur != target) {
-                if (ht) {
-                    if (lane == __ffs(ht) - 1) loc = cur;
-                } else {
-                    const unsigned freel = __ballot_sync(0xffffffffu, orig < 0);
-                    if (lane == __ffs(freel) - 1) {
-                        orig = occ;
-                        loc = cur;
-                    }
-                }
-            } else if (ht && lane == __ffs(ht) - 1) {
-                orig = -1;
-            }
-            __syncwarp();
-        }
-        warp_unit_lower_inverse(LU, TP_W + 1, jmax, TP_W, Y, a.dinv);
-    } else if (warp == 1) {
-        // U11^-1 by back substitution, lane c computing column c (LU is the
-        // identity past jmax, so is the inverse)
-        const int c = lane;
-        for (int i = TP_W - 1; i >= 0; --i) {
-            Cx<T> s{T(i == c), T(0)};
-            for (int t = i + 1; t < TP_W; ++t) s = cms(s, LU[i * (TP_W + 1) + t], X[t * (TP_W + 1) + c]);
-            const Cx<T> d = LU[i * (TP_W + 1) + i];
-            const T den = d.re * d.re + d.im * d.im;
-            const T rd = den > T(0) ? T(1) / den : T(0);
-            X[i * (TP_W + 1) + c] = cmul(s, Cx<T>{d.re * rd, -d.im * rd});
-        }
-        for (int i = 0; i < TP_W; ++i) a.uinv[(size_t)i * TP_W + c] = X[i * (TP_W + 1) + c];
-    }
-}
-
-// The rest of a tournament-pivoted sub-panel's step, after the interchanges
-// and U12 = L11^-1 A12 (rows [k, k + TP_W) of the panel's columns right of
-// the sub-panel, [k + TP_W, pe)): rows [k, k + TP_W) of the sub-panel get
-// [L11 \ U11]; every row r below gets L21[r] = A[r, k:k+TP_W] U11^-1 and
-// A[r, k+TP_W:pe) -= L21[r] U12.  32 rows per CTA, 256 threads.
-constexpr int TT_ROWS = 32, TT_MAXC = 96;
-template <typename T>
-__global__ void __launch_bounds__(256) calu_tail_kernel(Cx<T> *A, int64_t ld, int n, int k, int pe, const Cx<T> *lu11,
-                                                       const Cx<T> *uinv) {
-    __shared__ Cx<T> Ui[TP_W][TP_W + 1];
-    __shared__ Cx<T> L[TT_ROWS][TP_W + 1];
-    __shared__ Cx<T> U12[TP_W][TT_MAXC + 1];
-    const int tid = threadIdx.x;
-    const int r0 = k + blockIdx.x * TT_ROWS;
-    const int ncols = max(0, pe - k - TP_W);
-    const int jmax = min(TP_W, n - k);
-    for (int e = tid; e < TP_W * TP_W; e += 256) Ui[e / TP_W][e % TP_W] = uinv[e];
-    for (int e = tid; e < TT_ROWS * TP_W; e += 256) {
-        const int i = e / TP_W, c = e % TP_W, r = r0 + i;
-        L[i][c] = (r < n && c < jmax) ? A[(int64_t)r * ld + k + c] : Cx<T>{T(0), T(0)};
-    }
-    __syncthreads();
-    // L21 (rows >= k + TP_W), [L11 \ U11] (rows < k + TP_W)
-    Cx<T> l21[TT_ROWS * TP_W / 256];
-#pragma unroll
-    for (int u = 0; u < TT_ROWS * TP_W / 256; ++u) {
-        const int e = tid + u * 256, i = e / TP_W, c = e % TP_W, r = r0 + i;
-        Cx<T> v{T(0), T(0)};
-        if (r >= k + TP_W) {
-            for (int t = 0; t < TP_W; ++t) v = cfma(L[i][t], Ui[t][c], v);
-        } else if (r < k + jmax) {
-            v = lu11[(r - k) * TP_W + c];
-        }
-        l21[u] = v;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < TT_ROWS * TP_W / 256; ++u) {
-        const int e = tid + u * 256, i = e / TP_W, c = e % TP_W, r = r0 + i;
-        L[i][c] = l21[u];
-        if (r < n && c < jmax && (r >= k + TP_W || r < k + jmax)) A[(int64_t)r * ld + k + c] = l21[u];
-    }
-    // the panel's own trailing update, TT_MAXC columns at a time
-    for (int cb = 0; cb < ncols; cb += TT_MAXC) {
-        const int nc = min(TT_MAXC, ncols - cb);
-        __syncthreads();  // L written (first chunk), U12 of the previous chunk read
-        for (int e = tid; e < TP_W * nc; e += 256) {
-            const int t = e / nc, c = e % nc;
-            U12[t][c] = t < jmax ? A[(int64_t)(k + t) * ld + k + TP_W + cb + c] : Cx<T>{T(0), T(0)};
-        }
-        __syncthreads();
-        for (int e = tid; e < TT_ROWS * nc; e += 256) {
-            const int i = e / nc, c = e % nc, r = r0 + i;
-            if (r < k + TP_W || r >= n) continue;
-            Cx<T> acc{T(0), T(0)};
-            for (int t = 0; t < TP_W; ++t) acc = cfma(L[i][t], U12[t][c], acc);
-            Cx<T> &d = A[(int64_t)r * ld + k + TP_W + cb + c];
-            d.re -= acc.re;
-            d.im -= acc.im;
-        }
-    }
-}
-
-// shared memory of the tournament kernel for rpc rows
-template <typename T> static size_t tournament_smem(int rpc) {
-    return (size_t)std::max(rpc, TP_CAND + TP_SCRATCH_ROWS) * CP_ROW_BYTES;
-}
-
-// Launches the tournament kernel for the sub-panel at k; false when its rows
-// do not fit the cluster's shared memory or no cluster can be scheduled.
-template <typename T>
-static bool tournament_panel(beat_b200_ctx *c, const Cx<T> *A, int64_t ld, int n, int k, int *ipiv, Cx<T> *lu11,
-                             Cx<T> *uinv, Cx<T> *dinv) {
-    static_assert(TP_W * sizeof(Cx<T>) == 256, "tournament rows are 256 bytes");
-    const int m = n - k;
-    const int rpc = (m + CP_CTAS - 1) / CP_CTAS;
-    constexpr size_t cap = 200 * 1024;  // plus about 4 KB of static shared memory
-    if (rpc > CP_RMAX * CP_THREADS || n >= (1 << 30)) return false;
-    const size_t smem = tournament_smem<T>(rpc);
-    if (smem > cap) return false;
-    static std::atomic<bool> attr_done{false};  // sweep lanes call this from several threads
-    if (!attr_done) {
-        BB_CUDA(cudaFuncSetAttribute(tournament_panel_kernel<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-        BB_CUDA(cudaFuncSetAttribute(tournament_panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)cap));
-        attr_done = true;
-    }
-    TournamentArgs<T> a;
-    a.A = A;
-    a.ld = ld;
-    a.n = n;
-    a.k = k;
-    a.rpc = rpc;
-    a.ipiv = ipiv;
-    a.status = c->status.as<int>();
-    a.lu11 = lu11;
-    a.uinv = uinv;
-    a.dinv = dinv;
-    a.timeout_ns = 100000000ull;  // 0.1 s per wait
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(CP_CTAS);
-    cfg.blockDim = dim3(CP_THREADS);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = c->stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = CP_CTAS;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    if (!c->tournament_checked) {
-        int nclusters = 0;
-        cfg.dynamicSmemBytes = cap;
-        cudaError_t e = cudaOccupancyMaxActiveClusters(&nclusters, (void *)tournament_panel_kernel<T>, &cfg);
-        cfg.dynamicSmemBytes = smem;
-        c->tournament_ok = (e == cudaSuccess && nclusters >= 1);
-        cudaGetLastError();
-        c->tournament_checked = true;
-    }
-    if (!c->tournament_ok) return false;
-    BB_CUDA(cudaLaunchKernelEx(&cfg, tournament_panel_kernel<T>, a));
-    return true;
-}
-
 // FP32 form trailing update on the tensor cores (tc_gemm.cu)
 bool tc_update_supported(int nb);
 void tc_stage_l(beat_b200_ctx *c, int k, int nb, int split_terms, cudaStream_t st);
@@ -1517,7 +1129,7 @@ void tc_update_cols(beat_b200_ctx *c, int k, int nb, int split_terms, int col_lo
 // ---------------------------------------------------------------------------
 // host driver
 // ---------------------------------------------------------------------------
-template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int split_terms, bool tournament) {
+template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int split_terms) {
     Workspace &w = c->ws;
     const int n = c->V;
     const int64_t ld = w.ld;
@@ -1536,14 +1148,11 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
     const size_t scratch = rec_bytes + sizeof(Cx<T>) * (2 * (size_t)G * nb + 2 * nb);
     const size_t dinv_off = (scratch + 255) / 256 * 256;
     const size_t dinv_bytes = sizeof(Cx<T>) * (size_t)W * W * ((n + W - 1) / W);
-    const size_t tp_bytes = sizeof(Cx<T>) * 2 * (size_t)TP_W * TP_W;  // the tournament's [L11 \ U11] and U11^-1
-    w.panel_scratch.alloc(dinv_off + dinv_bytes + tp_bytes);
+    w.panel_scratch.alloc(dinv_off + dinv_bytes);
     PivotRec *recs = w.panel_scratch.as<PivotRec>();
     Cx<T> *pub_rows = reinterpret_cast<Cx<T> *>(recs + 2 * G);
     Cx<T> *pub_diag = pub_rows + 2 * (size_t)G * nb;
     Cx<T> *dinv = reinterpret_cast<Cx<T> *>(w.panel_scratch.as<unsigned char>() + dinv_off);
-    Cx<T> *tp_lu = reinterpret_cast<Cx<T> *>(w.panel_scratch.as<unsigned char>() + dinv_off + dinv_bytes);
-    Cx<T> *tp_uinv = tp_lu + (size_t)TP_W * TP_W;
     // blocked U12 solves need whole W-column sub-panels of 256-byte rows
     constexpr int WF = 256 / sizeof(Cx<T>);
     const bool blocked = W == WF && nb % W == 0;
@@ -1613,23 +1222,6 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
         for (int ks = k; ks < pe; ks += W) {
             const int m = n - ks;
             Cx<T> *dinv_s = blocked ? dinv + (size_t)(ks / W) * W * W : nullptr;
-            if constexpr (sizeof(T) == 4) {
-                if (tournament && W == TP_W && blocked &&
-                    tournament_panel<T>(c, A, ld, n, ks, ipiv, tp_lu, tp_uinv, dinv_s)) {
-                    // the sub-panel's interchanges on its whole panel (its own columns
-                    // included: the tournament kernel moves no rows), U12 of the panel's
-                    // remaining columns, then [L11 \ U11], L21 and the panel's own update
-                    laswp_range_kernel<T><<<(pe - k + 1 + 255) / 256, 256, 0, s0>>>(A, ld, n, ks, W, ipiv, k, pe,
-                                                                                    0, 0, nullptr);
-                    if (ks + W < pe)
-                        trsm_blocked_kernel<T, WF><<<(pe - ks - W + TB_COLS - 1) / TB_COLS, 256, tb_smem, s0>>>(
-                            A, ld, ks, 1, dinv_s, ks + W, pe);
-                    calu_tail_kernel<T><<<(n - ks + TT_ROWS - 1) / TT_ROWS, 256, 0, s0>>>(A, ld, n, ks, pe, tp_lu,
-                                                                                          tp_uinv);
-                    BB_CUDA(cudaGetLastError());
-                    continue;
-                }
-            }
             const bool on_cluster = cluster_panel<T>(c, A, ld, n, ks, W, ipiv, dinv_s);
             if (!on_cluster) {
                 // grid-wide panel kernel on the sub-panel
@@ -2138,12 +1730,12 @@ template <typename T> static void lu_solve_t(beat_b200_ctx *c, int R, const doub
     BB_CUDA(cudaGetLastError());
 }
 
-void lu_factor(beat_b200_ctx *c, int precision, int nb, int split_terms, bool tournament) {
+void lu_factor(beat_b200_ctx *c, int precision, int nb, int split_terms) {
     if (precision == BEAT_B200_FP64) {
-        lu_factor_t<double>(c, nb, split_terms, false);
+        lu_factor_t<double>(c, nb, split_terms);
         diag_inverses<double>(c);
     } else {
-        lu_factor_t<float>(c, nb, split_terms, tournament);
+        lu_factor_t<float>(c, nb, split_terms);
         diag_inverses<float>(c);
     }
 }

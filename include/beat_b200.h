@@ -94,13 +94,6 @@ typedef struct {
  * reported, never raised) and diag.precision reports BEAT_B200_FP64 with
  * diag.ir_converged = 0 and the failed refinement's iterations and residual. */
 #define BEAT_B200_FLAG_NO_FALLBACK 8
-/* opts.flags: the mixed form's FP32 LU pivots as LAPACK does (partial
- * pivoting, one cluster-wide pivot search per column) instead of by
- * tournament (each 32-column sub-panel's pivots chosen among every CTA's
- * local pivot rows, one exchange per sub-panel).  Both are stable; the FP64
- * refinement makes the answer the same to its tolerance.  The FP64 form
- * always pivots partially. */
-#define BEAT_B200_FLAG_PARTIAL_PIVOT 16
 
 /* Test hook (environment, read at every device allocation):
  * BEAT_B200_FAULT_OOM_BYTES=n makes each allocation of n bytes or more fail
