@@ -82,8 +82,15 @@ def tune(ctx, k_signed, eta, q, precision: int = _lib.MIXED_FP32_IR, cache: str 
     lu = {}
     for nb in blocks:
         opts = _lib.Context.opts(precision, lu_block=nb)
-        ctx.solve(k_signed, eta, q, opts)  # warm: workspace, first-launch costs
+        try:
+            ctx.solve(k_signed, eta, q, opts)  # warm: workspace, first-launch costs
+        except _lib.BeatB200Error as e:
+            if e.status != _lib.INVALID_ARG:  # a width this size cannot take (its panel outgrows shared memory)
+                raise
+            continue
         lu[nb] = min(ctx.solve(k_signed, eta, q, opts)[1]["lu_ms"] for _ in range(2))
+    if not lu:
+        raise ValueError(f"no panel width of {tuple(blocks)} fits this system")
     best_nb = min(lu, key=lu.get)
     fps = {}
     for L in lanes:

@@ -19,7 +19,9 @@ class FakeContext:
 
     def solve(self, k, eta, q, opts):
         self.calls += 1
-        return None, {"lu_ms": {64: 3.0, 128: 2.0, 256: 2.5}[opts.lu_block]}
+        if opts.lu_block == 256:  # a width the library refuses for this size
+            raise _lib.BeatB200Error(_lib.INVALID_ARG, "panel outgrows shared memory")
+        return None, {"lu_ms": {64: 3.0, 128: 2.0}[opts.lu_block]}
 
     def sweep(self, ks, etas, qs, opts):
         self.calls += 1
