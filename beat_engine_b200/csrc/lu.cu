@@ -1484,6 +1484,8 @@ __global__ void __launch_bounds__(SubstTile<T>::THREADS, 1) block_subst_kernel(c
     Cx<C> *base = reinterpret_cast<Cx<C> *>(smem_raw);
     __shared__ int s_blk;
     const int nblk = (n + SB - 1) / SB;
+    // persistent: a CTA claims the next block when it has released its last one
+    for (;;) {
     if (threadIdx.x == 0) s_blk = atomicAdd(counter, 1);
     __syncthreads();
     const int claim = s_blk;
@@ -1683,7 +1685,14 @@ __global__ void __launch_bounds__(SubstTile<T>::THREADS, 1) block_subst_kernel(c
     // and their loads
     __syncthreads();
     if (tid == 0) asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(flags + b), "r"(epoch) : "memory");
+    }
 }
+
+#define SUBST_CTAS_CAP(c) ((c)->sm_count)
+// CTAs of a substitution launch: every block's folded-in sum must be under
+// way well before the chain reaches it, but a CTA spinning on a flag holds its
+// SM, which the other lanes of a sweep could use
+static int subst_grid(const beat_b200_ctx *c, int nblk) { return std::min(nblk, SUBST_CTAS_CAP(c)); }
 
 template <typename T> static void diag_inverses(beat_b200_ctx *c) {
     Workspace &w = c->ws;
@@ -1720,10 +1729,10 @@ template <typename T> static void lu_solve_t(beat_b200_ctx *c, int R, const doub
             const int epoch = ++w.solve_epoch;
             BB_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), c->stream));
             if (pass == 0)
-                block_subst_kernel<T, true><<<nblk, SubstTile<T>::THREADS, smem, c->stream>>>(
+                block_subst_kernel<T, true><<<subst_grid(c, nblk), SubstTile<T>::THREADS, smem, c->stream>>>(
                     A, w.ld, n, Dinv, X, R, r0, counter, flags, epoch, c->status.as<int>(), 1u << 22);
             else
-                block_subst_kernel<T, false><<<nblk, SubstTile<T>::THREADS, smem, c->stream>>>(
+                block_subst_kernel<T, false><<<subst_grid(c, nblk), SubstTile<T>::THREADS, smem, c->stream>>>(
                     A, w.ld, n, Dinv, X, R, r0, counter, flags, epoch, c->status.as<int>(), 1u << 22);
         }
     }
@@ -1775,10 +1784,10 @@ static void lu_resolve_into_t(beat_b200_ctx *c, int R, const double *b, double *
             ++epoch;
             BB_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), c->stream));
             if (pass == 0)
-                block_subst_kernel<T, true><<<nblk, SubstTile<T>::THREADS, smem, c->stream>>>(
+                block_subst_kernel<T, true><<<subst_grid(c, nblk), SubstTile<T>::THREADS, smem, c->stream>>>(
                     A, w.ld, n, Dinv, X, R, r0, counter, flags, epoch, c->status.as<int>(), 1u << 22);
             else
-                block_subst_kernel<T, false><<<nblk, SubstTile<T>::THREADS, smem, c->stream>>>(
+                block_subst_kernel<T, false><<<subst_grid(c, nblk), SubstTile<T>::THREADS, smem, c->stream>>>(
                     A, w.ld, n, Dinv, X, R, r0, counter, flags, epoch, c->status.as<int>(), 1u << 22);
         }
     }
