@@ -886,7 +886,7 @@ __global__ void __launch_bounds__(256, 2) singular_pairs_kernel(SingArgs<T> g) {
         const double rx = y[0] - x[0], ry = y[1] - x[1], rz = y[2] - x[2];
         const double r2 = rx * rx + ry * ry + rz * rz;
         if (r2 == 0.0) continue;
-        const double rad = sqrt(r2), ir = 1.0 / rad;
+        const double ir = rsqrt(r2), rad = r2 * ir;  // one reciprocal square root, no divide
         double sn_, cs_;
         sincos_cw(k * rad, &sn_, &cs_);
         const double scl = ir * (0.07957747154594767 * w);
@@ -977,7 +977,7 @@ __device__ __forceinline__ void bm_point_d(const double *x, const double *y, con
     const double rx = y[0] - x[0], ry = y[1] - x[1], rz = y[2] - x[2];
     const double r2 = rx * rx + ry * ry + rz * rz;
     if (r2 == 0.0) return;
-    const double rad = sqrt(r2), ir = 1.0 / rad;
+    const double ir = rsqrt(r2), rad = r2 * ir;
     double sn_, cs_;
     sincos_cw(k * rad, &sn_, &cs_);
     const double scl = sign * ir * (0.07957747154594767 * w);

@@ -113,9 +113,9 @@ __global__ void __launch_bounds__(FLD_THREADS) field_eval_kernel(const double *p
             double gr, gi, dr, di;  // green and double-layer factors
             if (!FAR) {
                 const double rx = sy[j][0] - x0, ry = sy[j][1] - x1, rz = sy[j][2] - x2;
-                const double rad = sqrt(rx * rx + ry * ry + rz * rz);
-                if (rad == 0.0) continue;
-                const double ir = 1.0 / rad;
+                const double r2 = rx * rx + ry * ry + rz * rz;
+                if (r2 == 0.0) continue;
+                const double ir = rsqrt(r2), rad = r2 * ir;
                 double sn_, cs_;
                 sincos_cw(k * rad, &sn_, &cs_);
                 gr = cs_ * inv4pi * ir;
@@ -288,9 +288,9 @@ __device__ __forceinline__ void grad_source(double x0, double x1, double x2, dou
                                             double n1, double n2, double w, double k, const double2 *P,
                                             const double2 *Qn, double (&acc)[RC][8]) {
     const double rx = y0 - x0, ry = y1 - x1, rz = y2 - x2;
-    const double rad = sqrt(rx * rx + ry * ry + rz * rz);
-    if (rad == 0.0) return;
-    const double ir = 1.0 / rad;
+    const double r2 = rx * rx + ry * ry + rz * rz;
+    if (r2 == 0.0) return;
+    const double ir = rsqrt(r2), rad = r2 * ir;
     const double u[3] = {rx * ir, ry * ir, rz * ir}, nn[3] = {n0, n1, n2};
     double sn_, cs_;
     sincos_cw(k * rad, &sn_, &cs_);

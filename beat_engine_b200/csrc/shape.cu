@@ -86,7 +86,7 @@ __device__ __forceinline__ void reverse_point(const double (&x)[3], const double
     const double r[3] = {y[0] - x[0], y[1] - x[1], y[2] - x[2]};
     const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
     if (r2 == 0.0) return;
-    const double R = sqrt(r2), iR = 1.0 / R;
+    const double iR = rsqrt(r2), R = r2 * iR;
     const double rh[3] = {r[0] * iR, r[1] * iR, r[2] * iR};
     double sn_, cs_;
     sincos_cw(k * R, &sn_, &cs_);
