@@ -813,8 +813,15 @@ template <typename T> struct ClusterPanelArgs {
     int *ipiv;
     int *status;
     Cx<T> *dinv;  // inverse of the unit lower w x w diagonal block (nullptr: not wanted)
+    int xc0, xc1; // the panel's columns: the interchanges go to [xc0, xc1) outside [k, k + w) as well
+                  // (xc0 == xc1: the caller swaps the other columns itself)
     uint64_t timeout_ns;
 };
+
+// values per thread that the interchange of the panel's other columns holds
+// between its read and write phases: moved rows (<= 2 w) x columns (< nb)
+template <typename T> struct CpMove { static constexpr int V = sizeof(T) == 4 ? 12 : 8; };
+constexpr int CP_MAXMOVED = 64;
 
 template <typename T>
 __global__ void __launch_bounds__(CP_THREADS) cluster_panel_kernel(ClusterPanelArgs<T> a) {
@@ -1051,11 +1058,59 @@ __global__ void __launch_bounds__(CP_THREADS) cluster_panel_kernel(ClusterPanelA
         if (i < nrows && mp[r] >= a.k && mp[r] < a.n)
             bulk_s2g(a.A + (int64_t)mp[r] * a.ld + a.k, sm_addr(P + (size_t)i * RS), row_bytes);
     }
+    // the same interchanges on the panel's other columns: every CTA reads its
+    // moved rows there before the cluster barrier and writes them at their
+    // final positions after it (a permutation: every destination is some moved
+    // row's origin, read before the barrier)
+    __shared__ int mv_src[CP_MAXMOVED], mv_dst[CP_MAXMOVED], mv_n;
+    constexpr int MV = CpMove<T>::V;
+    Cx<T> mvv[MV];
+    const int nleft = a.k - a.xc0, nother = (a.xc1 > a.xc0) ? nleft + (a.xc1 - a.k - w) : 0;
+    int nitems = 0;
+    if (nother > 0) {
+        if (tid == 0) mv_n = 0;
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < CP_RMAX; ++r) {
+            const int i = tid + r * CP_THREADS;
+            if (i < nrows && mp[r] >= a.k && mp[r] < a.n && mp[r] != gr0 + i) {
+                const int slot = atomicAdd(&mv_n, 1);
+                if (slot < CP_MAXMOVED) {
+                    mv_src[slot] = gr0 + i;
+                    mv_dst[slot] = mp[r];
+                }
+            }
+        }
+        __syncthreads();
+        nitems = min(mv_n, CP_MAXMOVED) * nother;
+        if (mv_n > CP_MAXMOVED || nitems > MV * CP_THREADS) {  // the host sizes the panel so that this cannot happen
+            if (tid == 0) atomicOr(a.status, (int)DEV_BARRIER_TIMEOUT);
+            nitems = 0;
+        }
+#pragma unroll
+        for (int u = 0; u < MV; ++u) {
+            const int it = tid + u * CP_THREADS;
+            if (it < nitems) {
+                const int row = it / nother, cc = it % nother;
+                const int col = cc < nleft ? a.xc0 + cc : a.k + w + (cc - nleft);
+                mvv[u] = a.A[(int64_t)mv_src[row] * a.ld + col];
+            }
+        }
+    }
     bulk_commit_wait_all();
     if (rank == 0 && warp == 0 && a.dinv && lane < w)  // the inverse, identity past jmax
         for (int i = 0; i < w; ++i)
             a.dinv[(size_t)i * w + lane] = i < jmax ? ublk[i * (w + 1) + lane] : Cx<T>{T(i == lane), T(0)};
-    cl_sync();  // no CTA leaves while a peer may still store into its shared memory
+    cl_sync();  // every CTA's reads are done; no CTA leaves while a peer may still store into its shared memory
+#pragma unroll
+    for (int u = 0; u < MV; ++u) {
+        const int it = tid + u * CP_THREADS;
+        if (it < nitems) {
+            const int row = it / nother, cc = it % nother;
+            const int col = cc < nleft ? a.xc0 + cc : a.k + w + (cc - nleft);
+            a.A[(int64_t)mv_dst[row] * a.ld + col] = mvv[u];
+        }
+    }
 }
 
 // shared memory of the cluster kernel for rpc rows of width w
@@ -1067,7 +1122,8 @@ template <typename T> static size_t cluster_panel_smem(int rpc, int w) {
 // Launches the cluster kernel for a sub-panel; false when the rows do not fit
 // the cluster's shared memory or no cluster of CP_CTAS can be scheduled.
 template <typename T>
-static bool cluster_panel(beat_b200_ctx *c, Cx<T> *A, int64_t ld, int n, int k, int w, int *ipiv, Cx<T> *dinv) {
+static bool cluster_panel(beat_b200_ctx *c, Cx<T> *A, int64_t ld, int n, int k, int w, int *ipiv, Cx<T> *dinv,
+                          int xc0 = 0, int xc1 = 0) {
     const int m = n - k;
     const int rpc = (m + CP_CTAS - 1) / CP_CTAS;
     constexpr size_t cap = 220 * 1024;
@@ -1092,6 +1148,8 @@ static bool cluster_panel(beat_b200_ctx *c, Cx<T> *A, int64_t ld, int n, int k, 
     a.ipiv = ipiv;
     a.status = c->status.as<int>();
     a.dinv = dinv;
+    a.xc0 = xc0;
+    a.xc1 = xc1;
     a.timeout_ns = 100000000ull;  // 0.1 s per column wait
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(CP_CTAS);
@@ -1222,7 +1280,12 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
         for (int ks = k; ks < pe; ks += W) {
             const int m = n - ks;
             Cx<T> *dinv_s = blocked ? dinv + (size_t)(ks / W) * W * W : nullptr;
-            const bool on_cluster = cluster_panel<T>(c, A, ld, n, ks, W, ipiv, dinv_s);
+            // the cluster kernel also swaps the panel's other columns when they fit its
+            // registers: moved rows (<= 2 W) x other columns (< nb) per CTA_THREADS x CpMove::V
+            const bool own_swaps = pe - k > W && 2 * W * (pe - k - W) <= CpMove<T>::V * CP_THREADS &&
+                                   2 * W <= CP_MAXMOVED;
+            const bool on_cluster =
+                cluster_panel<T>(c, A, ld, n, ks, W, ipiv, dinv_s, own_swaps ? k : 0, own_swaps ? pe : 0);
             if (!on_cluster) {
                 // grid-wide panel kernel on the sub-panel
                 int g = std::min(G, std::max(1, (m + 15) / 16));
@@ -1247,8 +1310,8 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
                 BB_CUDA(cudaLaunchCooperativeKernel((void *)panel_kernel<T>, dim3(g), dim3(PANEL_THREADS), args, ps,
                                                     s0));
             }
-            // this sub-panel's interchanges on the rest of the panel
-            if (pe - k > W) {
+            // this sub-panel's interchanges on the rest of the panel (unless the cluster kernel did them)
+            if (pe - k > W && !(on_cluster && own_swaps)) {
                 laswp_range_kernel<T><<<(pe - k + 1 + 255) / 256, 256, 0, s0>>>(A, ld, n, ks, W, ipiv, k, pe, ks,
                                                                                 ks + W, nullptr);
                 BB_CUDA(cudaGetLastError());
