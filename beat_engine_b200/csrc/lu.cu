@@ -401,9 +401,20 @@ __global__ void __launch_bounds__(32) diag_block_inverse_kernel(const Cx<T> *A, 
 // complex outputs of a W x 32 block per product; one barrier per block step
 // instead of one per row.
 constexpr int TB_COLS = 32;
+// With bhi non-null (FP32, the tensor-core path) the solved block is also
+// written in the trailing update's B-operand layout (the staging of
+// tc_gemm.cu: rows 2j and 2j + 1 of B_s hold (Ur, -Ui) and (Ui, Ur) at K = 2kk
+// for column j = c - j0 and row kk of the block, split into a TF32 high part
+// and an FP32 remainder when split == 3), so no separate staging pass rereads
+// U12.
+__device__ __forceinline__ void tf32_split(float x, float &hi, float &lo) {
+    hi = __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
+    lo = x - hi;
+}
 template <typename T, int W>
 __global__ void __launch_bounds__(256) trsm_blocked_kernel(Cx<T> *A, int64_t ld, int k, int S, const Cx<T> *D,
-                                                            int c_begin, int c_end) {
+                                                            int c_begin, int c_end, float *bhi = nullptr,
+                                                            float *blo = nullptr, int j0 = 0, int split = 3) {
     constexpr int OPT = W * TB_COLS / 256;  // outputs per thread: 4 (W = 32) or 2 (W = 16)
     constexpr int CG = TB_COLS / OPT;       // column groups
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -468,6 +479,27 @@ __global__ void __launch_bounds__(256) trsm_blocked_kernel(Cx<T> *A, int64_t ld,
     for (int i = tid; i < kb * TB_COLS; i += 256) {
         const int rr = i / TB_COLS, c = i % TB_COLS;
         if (c < nc) A[(int64_t)(k + rr) * ld + c0 + c] = X[rr * TB_COLS + c];
+    }
+    if constexpr (sizeof(T) == 4) {
+        if (bhi) {
+            // consecutive threads: consecutive K (rows kk of the block) of one B_s row
+            for (int i = tid; i < 2 * TB_COLS * kb; i += 256) {
+                const int row = i / kb, kk = i % kb, c = row >> 1;
+                if (c >= nc) continue;
+                const Cx<T> u = X[kk * TB_COLS + c];
+                const float2 v = (row & 1) ? make_float2(u.im, u.re) : make_float2(u.re, -u.im);
+                const int64_t at = (int64_t)(2 * (c0 + c - j0) + (row & 1)) * 2 * kb + 2 * kk;
+                if (split == 3) {
+                    float2 h, l;
+                    tf32_split(v.x, h.x, l.x);
+                    tf32_split(v.y, h.y, l.y);
+                    *reinterpret_cast<float2 *>(bhi + at) = h;
+                    *reinterpret_cast<float2 *>(blo + at) = l;
+                } else {
+                    *reinterpret_cast<float2 *>(bhi + at) = v;
+                }
+            }
+        }
     }
 }
 
@@ -1181,6 +1213,7 @@ static bool cluster_panel(beat_b200_ctx *c, Cx<T> *A, int64_t ld, int n, int k, 
 bool tc_update_supported(int nb);
 void tc_stage_l(beat_b200_ctx *c, int k, int nb, int split_terms, cudaStream_t st);
 void tc_stage_u(beat_b200_ctx *c, int k, int nb, int split_terms, int col_lo, int col_hi, cudaStream_t st);
+void tc_stage_u_buffers(beat_b200_ctx *c, int k, int nb, float **bhi, float **blo);
 void tc_update_cols(beat_b200_ctx *c, int k, int nb, int split_terms, int col_lo, int col_hi, cudaStream_t st,
                     int max_ctas);
 
@@ -1238,12 +1271,16 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
     // 16-CTA cluster); the grid-wide panel fallback waits for its own SMs
     const int side_cap = std::max(1, G - CP_CTAS);
     // U12 = L11^-1 A12 of panel k for the columns [c_lo, c_hi), on stream st
+    // with the tensor-core update (blocked) the same launch stages U12 as the update's B operand
+    const bool fused_stage = tc && blocked;
     auto u_solve = [&](int k, int c_lo, int c_hi, cudaStream_t st) {
         const int cols = c_hi - c_lo;
         if (cols <= 0) return;
+        float *bhi = nullptr, *blo = nullptr;
+        if (fused_stage) tc_stage_u_buffers(c, k, nb, &bhi, &blo);
         if (blocked)
             trsm_blocked_kernel<T, WF><<<(cols + TB_COLS - 1) / TB_COLS, 256, tb_smem, st>>>(
-                A, ld, k, nb / W, dinv + (size_t)(k / W) * W * W, c_lo, c_hi);
+                A, ld, k, nb / W, dinv + (size_t)(k / W) * W * W, c_lo, c_hi, bhi, blo, k + nb, split_terms);
         else
             trsm_kernel<T><<<(cols + TRSM_COLS - 1) / TRSM_COLS, 256, trsm_smem, st>>>(A, ld, n, k, nb, c_lo, c_hi);
         BB_CUDA(cudaGetLastError());
@@ -1252,7 +1289,7 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
     auto update = [&](int k, int c_lo, int c_hi, cudaStream_t st, int cap) {
         if (c_hi <= c_lo || k + nb >= n) return;
         if (tc) {
-            tc_stage_u(c, k, nb, split_terms, c_lo, c_hi, st);
+            if (!fused_stage) tc_stage_u(c, k, nb, split_terms, c_lo, c_hi, st);
             tc_update_cols(c, k, nb, split_terms, c_lo, c_hi, st, cap);
         } else {
             // one CTA per tile: capping this grid as the tensor-core one is capped

@@ -463,6 +463,14 @@ void tc_stage_u(beat_b200_ctx *c, int k, int nb, int split_terms, int col_lo, in
     BB_CUDA(cudaGetLastError());
 }
 
+// The B-operand staging of panel k (rows 2 j, 2 j + 1 for column k + nb + j, K = 2 nb):
+// the blocked U12 solve writes it directly (lu.cu).
+void tc_stage_u_buffers(beat_b200_ctx *c, int k, int nb, float **bhi, float **blo) {
+    const TcStage s = tc_stage_buffers(c, k, nb);
+    *bhi = s.bhi;
+    *blo = s.blo;
+}
+
 // A[k+nb.., col_lo..col_hi) -= L21 U12 from the staged operands, on `st`,
 // with at most max_ctas persistent CTAs (0: one per SM).
 void tc_update_cols(beat_b200_ctx *c, int k, int nb, int split_terms, int col_lo, int col_hi, cudaStream_t st,
