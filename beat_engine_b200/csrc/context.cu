@@ -739,6 +739,7 @@ void ensure_workspace(beat_b200_ctx *c, int precision, int R, int rhs_request) {
 }
 
 void release_workspace(beat_b200_ctx *c) {
+    lu_graph_release(c);
     Workspace &w = c->ws;
     for (DevBuf *b : {&w.A, &w.Aop, &w.B, &w.b, &w.x, &w.ipiv, &w.perm, &w.panel_scratch, &w.stage, &w.krylov,
                       &w.small, &w.q, &w.small_solve, &w.dinv, &w.field, &w.io, &w.qeff, &w.grad})

@@ -214,6 +214,11 @@ struct beat_b200_ctx {
     // (lower priority) while panel k + 1 is factored on `stream`
     cudaStream_t side_stream = nullptr;
     cudaEvent_t la_fork = nullptr, la_join = nullptr;
+    // the factorisation's launch sequence as a CUDA graph, replayed while its
+    // key (sizes, options and every buffer it touches) stays the same
+    cudaGraphExec_t lu_graph = nullptr;
+    uint64_t lu_graph_key[12] = {};
+    int lu_graph_state = 0;  // 0: key not seen, 1: ran once eagerly (buffers allocated), 2: graph ready, 3: capture failed
     float last_regular_ms = 0.f;
     bool cluster_checked = false;  // can a 16-CTA cluster of the panel kernel be scheduled?
     bool cluster_ok = false;
@@ -249,6 +254,7 @@ void assemble(beat_b200_ctx *c, double k, double eta, int precision, int R, cons
 
 // lu.cu
 void lu_factor(beat_b200_ctx *c, int precision, int nb, int split_terms);
+void lu_graph_release(beat_b200_ctx *c);  // drops the captured factorisation (buffers about to change)
 void lu_solve_fp64(beat_b200_ctx *c, int R, double *x_dev);          // in place, N x R col-major
 void lu_precond_fp32(beat_b200_ctx *c, int R, const double *in, double *out);
 
