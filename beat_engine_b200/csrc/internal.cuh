@@ -218,7 +218,7 @@ struct beat_b200_ctx {
     // key (sizes, options and every buffer it touches) stays the same
     cudaGraphExec_t lu_graph = nullptr;
     uint64_t lu_graph_key[12] = {};
-    int lu_graph_state = 0;  // 0: key not seen, 1: ran once eagerly (buffers allocated), 2: graph ready, 3: capture failed
+    int lu_graph_state = 0;  // 0: none, 2: graph of lu_graph_key ready, 3: that key runs eagerly
     float last_regular_ms = 0.f;
     bool cluster_checked = false;  // can a 16-CTA cluster of the panel kernel be scheduled?
     bool cluster_ok = false;

@@ -1858,51 +1858,62 @@ void lu_graph_release(beat_b200_ctx *c) {
 
 // The factorisation is about 1,300 launches on two streams whose arguments
 // depend only on the sizes, the options and the workspace's buffers.  The
-// first factorisation with a given key runs eagerly (it allocates what it
-// needs); the second captures the launches into a CUDA graph, and later ones
-// replay it.  A capture that fails leaves the eager path in place for that key.
-void lu_factor(beat_b200_ctx *c, int precision, int nb, int split_terms) {
+// first factorisation with a given key runs eagerly (allocating what it
+// needs) and is then captured, without running, into a CUDA graph that later
+// factorisations with the same key replay.  The graph keeps each kernel's
+// stream priority (the look-ahead's side stream stays below the panels').  A
+// capture that fails leaves the eager path in place for that key.
+static void lu_key(const beat_b200_ctx *c, int precision, int nb, int split_terms, uint64_t (&key)[12]) {
     const Workspace &w = c->ws;
-    const uint64_t key[12] = {(uint64_t)precision, (uint64_t)nb, (uint64_t)split_terms, (uint64_t)c->V,
-                              (uint64_t)w.ld, (uint64_t)(uintptr_t)w.A.p, (uint64_t)(uintptr_t)w.ipiv.p,
-                              (uint64_t)(uintptr_t)w.perm.p, (uint64_t)(uintptr_t)w.panel_scratch.p,
-                              (uint64_t)(uintptr_t)w.stage.p, (uint64_t)(uintptr_t)w.dinv.p,
-                              (uint64_t)(uintptr_t)c->status.p};
-    if (std::memcmp(key, c->lu_graph_key, sizeof(key)) != 0) {
-        lu_graph_release(c);
-        std::memcpy(c->lu_graph_key, key, sizeof(key));
-    }
-    if (c->lu_graph_state == 2) {
+    const uint64_t k[12] = {(uint64_t)precision, (uint64_t)nb, (uint64_t)split_terms, (uint64_t)c->V,
+                            (uint64_t)w.ld, (uint64_t)(uintptr_t)w.A.p, (uint64_t)(uintptr_t)w.ipiv.p,
+                            (uint64_t)(uintptr_t)w.perm.p, (uint64_t)(uintptr_t)w.panel_scratch.p,
+                            (uint64_t)(uintptr_t)w.stage.p, (uint64_t)(uintptr_t)w.dinv.p,
+                            (uint64_t)(uintptr_t)c->status.p};
+    std::memcpy(key, k, sizeof(k));
+}
+
+void lu_factor(beat_b200_ctx *c, int precision, int nb, int split_terms) {
+    uint64_t key[12];
+    lu_key(c, precision, nb, split_terms, key);
+    const bool same = std::memcmp(key, c->lu_graph_key, sizeof(key)) == 0;
+    if (same && c->lu_graph_state == 2) {
         BB_CUDA(cudaGraphLaunch(c->lu_graph, c->stream));
         return;
     }
-    if (c->lu_graph_state == 1) {
-        cudaGraph_t g = nullptr;
-        cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
-        if (e == cudaSuccess) {
-            try {
-                lu_factor_eager(c, precision, nb, split_terms);
-            } catch (...) {
-                cudaStreamEndCapture(c->stream, &g);
-                if (g) cudaGraphDestroy(g);
-                cudaGetLastError();
-                throw;
-            }
-            e = cudaStreamEndCapture(c->stream, &g);
-        }
-        if (e == cudaSuccess && g) e = cudaGraphInstantiate(&c->lu_graph, g, 0);
-        if (g) cudaGraphDestroy(g);
-        if (e == cudaSuccess && c->lu_graph) {
-            c->lu_graph_state = 2;
-            BB_CUDA(cudaGraphLaunch(c->lu_graph, c->stream));
-            return;
-        }
-        cudaGetLastError();  // the capture is not available: stay eager for this key
-        c->lu_graph = nullptr;
-        c->lu_graph_state = 3;
+    if (same && c->lu_graph_state == 3) {
+        lu_factor_eager(c, precision, nb, split_terms);
+        return;
     }
+    lu_graph_release(c);
     lu_factor_eager(c, precision, nb, split_terms);
-    if (c->lu_graph_state == 0) c->lu_graph_state = 1;
+    // the buffers exist now: capture the same sequence for the next time
+    lu_key(c, precision, nb, split_terms, key);
+    std::memcpy(c->lu_graph_key, key, sizeof(key));
+    c->lu_graph_state = 3;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    try {
+        lu_factor_eager(c, precision, nb, split_terms);
+    } catch (...) {
+        cudaStreamEndCapture(c->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return;  // the eager factorisation above stands; this key stays eager
+    }
+    e = cudaStreamEndCapture(c->stream, &g);
+    if (e == cudaSuccess && g) e = cudaGraphInstantiateWithFlags(&c->lu_graph, g, cudaGraphInstantiateFlagUseNodePriority);
+    if (g) cudaGraphDestroy(g);
+    if (e == cudaSuccess && c->lu_graph) {
+        c->lu_graph_state = 2;
+    } else {
+        c->lu_graph = nullptr;
+        cudaGetLastError();
+    }
 }
 
 void lu_solve_fp64(beat_b200_ctx *c, int R, double *x_dev) {
