@@ -1908,9 +1908,12 @@ void lu_factor(beat_b200_ctx *c, int precision, int nb, int split_terms) {
     e = cudaStreamEndCapture(c->stream, &g);
     if (e == cudaSuccess && g) e = cudaGraphInstantiateWithFlags(&c->lu_graph, g, cudaGraphInstantiateFlagUseNodePriority);
     if (g) cudaGraphDestroy(g);
+    // upload now, so that the first replay does not pay for it
+    if (e == cudaSuccess && c->lu_graph) e = cudaGraphUpload(c->lu_graph, c->stream);
     if (e == cudaSuccess && c->lu_graph) {
         c->lu_graph_state = 2;
     } else {
+        if (c->lu_graph) cudaGraphExecDestroy(c->lu_graph);
         c->lu_graph = nullptr;
         cudaGetLastError();
     }

@@ -416,9 +416,11 @@ def run_gpu(args):
         return float(t.item())
 
     def run_form(form, n_steps):
-        # warm-up: at least one frequency per lane, so every lane exists and
-        # holds its workspace before the timed sweep
+        # warm-up: twice at least one frequency per lane, so every lane exists,
+        # holds its workspace and has run its captured factorisation once
+        # before the timed sweep
         _, ks, qs, ps, ffs = sweep_inputs(0, max(args.warmup, 6))
+        form.sweep(ks, qs, ps, dirs, ffs)
         form.sweep(ks, qs, ps, dirs, ffs)
         fs, ks, qs, ps, ffs = sweep_inputs(args.warmup, n_steps)
         torch.cuda.synchronize()
@@ -622,7 +624,7 @@ def run_sweep_config(args):
                                        [t.data_ptr() for t in d_p], opts)
 
     stream = torch.cuda.ExternalStream(ctxs[0].stream_handle(), device=dev)
-    for _ in range(max(1, args.warmup - 2)):
+    for _ in range(max(2, args.warmup - 1)):  # every lane's factorisation captured and replayed once
         batch()
     with ClockSampler(0) as clk:
         ms, diags, _ = timed(stream, batch)
