@@ -41,6 +41,9 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
 }
 
 template <typename T> __device__ __forceinline__ T cabs1(Cx<T> v) { return fabs(v.re) + fabs(v.im); }
+// correctly rounded reciprocal (the same value as 1 / x)
+__device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
 template <typename T> __device__ __forceinline__ Cx<T> cms(Cx<T> x, Cx<T> l, Cx<T> u) {  // x - l u
     return Cx<T>{x.re - (l.re * u.re - l.im * u.im), x.im - (l.re * u.im + l.im * u.re)};
 }
@@ -504,6 +507,115 @@ __global__ void __launch_bounds__(256) trsm_blocked_kernel(Cx<T> *A, int64_t ld,
     }
 }
 
+// one complex element, global -> shared, through the asynchronous copy unit
+template <typename T> __device__ __forceinline__ void cp_async_cx(Cx<T> *smem, const Cx<T> *gmem) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+    if constexpr (sizeof(Cx<T>) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem) : "memory");
+}
+
+// The same solve for the launches on the factorisation's critical path (the
+// next panel's columns, the rest of a panel after each sub-panel).  256 / W
+// columns per CTA, one entry of a W-row block per thread, so that the columns
+// spread over 4 times more CTAs; the right-hand sides, every diagonal-block
+// inverse and every off-diagonal L block of the triangle are in flight
+// together before the first block step, so the S dependent steps wait on no
+// global load.  Two partial sums per product.  The same optional B-operand
+// staging as trsm_blocked_kernel.
+template <int W> __host__ __device__ constexpr int narrow_cols() { return 256 / W; }
+template <typename T, int W> static size_t trsm_narrow_smem(int S) {
+    const size_t NC = narrow_cols<W>();
+    return sizeof(Cx<T>) * ((size_t)S * W * NC + (size_t)S * W * (W + 1) +
+                            (size_t)W * ((size_t)W * S * (S - 1) / 2 + (S - 1)) + (size_t)W * NC);
+}
+template <typename T, int W>
+__global__ void __launch_bounds__(256) trsm_narrow_kernel(Cx<T> *A, int64_t ld, int k, int S, const Cx<T> *D,
+                                                          int c_begin, int c_end, float *bhi, float *blo, int j0,
+                                                          int split) {
+    constexpr int NC = narrow_cols<W>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int kb = S * W;
+    Cx<T> *X = reinterpret_cast<Cx<T> *>(smem_raw);  // kb x NC
+    Cx<T> *Ds = X + (size_t)kb * NC;                  // S blocks of W x (W + 1)
+    Cx<T> *Ls = Ds + (size_t)S * W * (W + 1);         // block row s >= 1: W x (s W + 1)
+    Cx<T> *Z = Ls + (size_t)W * ((size_t)W * S * (S - 1) / 2 + (S - 1));  // W x NC
+    const int tid = threadIdx.x, r = tid / NC, cc = tid % NC;
+    const int c0 = c_begin + blockIdx.x * NC;
+    const int nc = min(NC, c_end - c0);
+    for (int i = tid; i < kb * NC; i += 256) {
+        const int c = i % NC;
+        if (c < nc)
+            cp_async_cx(&X[i], &A[(int64_t)(k + i / NC) * ld + c0 + c]);
+        else
+            X[i] = Cx<T>{T(0), T(0)};
+    }
+    for (int i = tid; i < S * W * W; i += 256) {
+        const int s = i / (W * W), e = i % (W * W);
+        cp_async_cx(&Ds[(size_t)s * W * (W + 1) + (e / W) * (W + 1) + e % W], &D[i]);
+    }
+    for (int s = 1; s < S; ++s) {  // L rows [s W, s W + W) x columns [0, s W)
+        const int r0 = s * W;
+        Cx<T> *Lb = Ls + (size_t)W * ((size_t)W * s * (s - 1) / 2 + (s - 1));
+        for (int i = tid; i < W * r0; i += 256)
+            cp_async_cx(&Lb[(i / r0) * (r0 + 1) + i % r0], &A[(int64_t)(k + r0 + i / r0) * ld + k + i % r0]);
+    }
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+    for (int s = 0; s < S; ++s) {
+        const int r0 = s * W;
+        Cx<T> a0 = X[(r0 + r) * NC + cc], a1{T(0), T(0)};
+        if (s > 0) {  // A_s - L_s,<s X_<s
+            const Cx<T> *Lr = Ls + (size_t)W * ((size_t)W * s * (s - 1) / 2 + (s - 1)) + (size_t)r * (r0 + 1);
+            for (int t = 0; t < r0; t += 2) {  // r0 is a multiple of W, so even
+                a0 = cms(a0, Lr[t], X[t * NC + cc]);
+                a1 = cms(a1, Lr[t + 1], X[(t + 1) * NC + cc]);
+            }
+        }
+        Z[r * NC + cc] = Cx<T>{a0.re + a1.re, a0.im + a1.im};
+        __syncthreads();
+        const Cx<T> *Dr = Ds + (size_t)s * W * (W + 1) + (size_t)r * (W + 1);
+        Cx<T> y0{T(0), T(0)}, y1{T(0), T(0)};
+        int t = 0;
+        for (; t + 1 <= r; t += 2) {  // D_s is lower triangular
+            const Cx<T> d0 = Dr[t], d1 = Dr[t + 1], z0 = Z[t * NC + cc], z1 = Z[(t + 1) * NC + cc];
+            y0 = Cx<T>{y0.re + (d0.re * z0.re - d0.im * z0.im), y0.im + (d0.re * z0.im + d0.im * z0.re)};
+            y1 = Cx<T>{y1.re + (d1.re * z1.re - d1.im * z1.im), y1.im + (d1.re * z1.im + d1.im * z1.re)};
+        }
+        if (t == r) {
+            const Cx<T> d0 = Dr[t], z0 = Z[t * NC + cc];
+            y0 = Cx<T>{y0.re + (d0.re * z0.re - d0.im * z0.im), y0.im + (d0.re * z0.im + d0.im * z0.re)};
+        }
+        X[(r0 + r) * NC + cc] = Cx<T>{y0.re + y1.re, y0.im + y1.im};
+        __syncthreads();  // block s of X is complete; Z is free again
+    }
+    for (int i = tid; i < kb * NC; i += 256) {
+        const int c = i % NC;
+        if (c < nc) A[(int64_t)(k + i / NC) * ld + c0 + c] = X[i];
+    }
+    if constexpr (sizeof(T) == 4) {
+        if (bhi) {
+            for (int i = tid; i < 2 * NC * kb; i += 256) {
+                const int row = i / kb, kk = i % kb, c = row >> 1;
+                if (c >= nc) continue;
+                const Cx<T> u = X[kk * NC + c];
+                const float2 v = (row & 1) ? make_float2(u.im, u.re) : make_float2(u.re, -u.im);
+                const int64_t at = (int64_t)(2 * (c0 + c - j0) + (row & 1)) * 2 * kb + 2 * kk;
+                if (split == 3) {
+                    float2 h, l;
+                    tf32_split(v.x, h.x, l.x);
+                    tf32_split(v.y, h.y, l.y);
+                    *reinterpret_cast<float2 *>(bhi + at) = h;
+                    *reinterpret_cast<float2 *>(blo + at) = l;
+                } else {
+                    *reinterpret_cast<float2 *>(bhi + at) = v;
+                }
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // SIMT complex GEMM for the trailing update: C[m0.., n0..] -= L U
 // L = A[r, k:k+kk], U = A[k:k+kk, c]; 64 x 64 output tile, 256 threads,
@@ -683,6 +795,78 @@ static void launch_update(cudaStream_t st, dim3 grid, Cx<T> *A, int64_t ld, int 
 }
 
 // ---------------------------------------------------------------------------
+// FP32 update inside a panel, after each of its sub-panels: C[row0.., col0 ..
+// col_end) -= L U with L = A[r, k:k+kk], U = A[k:k+kk, c], kk <= 32.  The
+// update is 32, 64 or 96 columns wide, so the tiles are 128 x 32 complex: the
+// whole K is staged at once by the asynchronous copy unit while each thread
+// prefetches its 4 x 4 outputs, then one barrier and kk rank-1 steps from
+// shared memory.  (The square 64 x 64 tiles of gemm_update_kernel left half of
+// each tile idle on the 32-column updates and staged K in two synchronised
+// chunks.)  C never overlaps L or U: rows >= row0 > k + kk, columns >= col0.
+// ---------------------------------------------------------------------------
+constexpr int PU_ROWS = 128, PU_COLS = 32, PU_K = 32;
+__global__ void __launch_bounds__(256, 2) panel_update_kernel(Cx<float> *A, int64_t ld, int n, int k, int kk, int row0,
+                                                             int col0, int col_end) {
+    __shared__ __align__(16) Cx<float> sL[PU_ROWS][PU_K + 1];
+    __shared__ __align__(16) Cx<float> sU[PU_K][PU_COLS];
+    const int tid = threadIdx.x, tx = tid % 8, ty = tid / 8;  // outputs: rows ty + 32 i, columns tx + 8 j
+    const int r0 = row0 + blockIdx.y * PU_ROWS, c0 = col0 + blockIdx.x * PU_COLS;
+    for (int i = tid; i < PU_ROWS * PU_K; i += 256) {
+        const int rr = i / PU_K, q = i % PU_K, r = r0 + rr;
+        if (r < n && q < kk)
+            cp_async_cx(&sL[rr][q], &A[(int64_t)r * ld + k + q]);
+        else
+            sL[rr][q] = Cx<float>{0.f, 0.f};
+    }
+    for (int i = tid; i < PU_K * PU_COLS; i += 256) {
+        const int q = i / PU_COLS, cc = i % PU_COLS, c = c0 + cc;
+        if (c < col_end && q < kk)
+            cp_async_cx(&sU[q][cc], &A[(int64_t)(k + q) * ld + c]);
+        else
+            sU[q][cc] = Cx<float>{0.f, 0.f};
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    Cx<float> cur[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int r = r0 + ty + 32 * i, c = c0 + tx + 8 * j;
+            cur[i][j] = (r < n && c < col_end) ? A[(int64_t)r * ld + c] : Cx<float>{0.f, 0.f};
+        }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+    float acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.f;
+#pragma unroll 4
+    for (int q = 0; q < PU_K; ++q) {
+        Cx<float> a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = sL[ty + 32 * i][q];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = sU[q][tx + 8 * j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                acc[i][j][0] += a[i].re * b[j].re - a[i].im * b[j].im;
+                acc[i][j][1] += a[i].re * b[j].im + a[i].im * b[j].re;
+            }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int r = r0 + ty + 32 * i, c = c0 + tx + 8 * j;
+            if (r < n && c < col_end)
+                A[(int64_t)r * ld + c] = Cx<float>{cur[i][j].re - acc[i][j][0], cur[i][j].im - acc[i][j][1]};
+        }
+}
+
+// ---------------------------------------------------------------------------
 // Sub-panel factorisation on one thread-block cluster.  CP_CTAS CTAs hold all
 // rows of a w-column sub-panel (256-byte rows) in shared memory; rows never
 // move: each row carries its logical position, and an interchange only swaps
@@ -743,15 +927,16 @@ __device__ __forceinline__ void mb_arrive_expect(uint64_t *b, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sm_addr(b)), "r"(bytes) : "memory");
 }
 // true once the phase of the given parity completed (the thread may be
-// suspended up to about a microsecond inside)
+// suspended inside until the phase completes or a time limit of the system
+// passes; with a suspend-time hint of 1 us the panels measured 3 % slower)
 __device__ __forceinline__ bool mb_try(uint64_t *b, unsigned parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(sm_addr(b)), "r"(parity), "r"(1000u)
+        : "r"(sm_addr(b)), "r"(parity)
         : "memory");
     return ok != 0;
 }
@@ -796,6 +981,8 @@ template <typename T> __device__ __forceinline__ int warp_argbest(uint64_t m, in
         const uint32_t mm = __reduce_max_sync(0xffffffffu, (uint32_t)m);
         tie = (uint32_t)m == mm;
     }
+    const unsigned ties = __ballot_sync(0xffffffffu, tie);
+    if (__popc(ties) == 1) return __ffs(ties) - 1;  // one largest magnitude: no position to compare
     const int mpos = __reduce_min_sync(0xffffffffu, tie ? pos : CP_NONE);
     return __ffs(__ballot_sync(0xffffffffu, tie && pos == mpos)) - 1;
 }
@@ -1009,7 +1196,7 @@ __global__ void __launch_bounds__(CP_THREADS) cluster_panel_kernel(ClusterPanelA
         }
         const Cx<T> pv = prow[j];
         const T den = pv.re * pv.re + pv.im * pv.im;
-        const T rd = den > T(0) ? T(1) / den : T(0);
+        const T rd = den > T(0) ? rcp_rn(den) : T(0);
         const Cx<T> inv{pv.re * rd, -pv.im * rd};
         // interchange of positions jr and p; the pivot row retires at jr
 #pragma unroll
@@ -1252,6 +1439,12 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
     if (blocked)
         BB_CUDA(cudaFuncSetAttribute(trsm_blocked_kernel<T, WF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)tb_smem));
+    // the critical-path solves take the narrow kernel when its whole triangle fits
+    constexpr int NC = narrow_cols<WF>();
+    const bool narrow = blocked && trsm_narrow_smem<T, WF>(nb / W) <= 227 * 1024;
+    if (narrow)
+        BB_CUDA(cudaFuncSetAttribute(trsm_narrow_kernel<T, WF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)trsm_narrow_smem<T, WF>(nb / W)));
     c->barrier.alloc(sizeof(unsigned) * 4096);
     BB_CUDA(cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
     // the unblocked U12 solve (used only when the blocked one does not apply)
@@ -1268,18 +1461,25 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
     int *perm = w.perm.as<int>();
     cudaStream_t s0 = c->stream, s1 = c->side_stream;
     const bool tc = sizeof(T) == 4 && tc_update_supported(nb);
-    // SMs the look-ahead update leaves to the panel factorisation beside it (one
-    // 16-CTA cluster); the grid-wide panel fallback waits for its own SMs
-    const int side_cap = std::max(1, G - CP_CTAS);
+    // SMs the look-ahead update leaves to the panel factorisation beside it: one
+    // 16-CTA cluster, and as many again for the panel's own updates and solves
+    // between its sub-panels (measured at N = 10,242: mixed LU 46.4 ms with one
+    // cluster's SMs left, 44.5 with two, 44.0 with three, where the sweep slows);
+    // the grid-wide panel fallback waits for its own SMs
+    const int side_cap = std::max(1, G - 2 * CP_CTAS);
     // U12 = L11^-1 A12 of panel k for the columns [c_lo, c_hi), on stream st
     // with the tensor-core update (blocked) the same launch stages U12 as the update's B operand
     const bool fused_stage = tc && blocked;
-    auto u_solve = [&](int k, int c_lo, int c_hi, cudaStream_t st) {
+    // (crit: the next panel's columns, on the critical path)
+    auto u_solve = [&](int k, int c_lo, int c_hi, cudaStream_t st, bool crit) {
         const int cols = c_hi - c_lo;
         if (cols <= 0) return;
         float *bhi = nullptr, *blo = nullptr;
         if (fused_stage) tc_stage_u_buffers(c, k, nb, &bhi, &blo);
-        if (blocked)
+        if (crit && narrow)
+            trsm_narrow_kernel<T, WF><<<(cols + NC - 1) / NC, 256, trsm_narrow_smem<T, WF>(nb / W), st>>>(
+                A, ld, k, nb / W, dinv + (size_t)(k / W) * W * W, c_lo, c_hi, bhi, blo, k + nb, split_terms);
+        else if (blocked)
             trsm_blocked_kernel<T, WF><<<(cols + TB_COLS - 1) / TB_COLS, 256, tb_smem, st>>>(
                 A, ld, k, nb / W, dinv + (size_t)(k / W) * W * W, c_lo, c_hi, bhi, blo, k + nb, split_terms);
         else
@@ -1361,14 +1561,22 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
             if (ks + W < pe) {
                 // rest of this panel: U row block, then the panel's own trailing update
                 const int cols = pe - ks - W;
-                if (blocked)
+                if (narrow)
+                    trsm_narrow_kernel<T, WF><<<(cols + NC - 1) / NC, 256, trsm_narrow_smem<T, WF>(1), s0>>>(
+                        A, ld, ks, 1, dinv + (size_t)(ks / W) * W * W, ks + W, pe, nullptr, nullptr, 0, split_terms);
+                else if (blocked)
                     trsm_blocked_kernel<T, WF><<<(cols + TB_COLS - 1) / TB_COLS, 256, tb_smem, s0>>>(
                         A, ld, ks, 1, dinv + (size_t)(ks / W) * W * W, ks + W, pe);
                 else
                     trsm_kernel<T><<<(cols + TRSM_COLS - 1) / TRSM_COLS, 256, trsm_w_smem, s0>>>(
                         A, ld, n, ks, W, ks + W, pe);
-                dim3 grid((cols + GT - 1) / GT, (n - ks - W + GT - 1) / GT);
-                launch_update<T>(s0, grid, A, ld, n, ks, W, ks + W, ks + W, pe);
+                if constexpr (sizeof(T) == 4) {
+                    dim3 grid((cols + PU_COLS - 1) / PU_COLS, (n - ks - W + PU_ROWS - 1) / PU_ROWS);
+                    panel_update_kernel<<<grid, 256, 0, s0>>>(A, ld, n, ks, W, ks + W, ks + W, pe);
+                } else {
+                    dim3 grid((cols + GT - 1) / GT, (n - ks - W + GT - 1) / GT);
+                    launch_update<T>(s0, grid, A, ld, n, ks, W, ks + W, ks + W, pe);
+                }
                 BB_CUDA(cudaGetLastError());
             }
         }
@@ -1382,12 +1590,12 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
         if (pe >= n) break;
         const int ne = std::min(pe + nb, n);  // end of the next panel
         if (tc) tc_stage_l(c, k, nb, split_terms, s0);
-        u_solve(k, pe, ne, s0);
+        u_solve(k, pe, ne, s0, true);
         update(k, pe, ne, s0, 0);
         if (ne < n) {
             BB_CUDA(cudaEventRecord(c->la_fork, s0));
             BB_CUDA(cudaStreamWaitEvent(s1, c->la_fork, 0));
-            u_solve(k, ne, n, s1);
+            u_solve(k, ne, n, s1, false);
             update(k, ne, n, s1, side_cap);
             BB_CUDA(cudaEventRecord(c->la_join, s1));
             side_pending = true;
