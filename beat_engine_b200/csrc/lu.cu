@@ -316,6 +316,96 @@ __global__ void laswp_range_kernel(Cx<T> *A, int64_t ld, int n, int k, int nsw, 
     }
 }
 
+// The same interchanges as laswp_range_kernel (nsw <= LS_MAX), as one
+// permutation of at most 2 nsw rows: every CTA derives the moves from ipiv,
+// then loads every moved entry of its LS_COLS columns before it stores any, so
+// no column walks a chain of dependent global loads.  With swap j exchanging
+// positions k + j and p_j >= k + j, position k + j is final after swap j; its
+// content then is what stood at p_j just before, and
+//   X_j (the content of k + j just before swap j) = X_prevX[j], or the row k + j
+//       itself when no earlier swap's far end was k + j;
+//   V_j (the content of p_j just before swap j) = X_j when p_j = k + j, else
+//       X_lastP[j] for the last earlier swap with the same far end, else p_j.
+// Final contents: k + j <- V_j; a far end q >= k + nsw <- X_j of the last swap
+// that names it.  X is a root search over prevX (pointer jumping).
+constexpr int LS_MAX = 256;
+template <typename T> __host__ __device__ constexpr int ls_cols() { return sizeof(T) == 4 ? 32 : 16; }
+template <typename T> static size_t laswp_panel_smem(int nsw) {
+    return sizeof(Cx<T>) * 2 * (size_t)nsw * ls_cols<T>();
+}
+template <typename T>
+__global__ void __launch_bounds__(256) laswp_panel_kernel(Cx<T> *A, int64_t ld, int n, int k, int nsw, const int *ipiv,
+                                                          int c_lo, int c_hi, int x_lo, int x_hi, int *perm) {
+    constexpr int LC = ls_cols<T>();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cx<T> *vals = reinterpret_cast<Cx<T> *>(smem_raw);  // [moves][LC]
+    __shared__ int sp[LS_MAX], root[2][LS_MAX], xs[LS_MAX], msrc[2 * LS_MAX], mdst[2 * LS_MAX], pv[2 * LS_MAX];
+    __shared__ int nmove;
+    const int tid = threadIdx.x;
+    const int jmax = min(min(nsw, n - k), LS_MAX);
+    if (tid == 0) nmove = 0;
+    for (int j = tid; j < jmax; j += 256) {
+        const int p = ipiv[k + j];
+        sp[j] = (p > k + j && p < n) ? p : k + j;  // out-of-range entries are no interchange, as in laswp_range_kernel
+    }
+    __syncthreads();
+    int prev_x = -1, last_p = -1;
+    bool has_next = false;
+    const int j = tid;
+    if (j < jmax) {
+        const int pj = sp[j];
+        for (int i = 0; i < jmax; ++i) {
+            const int pi = sp[i];
+            if (i < j) {
+                if (pi == k + j) prev_x = i;
+                if (pi == pj && pj != k + j) last_p = i;
+            } else if (i > j && pi == pj) {
+                has_next = true;
+            }
+        }
+        root[0][j] = prev_x < 0 ? j : prev_x;
+    }
+    __syncthreads();
+    int b = 0;
+    for (int step = 1; step < LS_MAX; step *= 2) {  // log2(LS_MAX) rounds
+        if (j < jmax) root[b ^ 1][j] = root[b][root[b][j]];
+        b ^= 1;
+        __syncthreads();
+    }
+    if (j < jmax) xs[j] = k + root[b][j];
+    __syncthreads();
+    if (j < jmax) {
+        const int pj = sp[j], xj = xs[j];
+        const int vj = pj == k + j ? xj : (last_p >= 0 ? xs[last_p] : pj);
+        if (vj != k + j) {
+            const int m = atomicAdd(&nmove, 1);
+            msrc[m] = vj;
+            mdst[m] = k + j;
+        }
+        if (pj >= k + jmax && !has_next) {
+            const int m = atomicAdd(&nmove, 1);
+            msrc[m] = xj;
+            mdst[m] = pj;
+        }
+    }
+    __syncthreads();
+    const int nm = nmove;
+    const int cbase = c_lo + (int)blockIdx.x * LC;
+    for (int i = tid; i < nm * LC; i += 256) {
+        const int c = cbase + i % LC;
+        if (c < c_hi && (c < x_lo || c >= x_hi)) vals[i] = A[(int64_t)msrc[i / LC] * ld + c];
+    }
+    if (perm && blockIdx.x == 0)
+        for (int m = tid; m < nm; m += 256) pv[m] = perm[msrc[m]];
+    __syncthreads();
+    for (int i = tid; i < nm * LC; i += 256) {
+        const int c = cbase + i % LC;
+        if (c < c_hi && (c < x_lo || c >= x_hi)) A[(int64_t)mdst[i / LC] * ld + c] = vals[i];
+    }
+    if (perm && blockIdx.x == 0)
+        for (int m = tid; m < nm; m += 256) perm[mdst[m]] = pv[m];
+}
+
 __global__ void iota_kernel(int *perm, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) perm[i] = i;
@@ -1454,6 +1544,9 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
                    "LU: lu_block " + std::to_string(nb) + " is too wide for the unblocked U12 solve");
         BB_CUDA(cudaFuncSetAttribute(trsm_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
     }
+    constexpr int LC = ls_cols<T>();
+    BB_CUDA(cudaFuncSetAttribute(laswp_panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)laswp_panel_smem<T>(std::min(nb, LS_MAX))));
     iota_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(w.perm.as<int>(), n);
     BB_CUDA(cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream));
     const size_t trsm_w_smem = sizeof(Cx<T>) * ((size_t)W * W + (size_t)W * TRSM_COLS);
@@ -1550,8 +1643,12 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
             }
             // this sub-panel's interchanges on the rest of the panel (unless the cluster kernel did them)
             if (pe - k > W && !(on_cluster && own_swaps)) {
-                laswp_range_kernel<T><<<(pe - k + 1 + 255) / 256, 256, 0, s0>>>(A, ld, n, ks, W, ipiv, k, pe, ks,
-                                                                                ks + W, nullptr);
+                if (W <= LS_MAX)
+                    laswp_panel_kernel<T><<<(pe - k + LC - 1) / LC, 256, laswp_panel_smem<T>(W), s0>>>(
+                        A, ld, n, ks, W, ipiv, k, pe, ks, ks + W, nullptr);
+                else
+                    laswp_range_kernel<T><<<(pe - k + 1 + 255) / 256, 256, 0, s0>>>(A, ld, n, ks, W, ipiv, k, pe, ks,
+                                                                                    ks + W, nullptr);
                 BB_CUDA(cudaGetLastError());
             }
             if (blocked && !on_cluster) {
@@ -1585,7 +1682,11 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
             side_pending = false;
         }
         // the panel's interchanges on every column outside it, and on perm
-        laswp_range_kernel<T><<<(n + 1 + 255) / 256, 256, 0, s0>>>(A, ld, n, k, pe - k, ipiv, 0, n, k, pe, perm);
+        if (pe - k <= LS_MAX)
+            laswp_panel_kernel<T><<<(n + LC - 1) / LC, 256, laswp_panel_smem<T>(pe - k), s0>>>(A, ld, n, k, pe - k, ipiv,
+                                                                                            0, n, k, pe, perm);
+        else
+            laswp_range_kernel<T><<<(n + 1 + 255) / 256, 256, 0, s0>>>(A, ld, n, k, pe - k, ipiv, 0, n, k, pe, perm);
         BB_CUDA(cudaGetLastError());
         if (pe >= n) break;
         const int ne = std::min(pe + nb, n);  // end of the next panel
