@@ -1690,8 +1690,16 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
         BB_CUDA(cudaGetLastError());
         if (pe >= n) break;
         const int ne = std::min(pe + nb, n);  // end of the next panel
-        if (tc) tc_stage_l(c, k, nb, split_terms, s0);
+        if (tc) {
+            // L21's staging reads rows >= pe, the U12 solve writes rows < pe: the staging runs on
+            // the side stream (idle since the join) beside the solve
+            BB_CUDA(cudaEventRecord(c->la_fork, s0));
+            BB_CUDA(cudaStreamWaitEvent(s1, c->la_fork, 0));
+            tc_stage_l(c, k, nb, split_terms, s1);
+            BB_CUDA(cudaEventRecord(c->la_join, s1));
+        }
         u_solve(k, pe, ne, s0, true);
+        if (tc) BB_CUDA(cudaStreamWaitEvent(s0, c->la_join, 0));
         update(k, pe, ne, s0, 0);
         if (ne < n) {
             BB_CUDA(cudaEventRecord(c->la_fork, s0));
