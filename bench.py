@@ -283,8 +283,9 @@ def config_dict(args, mesh):
                               "the FP64 form timed beside it", "lu_split_terms": args.split,
             "l2": "inputs larger than L2: every step rewrites A (N^2 complex) and the N x F RHS operator",
             "parallelism": f"frequency replicas x{args.gpus} (no collective); "
-                           "up to 6 solve lanes per GPU, 4 in the FP64 form (pipelined frequency sweep, "
-                           "each lane takes the next frequency when it finishes one)"}
+                           + ("up to 6 solve lanes per GPU, 4 in the FP64 form" if args.lanes == 0
+                              else f"{args.lanes} solve lane(s) per GPU")
+                           + " (pipelined frequency sweep, each lane takes the next frequency when it finishes one)"}
 
 
 # --------------------------------------------------------------------------
@@ -308,13 +309,13 @@ class Form:
     """One precision form on its own context: the sweep lanes of each form
     stay allocated, so neither form's timed sweep pays for the other's."""
 
-    def __init__(self, lib, mesh, device, precision, split):
+    def __init__(self, lib, mesh, device, precision, split, lanes=0):
         import torch
         self.lib = lib
         self.precision = precision
         self.ctx = lib.Context(device)
         self.ctx.set_mesh(mesh.vertices, mesh.faces, 4, 4)
-        self.opts = lib.Context.opts(precision, lu_split_terms=split)
+        self.opts = lib.Context.opts(precision, lu_split_terms=split, sweep_lanes=lanes)
         self.stream = torch.cuda.ExternalStream(self.ctx.stream_handle(), device=torch.device("cuda", device))
 
     def sweep(self, ks, qs, ps, dirs, ffs):
@@ -444,7 +445,7 @@ def run_gpu(args):
         ms, _, _ = timed(form.stream, lambda: form.ctx.sweep(ks, 1.0 / ks, qh, form.opts, dirs))
         return max_over_ranks(ms)
 
-    mixed = Form(_lib, mesh, local, _lib.MIXED_FP32_IR, args.split)
+    mixed = Form(_lib, mesh, local, _lib.MIXED_FP32_IR, args.split, args.lanes)
     ms, sweep_diags, clocks, fs, ps_mixed, ff_mixed = run_form(mixed, K)
     value = world * K / (ms / 1e3)
     e2e_ms = run_e2e(mixed, K)
@@ -452,7 +453,7 @@ def run_gpu(args):
 
     fp64 = None
     if not args.no_fp64:
-        fp64 = Form(_lib, mesh, local, _lib.FP64, args.split)
+        fp64 = Form(_lib, mesh, local, _lib.FP64, args.split, args.lanes)
         ms64, diags64, clocks64, fs64, ps_64, ff_64 = run_form(fp64, K)
         fp64_value = world * K / (ms64 / 1e3)
         fp64_e2e = world * K / (run_e2e(fp64, K) / 1e3)
@@ -748,6 +749,9 @@ def main():
     ap.add_argument("--config", choices=("headline", "sweep"), default="headline",
                     help="sweep: the batched 6-enclosure x 64-frequency sweep against the FP64 loop")
     ap.add_argument("--tune-cache", default=None, help="autotuner JSON cache (default ~/.cache/beat_b200)")
+    ap.add_argument("--lanes", type=int, default=0,
+                    help="frequencies in flight in the sweep (0: the library's default); 1 runs them one after "
+                         "another on one host thread, as a profiler capture wants")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         ap.error("--warmup must be >= 3")
