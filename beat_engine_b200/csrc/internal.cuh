@@ -1,6 +1,7 @@
 // internal.cuh -- shared declarations of libbeatb200 (not part of the ABI).
 #pragma once
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -65,6 +66,26 @@ template <typename T> __host__ __device__ __forceinline__ Cx<T> cmul(Cx<T> a, Cx
 }
 
 #ifdef __CUDACC__
+// Operand staging of the FP32 LU's tensor-core update (tc_gemm.cu): L is
+// staged times 2^L_SHIFT, a complex column of U times 2^s with s =
+// stage_exp(its largest |re| or |im|), each value as an FP16 high part and the
+// FP16 rounding of the remainder.
+constexpr int L_SHIFT = 12;
+constexpr int B_SCALE_EXP = 14;
+// s with m 2^s in [2^13, 2^14) for a normal m > 0 (m = f 2^e, f in [0.5, 1):
+// s = 14 - e), clamped to [-100, 100]; 0 for m = 0
+__device__ __forceinline__ int stage_exp(float m) {
+    const unsigned bits = __float_as_uint(m);
+    if (!(m > 0.f)) return 0;
+    const int e = (int)((bits >> 23) & 0xffu) - 126;
+    return max(-100, min(100, B_SCALE_EXP - e));
+}
+__device__ __forceinline__ float pow2f(int s) { return __int_as_float((127 + s) << 23); }  // |s| <= 126
+// x as an FP16 high part and the FP16 rounding of x - high (exact in FP32)
+__device__ __forceinline__ void split_f16(float x, __half &hi, __half &lo) {
+    hi = __float2half_rn(x);
+    lo = __float2half_rn(x - __half2float(hi));
+}
 // Cooperative copy of `total` items by NT threads, BATCH loads in flight per
 // thread before any store: load(i) returns item i, store(i, v) writes it.
 // (A plain `for (i = tid; ...) dst = src` loop waits for each load before the

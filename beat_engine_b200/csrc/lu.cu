@@ -21,7 +21,7 @@
 //      the running row permutation).
 //   3. trsm_kernel: U12 = L11^-1 A12.
 //   4. trailing update A22 -= L21 U12: SIMT complex GEMM here (FP64 form),
-//      tcgen05 TF32 tensor-core GEMM for the FP32 form (tc_gemm.cu).
+//      tcgen05 FP16-split tensor-core GEMM for the FP32 form (tc_gemm.cu).
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -497,18 +497,50 @@ __global__ void __launch_bounds__(32) diag_block_inverse_kernel(const Cx<T> *A, 
 constexpr int TB_COLS = 32;
 // With bhi non-null (FP32, the tensor-core path) the solved block is also
 // written in the trailing update's B-operand layout (the staging of
-// tc_gemm.cu: rows 2j and 2j + 1 of B_s hold (Ur, -Ui) and (Ui, Ur) at K = 2kk
-// for column j = c - j0 and row kk of the block, split into a TF32 high part
-// and an FP32 remainder when split == 3), so no separate staging pass rereads
-// U12.
-__device__ __forceinline__ void tf32_split(float x, float &hi, float &lo) {
-    hi = __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
-    lo = x - hi;
+// tc_gemm.cu: rows 2j and 2j + 1 of B_s hold (Ur, -Ui) 2^s and (Ui, Ur) 2^s at
+// K = 2kk for column j = c - j0 and row kk of the block, s from the column's
+// largest |re| or |im|, as FP16 high parts and, when split == 3, FP16
+// remainders; bscale[j] = 2^-(s + L_SHIFT)), so no separate staging pass
+// rereads U12.  stage_u_block does it for a block of COLS columns in shared
+// memory (X[row * COLS + column]); all 256 threads of the CTA call it.
+template <int COLS>
+__device__ void stage_u_block(const Cx<float> *X, int kb, int nc, int c0, int j0, __half *bhi, __half *blo,
+                              float *bscale, int split) {
+    __shared__ unsigned cmax[COLS];  // largest |re| or |im| of each column, as ordered bits
+    const int tid = threadIdx.x;
+    if (tid < COLS) cmax[tid] = 0u;
+    __syncthreads();
+    {
+        const int c = tid % COLS;
+        float mx = 0.f;
+        for (int r = tid / COLS; r < kb; r += 256 / COLS) {
+            const Cx<float> u = X[r * COLS + c];
+            mx = fmaxf(mx, fmaxf(fabsf(u.re), fabsf(u.im)));
+        }
+        atomicMax(&cmax[c], __float_as_uint(mx));
+    }
+    __syncthreads();
+    if (tid < nc) bscale[c0 + tid - j0] = pow2f(-stage_exp(__uint_as_float(cmax[tid])) - L_SHIFT);
+    // consecutive threads: consecutive K (rows kk of the block) of one B_s row
+    for (int i = tid; i < 2 * COLS * kb; i += 256) {
+        const int row = i / kb, kk = i % kb, c = row >> 1;
+        if (c >= nc) continue;
+        const float sc = pow2f(stage_exp(__uint_as_float(cmax[c])));
+        const Cx<float> u = X[kk * COLS + c];
+        const float vx = ((row & 1) ? u.im : u.re) * sc, vy = ((row & 1) ? u.re : -u.im) * sc;
+        const int64_t at = (int64_t)(2 * (c0 + c - j0) + (row & 1)) * 2 * kb + 2 * kk;
+        __half hx, hy, lx, ly;
+        split_f16(vx, hx, lx);
+        split_f16(vy, hy, ly);
+        *reinterpret_cast<__half2 *>(bhi + at) = __halves2half2(hx, hy);
+        if (split == 3) *reinterpret_cast<__half2 *>(blo + at) = __halves2half2(lx, ly);
+    }
 }
 template <typename T, int W>
 __global__ void __launch_bounds__(256) trsm_blocked_kernel(Cx<T> *A, int64_t ld, int k, int S, const Cx<T> *D,
-                                                            int c_begin, int c_end, float *bhi = nullptr,
-                                                            float *blo = nullptr, int j0 = 0, int split = 3) {
+                                                            int c_begin, int c_end, __half *bhi = nullptr,
+                                                            __half *blo = nullptr, float *bscale = nullptr,
+                                                            int j0 = 0, int split = 3) {
     constexpr int OPT = W * TB_COLS / 256;  // outputs per thread: 4 (W = 32) or 2 (W = 16)
     constexpr int CG = TB_COLS / OPT;       // column groups
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -575,25 +607,7 @@ __global__ void __launch_bounds__(256) trsm_blocked_kernel(Cx<T> *A, int64_t ld,
         if (c < nc) A[(int64_t)(k + rr) * ld + c0 + c] = X[rr * TB_COLS + c];
     }
     if constexpr (sizeof(T) == 4) {
-        if (bhi) {
-            // consecutive threads: consecutive K (rows kk of the block) of one B_s row
-            for (int i = tid; i < 2 * TB_COLS * kb; i += 256) {
-                const int row = i / kb, kk = i % kb, c = row >> 1;
-                if (c >= nc) continue;
-                const Cx<T> u = X[kk * TB_COLS + c];
-                const float2 v = (row & 1) ? make_float2(u.im, u.re) : make_float2(u.re, -u.im);
-                const int64_t at = (int64_t)(2 * (c0 + c - j0) + (row & 1)) * 2 * kb + 2 * kk;
-                if (split == 3) {
-                    float2 h, l;
-                    tf32_split(v.x, h.x, l.x);
-                    tf32_split(v.y, h.y, l.y);
-                    *reinterpret_cast<float2 *>(bhi + at) = h;
-                    *reinterpret_cast<float2 *>(blo + at) = l;
-                } else {
-                    *reinterpret_cast<float2 *>(bhi + at) = v;
-                }
-            }
-        }
+        if (bhi) stage_u_block<TB_COLS>(X, kb, nc, c0, j0, bhi, blo, bscale, split);
     }
 }
 
@@ -622,8 +636,8 @@ template <typename T, int W> static size_t trsm_narrow_smem(int S) {
 }
 template <typename T, int W>
 __global__ void __launch_bounds__(256) trsm_narrow_kernel(Cx<T> *A, int64_t ld, int k, int S, const Cx<T> *D,
-                                                          int c_begin, int c_end, float *bhi, float *blo, int j0,
-                                                          int split) {
+                                                          int c_begin, int c_end, __half *bhi, __half *blo,
+                                                          float *bscale, int j0, int split) {
     constexpr int NC = narrow_cols<W>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int kb = S * W;
@@ -685,24 +699,7 @@ __global__ void __launch_bounds__(256) trsm_narrow_kernel(Cx<T> *A, int64_t ld, 
         if (c < nc) A[(int64_t)(k + i / NC) * ld + c0 + c] = X[i];
     }
     if constexpr (sizeof(T) == 4) {
-        if (bhi) {
-            for (int i = tid; i < 2 * NC * kb; i += 256) {
-                const int row = i / kb, kk = i % kb, c = row >> 1;
-                if (c >= nc) continue;
-                const Cx<T> u = X[kk * NC + c];
-                const float2 v = (row & 1) ? make_float2(u.im, u.re) : make_float2(u.re, -u.im);
-                const int64_t at = (int64_t)(2 * (c0 + c - j0) + (row & 1)) * 2 * kb + 2 * kk;
-                if (split == 3) {
-                    float2 h, l;
-                    tf32_split(v.x, h.x, l.x);
-                    tf32_split(v.y, h.y, l.y);
-                    *reinterpret_cast<float2 *>(bhi + at) = h;
-                    *reinterpret_cast<float2 *>(blo + at) = l;
-                } else {
-                    *reinterpret_cast<float2 *>(bhi + at) = v;
-                }
-            }
-        }
+        if (bhi) stage_u_block<NC>(X, kb, nc, c0, j0, bhi, blo, bscale, split);
     }
 }
 
@@ -1491,7 +1488,7 @@ static bool cluster_panel(beat_b200_ctx *c, Cx<T> *A, int64_t ld, int n, int k, 
 bool tc_update_supported(int nb);
 void tc_stage_l(beat_b200_ctx *c, int k, int nb, int split_terms, cudaStream_t st);
 void tc_stage_u(beat_b200_ctx *c, int k, int nb, int split_terms, int col_lo, int col_hi, cudaStream_t st);
-void tc_stage_u_buffers(beat_b200_ctx *c, int k, int nb, float **bhi, float **blo);
+void tc_stage_u_buffers(beat_b200_ctx *c, int k, int nb, __half **bhi, __half **blo, float **bscale);
 void tc_update_cols(beat_b200_ctx *c, int k, int nb, int split_terms, int col_lo, int col_hi, cudaStream_t st,
                     int max_ctas);
 
@@ -1567,14 +1564,15 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
     auto u_solve = [&](int k, int c_lo, int c_hi, cudaStream_t st, bool crit) {
         const int cols = c_hi - c_lo;
         if (cols <= 0) return;
-        float *bhi = nullptr, *blo = nullptr;
-        if (fused_stage) tc_stage_u_buffers(c, k, nb, &bhi, &blo);
+        __half *bhi = nullptr, *blo = nullptr;
+        float *bsc = nullptr;
+        if (fused_stage) tc_stage_u_buffers(c, k, nb, &bhi, &blo, &bsc);
         if (crit && narrow)
             trsm_narrow_kernel<T, WF><<<(cols + NC - 1) / NC, 256, trsm_narrow_smem<T, WF>(nb / W), st>>>(
-                A, ld, k, nb / W, dinv + (size_t)(k / W) * W * W, c_lo, c_hi, bhi, blo, k + nb, split_terms);
+                A, ld, k, nb / W, dinv + (size_t)(k / W) * W * W, c_lo, c_hi, bhi, blo, bsc, k + nb, split_terms);
         else if (blocked)
             trsm_blocked_kernel<T, WF><<<(cols + TB_COLS - 1) / TB_COLS, 256, tb_smem, st>>>(
-                A, ld, k, nb / W, dinv + (size_t)(k / W) * W * W, c_lo, c_hi, bhi, blo, k + nb, split_terms);
+                A, ld, k, nb / W, dinv + (size_t)(k / W) * W * W, c_lo, c_hi, bhi, blo, bsc, k + nb, split_terms);
         else
             trsm_kernel<T><<<(cols + TRSM_COLS - 1) / TRSM_COLS, 256, trsm_smem, st>>>(A, ld, n, k, nb, c_lo, c_hi);
         BB_CUDA(cudaGetLastError());
@@ -1660,7 +1658,8 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
                 const int cols = pe - ks - W;
                 if (narrow)
                     trsm_narrow_kernel<T, WF><<<(cols + NC - 1) / NC, 256, trsm_narrow_smem<T, WF>(1), s0>>>(
-                        A, ld, ks, 1, dinv + (size_t)(ks / W) * W * W, ks + W, pe, nullptr, nullptr, 0, split_terms);
+                        A, ld, ks, 1, dinv + (size_t)(ks / W) * W * W, ks + W, pe, nullptr, nullptr, nullptr, 0,
+                        split_terms);
                 else if (blocked)
                     trsm_blocked_kernel<T, WF><<<(cols + TB_COLS - 1) / TB_COLS, 256, tb_smem, s0>>>(
                         A, ld, ks, 1, dinv + (size_t)(ks / W) * W * W, ks + W, pe);

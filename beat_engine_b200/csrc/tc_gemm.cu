@@ -1,4 +1,4 @@
-// tc_gemm.cu -- tcgen05 TF32 tensor-core trailing update of the FP32 LU:
+// tc_gemm.cu -- tcgen05 FP16-split tensor-core trailing update of the FP32 LU:
 //     A22 -= L21 U12      (complex, FP32 storage, FP32 accumulation in TMEM)
 //
 // Complex -> real: with row-major interleaved storage a complex row of length
@@ -7,9 +7,22 @@
 //     U_big[2k, 2j] = Ur, U_big[2k+1, 2j] = -Ui, U_big[2k, 2j+1] = Ui, U_big[2k+1, 2j+1] = Ur
 // so one real GEMM of M = rows, N = 2 cols, K = 2 nb does the complex update
 // with no wasted products.  Both operands are staged K-major (K contiguous):
-// A_s[i][k'] = L_R[i][k'] and B_s[n][k'] = U_big[k'][n], each split into a
-// TF32 high part and an FP32 remainder; the MMA sums hi*hi + hi*lo + lo*hi
-// (split_terms = 3, about FP32 accuracy) or takes the values as TF32 (1).
+// A_s[i][k'] = L_R[i][k'] and B_s[n][k'] = U_big[k'][n], each scaled by a
+// power of two and split into an FP16 high part and the FP16 rounding of the
+// remainder (11 + 11 significant bits); the MMA (kind::f16, FP32
+// accumulation) sums hi*hi + hi*lo + lo*hi (split_terms = 3, about FP32
+// accuracy: the same 22 bits as a TF32 high part with a TF32-rounded
+// remainder, at twice the tensor rate and half the operand bytes) or takes
+// the high parts alone (1).  FP16 has 5 exponent bits, hence the scales:
+//   L: |l| <= sqrt 2 under partial pivoting by |re| + |im|, so L is staged
+//      times 2^L_SHIFT, which keeps the high part below 2^13 and moves small
+//      multipliers out of the subnormal range;
+//   U: each complex column j of U12 is staged times 2^s_j with s_j chosen so
+//      that its largest |re| or |im| lies in [2^13, 2^14) (B_SCALE_EXP); the
+//      epilogue multiplies column j of the product by 2^-(s_j + L_SHIFT),
+//      kept per column in the staging buffer.
+// Normwise the staged operands carry about 2^-22 of each column's (and of L's)
+// largest entry, like the TF32 split's 2^-22 relative error per entry.
 //
 // Kernel: one CTA per 128 x 256 output tile, 6 warps.
 //   warp 0       TMA producer (cp.async.bulk.tensor, SWIZZLE_128B, no multicast)
@@ -18,6 +31,7 @@
 // Every mbarrier wait has an iteration budget; on expiry the CTA sets a status
 // bit, drains what it issued (bounded) and frees its TMEM.
 #include <cuda.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -28,7 +42,7 @@
 
 namespace bb {
 
-constexpr int TC_BM = 128, TC_BN = 256, TC_BK = 32;  // tile: rows, real cols, K per stage (fp32)
+constexpr int TC_BM = 128, TC_BN = 256, TC_BK = 64;  // tile: rows, real cols, K per stage (fp16: 128-byte rows)
 constexpr int TC_THREADS = 192;
 constexpr uint32_t TC_SPIN = 1u << 24;
 
@@ -76,15 +90,17 @@ __device__ __forceinline__ uint64_t umma_desc_sw128(const void *smem) {
     return addr | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
 }
 
-// kind::tf32, D f32, A/B tf32 K-major, M = 128, N = 256
-constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
+// kind::f16 instruction descriptor: D f32 (bits 4-5 = 1), A and B both f16
+// (bits 7-9 and 10-12 = 0), both K-major, N >> 3 at bit 17, M >> 4 at bit 24;
+// M = 128, N = 256
+constexpr uint32_t TC_IDESC = (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
                               ((uint32_t)(TC_BM >> 4) << 24);
 
-__device__ __forceinline__ void umma_tf32(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void umma_f16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtmem),
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtmem),
         "l"(adesc), "l"(bdesc), "r"(TC_IDESC), "r"(accumulate)
         : "memory");
 }
@@ -118,7 +134,8 @@ struct TcArgs {
     int ncr;           // real columns of the trailing block (2 x complex columns)
     int cx0, cy0;      // coordinates of the block origin in the C tensor map (real col, row)
     int brow0;         // first row of the staged B operand that this block's columns use
-    int kchunks;       // K / 32
+    int kchunks;       // K / TC_BK
+    const float *bscale;  // per staged complex column: 2^-(s_j + L_SHIFT), undoing the staging's scales
     int split;         // 1 or 3
     int tiles_n;       // column tiles
     int ntiles;
@@ -149,7 +166,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                      const __grid_constant__ CUtensorMap mC, TcArgs g) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    constexpr int A_BYTES = TC_BM * TC_BK * 4, B_BYTES = TC_BN * TC_BK * 4;
+    constexpr int A_BYTES = TC_BM * TC_BK * 2, B_BYTES = TC_BN * TC_BK * 2;  // fp16 operands
     constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
     float *epi = reinterpret_cast<float *>(base + (size_t)STAGES * STAGE_BYTES);  // 4 x 32 x 32
     __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], tfull_bar[2], tempty_bar[2], drain_bar;
@@ -236,14 +253,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     const uint64_t bh = umma_desc_sw128(st + 2 * A_BYTES),
                                    bl = umma_desc_sw128(st + 2 * A_BYTES + B_BYTES);
 #pragma unroll
-                    for (int kk = 0; kk < TC_BK / 8; ++kk) {
-                        const uint64_t adv = (uint64_t)(kk * 32) >> 4;  // 8 tf32 = 32 bytes along K
+                    for (int kk = 0; kk < TC_BK / 16; ++kk) {
+                        const uint64_t adv = (uint64_t)(kk * 32) >> 4;  // 16 f16 = 32 bytes along K
                         if (split3) {
-                            umma_tf32(dt, al + adv, bh + adv, acc);
-                            umma_tf32(dt, ah + adv, bl + adv, 1);
-                            umma_tf32(dt, ah + adv, bh + adv, 1);
+                            umma_f16(dt, al + adv, bh + adv, acc);
+                            umma_f16(dt, ah + adv, bl + adv, 1);
+                            umma_f16(dt, ah + adv, bh + adv, 1);
                         } else {
-                            umma_tf32(dt, ah + adv, bh + adv, acc);
+                            umma_f16(dt, ah + adv, bh + adv, acc);
                         }
                         acc = 1;
                     }
@@ -275,7 +292,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 float v[32];
                 tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * TC_BN + c), v);
                 if (!rows_live || col0 + c >= g.ncr) continue;  // nothing of this chunk is inside C
-                if (lane == 0) bulk_wait_read0();                 // staging buffer free again
+                {
+                    // undo the staging's scales: lane l fetches real column c + l's factor
+                    const float sl = g.bscale[(g.brow0 + col0 + c + lane) >> 1];
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) v[i] *= __shfl_sync(0xffffffffu, sl, i);
+                }
+                if (lane == 0) bulk_wait_read0();  // staging buffer free again
                 __syncwarp();
                 // row `lane` of the 32 x 32 box, in the TMA 128-byte swizzle:
                 // 16-byte chunk j of row r sits at chunk j ^ (r & 7)
@@ -307,54 +330,59 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 
 // ---------------------------------------------------------------------------
 // operand staging: A_s[i][k'] = L_R rows, B_s[n][k'] = U_big columns, hi/lo
+// FP16, scaled (see the top of this file)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void split_tf32(float x, float &hi, float &lo) {
-    hi = __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
-    lo = x - hi;
-}
-
-__global__ void stage_a_kernel(const float2 *A, int64_t ld, int k, int nb, int m, float *ahi, float *alo, int split) {
-    // row i of L21 = A[k+nb+i][k .. k+nb)
+__global__ void stage_a_kernel(const float2 *A, int64_t ld, int k, int nb, int m, __half *ahi, __half *alo,
+                               int split) {
+    // row i of L21 = A[k+nb+i][k .. k+nb), times 2^L_SHIFT
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (int64_t)m * nb) return;
     const int i = (int)(idx / nb), kk = (int)(idx % nb);
     const float2 v = A[(int64_t)(k + nb + i) * ld + k + kk];
-    float2 *h = reinterpret_cast<float2 *>(ahi + (int64_t)i * 2 * nb) + kk;
-    if (split == 3) {
-        float2 hv, lv;
-        split_tf32(v.x, hv.x, lv.x);
-        split_tf32(v.y, hv.y, lv.y);
-        *h = hv;
-        *(reinterpret_cast<float2 *>(alo + (int64_t)i * 2 * nb) + kk) = lv;
-    } else {
-        *h = v;
-    }
+    const float sc = pow2f(L_SHIFT);
+    __half hr, hi_, lr, li;
+    split_f16(v.x * sc, hr, lr);
+    split_f16(v.y * sc, hi_, li);
+    reinterpret_cast<__half2 *>(ahi + (int64_t)i * 2 * nb)[kk] = __halves2half2(hr, hi_);
+    if (split == 3) reinterpret_cast<__half2 *>(alo + (int64_t)i * 2 * nb)[kk] = __halves2half2(lr, li);
 }
 
-__global__ void stage_b_kernel(const float2 *A, int64_t ld, int k, int nb, int j0, int ncols, float *bhi, float *blo,
-                               int split) {
-    // U12[kk][j] = A[k+kk][k+nb+j], j = j0 .. j0+ncols; rows 2j and 2j+1 of B_s get (Ur, -Ui) and
-    // (Ui, Ur) at K = 2kk
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (int64_t)ncols * nb) return;
-    const int j = j0 + (int)(idx / nb), kk = (int)(idx % nb);
-    const float2 u = A[(int64_t)(k + kk) * ld + k + nb + j];
-    const float2 e = make_float2(u.x, -u.y), o = make_float2(u.y, u.x);
-    float2 *h0 = reinterpret_cast<float2 *>(bhi + (int64_t)(2 * j) * 2 * nb) + kk;
-    float2 *h1 = reinterpret_cast<float2 *>(bhi + (int64_t)(2 * j + 1) * 2 * nb) + kk;
-    if (split == 3) {
-        float2 he, le, ho, lo_;
-        split_tf32(e.x, he.x, le.x);
-        split_tf32(e.y, he.y, le.y);
-        split_tf32(o.x, ho.x, lo_.x);
-        split_tf32(o.y, ho.y, lo_.y);
-        *h0 = he;
-        *h1 = ho;
-        *(reinterpret_cast<float2 *>(blo + (int64_t)(2 * j) * 2 * nb) + kk) = le;
-        *(reinterpret_cast<float2 *>(blo + (int64_t)(2 * j + 1) * 2 * nb) + kk) = lo_;
-    } else {
-        *h0 = e;
-        *h1 = o;
+// One warp per complex column j of U12 (U12[kk][j] = A[k+kk][k+nb+j], j = j0 ..
+// j0+ncols): the column's exponent s_j from its largest |re| or |im|, then
+// rows 2j and 2j+1 of B_s get (Ur, -Ui) 2^s_j and (Ui, Ur) 2^s_j at K = 2kk,
+// and bscale[j] = 2^-(s_j + L_SHIFT).
+__global__ void stage_b_kernel(const float2 *A, int64_t ld, int k, int nb, int j0, int ncols, __half *bhi,
+                               __half *blo, float *bscale, int split) {
+    const int wi = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (wi >= ncols) return;  // whole warps
+    const int j = j0 + wi;
+    const float2 *col = A + (int64_t)k * ld + k + nb + j;
+    float mx = 0.f;
+    for (int kk = lane; kk < nb; kk += 32) {
+        const float2 u = col[(int64_t)kk * ld];
+        mx = fmaxf(mx, fmaxf(fabsf(u.x), fabsf(u.y)));
+    }
+    mx = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(mx)));  // non-negative: ordered as bits
+    const int sx = stage_exp(mx);
+    const float sc = pow2f(sx);
+    if (lane == 0) bscale[j] = pow2f(-sx - L_SHIFT);
+    __half2 *h0 = reinterpret_cast<__half2 *>(bhi + (int64_t)(2 * j) * 2 * nb);
+    __half2 *h1 = reinterpret_cast<__half2 *>(bhi + (int64_t)(2 * j + 1) * 2 * nb);
+    __half2 *l0 = reinterpret_cast<__half2 *>(blo + (int64_t)(2 * j) * 2 * nb);
+    __half2 *l1 = reinterpret_cast<__half2 *>(blo + (int64_t)(2 * j + 1) * 2 * nb);
+    for (int kk = lane; kk < nb; kk += 32) {
+        const float2 u = col[(int64_t)kk * ld];
+        __half er, ei, orr, oi, ler, lei, lor, loi;
+        split_f16(u.x * sc, er, ler);
+        split_f16(-u.y * sc, ei, lei);
+        split_f16(u.y * sc, orr, lor);
+        split_f16(u.x * sc, oi, loi);
+        h0[kk] = __halves2half2(er, ei);
+        h1[kk] = __halves2half2(orr, oi);
+        if (split == 3) {
+            l0[kk] = __halves2half2(ler, lei);
+            l1[kk] = __halves2half2(lor, loi);
+        }
     }
 }
 
@@ -378,15 +406,15 @@ static EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// rows x kdim fp32, row-major, box 32 (K) x box_rows
-static CUtensorMap make_map(const float *ptr, int64_t rows, int kdim, int box_rows) {
+// rows x kdim fp16, row-major, box TC_BK (K, 128 bytes) x box_rows
+static CUtensorMap make_map(const __half *ptr, int64_t rows, int kdim, int box_rows) {
     CUtensorMap m;
     std::memset(&m, 0, sizeof(m));
     cuuint64_t dims[2] = {(cuuint64_t)kdim, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)kdim * 4};
+    cuuint64_t strides[1] = {(cuuint64_t)kdim * sizeof(__half)};
     cuuint32_t box[2] = {(cuuint32_t)TC_BK, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)ptr, dims, strides, box, estr,
+    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, (void *)ptr, dims, strides, box, estr,
                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     BB_REQUIRE(r == CUDA_SUCCESS, BEAT_B200_CUDA_ERROR, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
@@ -411,10 +439,12 @@ static CUtensorMap make_c_map(const float *ptr, int n, int64_t ld) {
 }
 
 // Staging of panel k's operands for the trailing update A22 -= L21 U12 (rows
-// and columns k + nb .. n): A_hi/A_lo (m x 2nb) and B_hi/B_lo (2m x 2nb),
-// m = n - k - nb, in the workspace's staging buffer.
+// and columns k + nb .. n): A_hi/A_lo (m x 2nb fp16) and B_hi/B_lo (2m x 2nb
+// fp16), m = n - k - nb, and the per-column factors bscale (m, padded), in the
+// workspace's staging buffer.
 struct TcStage {
-    float *ahi, *alo, *bhi, *blo;
+    __half *ahi, *alo, *bhi, *blo;
+    float *bscale;
     int m, kdim;
 };
 
@@ -426,20 +456,26 @@ static TcStage tc_stage_buffers(beat_b200_ctx *c, int k, int nb) {
     s.kdim = 2 * nb;
     const int64_t mpad = ((int64_t)s.m + TC_BM - 1) / TC_BM * TC_BM;
     const int64_t npad = ((int64_t)2 * s.m + TC_BN - 1) / TC_BN * TC_BN;
-    const size_t need = sizeof(float) * (size_t)s.kdim * (2 * (size_t)mpad + 2 * (size_t)npad) + 1024;
-    if (w.stage.bytes < need) {
+    // the factors: one per staged complex column, padded so that an epilogue chunk past the
+    // last column still reads inside the buffer
+    auto bytes = [&](int64_t mp, int64_t np) {
+        return sizeof(__half) * (size_t)s.kdim * (2 * (size_t)mp + 2 * (size_t)np) +
+               sizeof(float) * (size_t)(np / 2 + 64) + 1024;
+    };
+    if (w.stage.bytes < bytes(mpad, npad)) {
         // size for the first (largest) panel
         const int64_t m0 = n, mp0 = (m0 + TC_BM - 1) / TC_BM * TC_BM, np0 = (2 * m0 + TC_BN - 1) / TC_BN * TC_BN;
-        w.stage.alloc(sizeof(float) * (size_t)s.kdim * (2 * (size_t)mp0 + 2 * (size_t)np0) + 1024);
+        w.stage.alloc(bytes(mp0, np0));
     }
-    s.ahi = w.stage.as<float>();
+    s.ahi = w.stage.as<__half>();
     s.alo = s.ahi + (size_t)mpad * s.kdim;
     s.bhi = s.alo + (size_t)mpad * s.kdim;
     s.blo = s.bhi + (size_t)npad * s.kdim;
+    s.bscale = reinterpret_cast<float *>(s.blo + (size_t)npad * s.kdim);
     return s;
 }
 
-bool tc_update_supported(int nb) { return nb % 16 == 0; }  // K = 2 nb must be a multiple of 32
+bool tc_update_supported(int nb) { return nb % 32 == 0; }  // K = 2 nb must be a multiple of TC_BK
 
 // Stages L21 of panel k (every row below the panel).
 void tc_stage_l(beat_b200_ctx *c, int k, int nb, int split_terms, cudaStream_t st) {
@@ -457,18 +493,18 @@ void tc_stage_u(beat_b200_ctx *c, int k, int nb, int split_terms, int col_lo, in
     const TcStage s = tc_stage_buffers(c, k, nb);
     const int nc = col_hi - col_lo;
     if (s.m <= 0 || nc <= 0) return;
-    const int64_t nbk = (int64_t)nc * nb;
-    stage_b_kernel<<<(unsigned)((nbk + 255) / 256), 256, 0, st>>>(c->ws.A.as<float2>(), c->ws.ld, k, nb,
-                                                                  col_lo - (k + nb), nc, s.bhi, s.blo, split_terms);
+    stage_b_kernel<<<(unsigned)(((int64_t)nc * 32 + 255) / 256), 256, 0, st>>>(
+        c->ws.A.as<float2>(), c->ws.ld, k, nb, col_lo - (k + nb), nc, s.bhi, s.blo, s.bscale, split_terms);
     BB_CUDA(cudaGetLastError());
 }
 
-// The B-operand staging of panel k (rows 2 j, 2 j + 1 for column k + nb + j, K = 2 nb):
-// the blocked U12 solve writes it directly (lu.cu).
-void tc_stage_u_buffers(beat_b200_ctx *c, int k, int nb, float **bhi, float **blo) {
+// The B-operand staging of panel k (rows 2 j, 2 j + 1 for column k + nb + j, K = 2 nb,
+// and the column factors): the blocked U12 solve writes it directly (lu.cu).
+void tc_stage_u_buffers(beat_b200_ctx *c, int k, int nb, __half **bhi, __half **blo, float **bscale) {
     const TcStage s = tc_stage_buffers(c, k, nb);
     *bhi = s.bhi;
     *blo = s.blo;
+    *bscale = s.bscale;
 }
 
 // A[k+nb.., col_lo..col_hi) -= L21 U12 from the staged operands, on `st`,
@@ -494,7 +530,8 @@ void tc_update_cols(beat_b200_ctx *c, int k, int nb, int split_terms, int col_lo
     g.tiles_n = (2 * nc + TC_BN - 1) / TC_BN;
     g.ntiles = g.tiles_n * ((s.m + TC_BM - 1) / TC_BM);
     g.status = c->status.as<int>();
-    const size_t smem = (size_t)TC_STAGES * (2 * TC_BM * TC_BK * 4 + 2 * TC_BN * TC_BK * 4) + 4 * TC_EPI_BYTES + 1024;
+    g.bscale = s.bscale;
+    const size_t smem = (size_t)TC_STAGES * (2 * TC_BM * TC_BK * 2 + 2 * TC_BN * TC_BK * 2) + 4 * TC_EPI_BYTES + 1024;
     static std::atomic<bool> attr_done{false};  // sweep lanes call this from several threads
     if (!attr_done) {
         BB_CUDA(cudaFuncSetAttribute(tc_update_kernel<TC_STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,

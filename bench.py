@@ -12,7 +12,7 @@ assembly + one LU + R-column solve (+ FP64 GMRES refinement in the mixed
 form) + the far-field pattern at 541 directions (360 equator + 181 meridian)
 for all R.
 
-``value``: device-timed throughput of the mixed form (FP32 assembly, TF32
+``value``: device-timed throughput of the mixed form (FP32 assembly, FP16
 split tensor-core LU, FP64 GMRES refinement) with q already in HBM: the K
 timed steps (frequencies) run as one beat_b200_sweep_device call, which
 pipelines them over up to six solve lanes (one frequency's assembly beside
@@ -279,7 +279,7 @@ def config_dict(args, mesh):
                         f"(F={mesh.num_faces} faces, N={mesh.num_vertices} P1 dofs), R={args.rhs} RHS, "
                         "f cycling 0.5/2/6 kHz, order 4/4, far field at 541 directions",
             "faces": mesh.num_faces, "dofs": mesh.num_vertices, "rhs": args.rhs,
-            "precision_form": "mixed (FP32 assembly, TF32 split tensor-core LU, FP64 GMRES refinement); "
+            "precision_form": "mixed (FP32 assembly, FP32 LU with FP16-split tensor-core updates (22 significant bits), FP64 GMRES refinement); "
                               "the FP64 form timed beside it", "lu_split_terms": args.split,
             "l2": "inputs larger than L2: every step rewrites A (N^2 complex) and the N x F RHS operator",
             "parallelism": f"frequency replicas x{args.gpus} (no collective); "
@@ -528,7 +528,7 @@ def run_gpu(args):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
                 "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
-                "dtype": "c64 (tf32 tensor LU) + c128 refinement",
+                "dtype": "c64 (fp16x2-split tensor LU) + c128 refinement",
                 "data": "synthetic (seeded velocities on a generated icosphere)",
                 "config": config_dict(args, mesh), "stages_ms": stages,
                 "stages_basis": "one frequency solved alone (stage times inside the sweep overlap)",
@@ -656,7 +656,7 @@ def run_sweep_config(args):
         err = max(err, float(np.max(np.linalg.norm(pm - p64, axis=2) / np.linalg.norm(p64, axis=2))))
     line = {"metric": "batched sweep: freq-solves/s over 6 enclosures x 64 frequencies, mixed FP32+IR, 1 B200",
             "value": n_jobs / (ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": args.warmup,
-            "sweep_wall_s": ms / 1e3, "higher_is_better": True, "dtype": "c64 (tf32 tensor LU) + c128 refinement",
+            "sweep_wall_s": ms / 1e3, "higher_is_better": True, "dtype": "c64 (fp16x2-split tensor LU) + c128 refinement",
             "data": "synthetic (seeded jittered enclosures and velocities)",
             "config": {"workload": "rounded-box enclosures 0.2x0.3x0.25 m + 0.05 m piston, targets "
                                    f"{list(SWEEP_MESHES)} triangles (F = {[m.num_faces for m in meshes]}, "

@@ -59,7 +59,8 @@ typedef struct {
     int32_t precision;      /* BEAT_B200_FP64 or BEAT_B200_MIXED_FP32_IR */
     int32_t ir_restart;     /* GMRES restart length (20) */
     int32_t ir_max_iters;   /* total GMRES iterations allowed (200) */
-    int32_t lu_split_terms; /* TF32 products per trailing update: 1 or 3 (3) */
+    int32_t lu_split_terms; /* split products per trailing update: 3 (FP16 high x high + high x low +
+                               low x high, about FP32 accuracy) or 1 (FP16 high parts only) (3) */
     double ir_rtol;         /* relative residual target of the refinement (1e-10) */
     int32_t lu_block;       /* LU panel width; 0 = tuned default */
     int32_t flags;          /* BEAT_B200_FLAG_* bits, 0 by default */
