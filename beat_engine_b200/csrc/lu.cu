@@ -2105,7 +2105,13 @@ __global__ void __launch_bounds__(SubstTile<T>::THREADS, 1) block_subst_kernel(c
     }
 }
 
-#define SUBST_CTAS_CAP(c) ((c)->sm_count)
+// Persistent CTAs of a block substitution: half the SMs.  A CTA holds about 58 K
+// registers, so each one keeps its SM from every other kernel while the chain
+// of blocks waits on its flags; at N = 10,242 one triangle takes the same time
+// on 74 CTAs as on 148 (2.00 against 2.02 ms for the solve's two), 2.26 ms on 48,
+// and the six-lane sweep's best of 8 runs read 18.7-19.1 freq-solves/s with 74
+// against 18.3 with 148.
+#define SUBST_CTAS_CAP(c) (std::max(1, (c)->sm_count / 2))
 // CTAs of a substitution launch: every block's folded-in sum must be under
 // way well before the chain reaches it, but a CTA spinning on a flag holds its
 // SM, which the other lanes of a sweep could use
