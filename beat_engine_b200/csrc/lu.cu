@@ -629,23 +629,25 @@ template <typename T> __device__ __forceinline__ void cp_async_cx(Cx<T> *smem, c
 // global load.  Two partial sums per product.  The same optional B-operand
 // staging as trsm_blocked_kernel.
 template <int W> __host__ __device__ constexpr int narrow_cols() { return 256 / W; }
-template <typename T, int W> static size_t trsm_narrow_smem(int S) {
-    const size_t NC = narrow_cols<W>();
+template <typename T, int W, int NC = narrow_cols<W>()> static size_t trsm_narrow_smem(int S) {
     return sizeof(Cx<T>) * ((size_t)S * W * NC + (size_t)S * W * (W + 1) +
                             (size_t)W * ((size_t)W * S * (S - 1) / 2 + (S - 1)) + (size_t)W * NC);
 }
-template <typename T, int W>
+// NC columns per CTA (a multiple of 256 / W): each thread holds OPT = NC W / 256
+// entries of a W-row block, row tid / (256 / W), columns tid % (256 / W) + (256 / W) o.
+template <typename T, int W, int NC = narrow_cols<W>()>
 __global__ void __launch_bounds__(256) trsm_narrow_kernel(Cx<T> *A, int64_t ld, int k, int S, const Cx<T> *D,
                                                           int c_begin, int c_end, __half *bhi, __half *blo,
                                                           float *bscale, int j0, int split) {
-    constexpr int NC = narrow_cols<W>();
+    constexpr int CG = narrow_cols<W>(), OPT = NC / CG;
+    static_assert(OPT >= 1 && NC % CG == 0, "NC: a multiple of 256 / W");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int kb = S * W;
     Cx<T> *X = reinterpret_cast<Cx<T> *>(smem_raw);  // kb x NC
     Cx<T> *Ds = X + (size_t)kb * NC;                  // S blocks of W x (W + 1)
     Cx<T> *Ls = Ds + (size_t)S * W * (W + 1);         // block row s >= 1: W x (s W + 1)
     Cx<T> *Z = Ls + (size_t)W * ((size_t)W * S * (S - 1) / 2 + (S - 1));  // W x NC
-    const int tid = threadIdx.x, r = tid / NC, cc = tid % NC;
+    const int tid = threadIdx.x, r = tid / CG, cg = tid % CG;
     const int c0 = c_begin + blockIdx.x * NC;
     const int nc = min(NC, c_end - c0);
     for (int i = tid; i < kb * NC; i += 256) {
@@ -669,29 +671,51 @@ __global__ void __launch_bounds__(256) trsm_narrow_kernel(Cx<T> *A, int64_t ld, 
     __syncthreads();
     for (int s = 0; s < S; ++s) {
         const int r0 = s * W;
-        Cx<T> a0 = X[(r0 + r) * NC + cc], a1{T(0), T(0)};
+        Cx<T> a0[OPT], a1[OPT];
+#pragma unroll
+        for (int o = 0; o < OPT; ++o) {
+            a0[o] = X[(r0 + r) * NC + cg + CG * o];
+            a1[o] = Cx<T>{T(0), T(0)};
+        }
         if (s > 0) {  // A_s - L_s,<s X_<s
             const Cx<T> *Lr = Ls + (size_t)W * ((size_t)W * s * (s - 1) / 2 + (s - 1)) + (size_t)r * (r0 + 1);
             for (int t = 0; t < r0; t += 2) {  // r0 is a multiple of W, so even
-                a0 = cms(a0, Lr[t], X[t * NC + cc]);
-                a1 = cms(a1, Lr[t + 1], X[(t + 1) * NC + cc]);
+                const Cx<T> l0 = Lr[t], l1 = Lr[t + 1];
+#pragma unroll
+                for (int o = 0; o < OPT; ++o) {
+                    a0[o] = cms(a0[o], l0, X[t * NC + cg + CG * o]);
+                    a1[o] = cms(a1[o], l1, X[(t + 1) * NC + cg + CG * o]);
+                }
             }
         }
-        Z[r * NC + cc] = Cx<T>{a0.re + a1.re, a0.im + a1.im};
+#pragma unroll
+        for (int o = 0; o < OPT; ++o) Z[r * NC + cg + CG * o] = Cx<T>{a0[o].re + a1[o].re, a0[o].im + a1[o].im};
         __syncthreads();
         const Cx<T> *Dr = Ds + (size_t)s * W * (W + 1) + (size_t)r * (W + 1);
-        Cx<T> y0{T(0), T(0)}, y1{T(0), T(0)};
+        Cx<T> y0[OPT], y1[OPT];
+#pragma unroll
+        for (int o = 0; o < OPT; ++o) y0[o] = y1[o] = Cx<T>{T(0), T(0)};
         int t = 0;
         for (; t + 1 <= r; t += 2) {  // D_s is lower triangular
-            const Cx<T> d0 = Dr[t], d1 = Dr[t + 1], z0 = Z[t * NC + cc], z1 = Z[(t + 1) * NC + cc];
-            y0 = Cx<T>{y0.re + (d0.re * z0.re - d0.im * z0.im), y0.im + (d0.re * z0.im + d0.im * z0.re)};
-            y1 = Cx<T>{y1.re + (d1.re * z1.re - d1.im * z1.im), y1.im + (d1.re * z1.im + d1.im * z1.re)};
+            const Cx<T> d0 = Dr[t], d1 = Dr[t + 1];
+#pragma unroll
+            for (int o = 0; o < OPT; ++o) {
+                const Cx<T> z0 = Z[t * NC + cg + CG * o], z1 = Z[(t + 1) * NC + cg + CG * o];
+                y0[o] = Cx<T>{y0[o].re + (d0.re * z0.re - d0.im * z0.im), y0[o].im + (d0.re * z0.im + d0.im * z0.re)};
+                y1[o] = Cx<T>{y1[o].re + (d1.re * z1.re - d1.im * z1.im), y1[o].im + (d1.re * z1.im + d1.im * z1.re)};
+            }
         }
         if (t == r) {
-            const Cx<T> d0 = Dr[t], z0 = Z[t * NC + cc];
-            y0 = Cx<T>{y0.re + (d0.re * z0.re - d0.im * z0.im), y0.im + (d0.re * z0.im + d0.im * z0.re)};
+            const Cx<T> d0 = Dr[t];
+#pragma unroll
+            for (int o = 0; o < OPT; ++o) {
+                const Cx<T> z0 = Z[t * NC + cg + CG * o];
+                y0[o] = Cx<T>{y0[o].re + (d0.re * z0.re - d0.im * z0.im), y0[o].im + (d0.re * z0.im + d0.im * z0.re)};
+            }
         }
-        X[(r0 + r) * NC + cc] = Cx<T>{y0.re + y1.re, y0.im + y1.im};
+#pragma unroll
+        for (int o = 0; o < OPT; ++o)
+            X[(r0 + r) * NC + cg + CG * o] = Cx<T>{y0[o].re + y1[o].re, y0[o].im + y1[o].im};
         __syncthreads();  // block s of X is complete; Z is free again
     }
     for (int i = tid; i < kb * NC; i += 256) {
@@ -1532,6 +1556,13 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
     if (narrow)
         BB_CUDA(cudaFuncSetAttribute(trsm_narrow_kernel<T, WF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)trsm_narrow_smem<T, WF>(nb / W)));
+    // the side stream's solve of the remaining columns: the same kernel with 16 columns per CTA
+    // (two entries per thread in FP32), two CTAs per SM
+    constexpr int NCS = NC > 16 ? NC : 16;
+    const bool wide = blocked && trsm_narrow_smem<T, WF, NCS>(nb / W) <= 110 * 1024;
+    if (wide)
+        BB_CUDA(cudaFuncSetAttribute(trsm_narrow_kernel<T, WF, NCS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)trsm_narrow_smem<T, WF, NCS>(nb / W)));
     c->barrier.alloc(sizeof(unsigned) * 4096);
     BB_CUDA(cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
     // the unblocked U12 solve (used only when the blocked one does not apply)
@@ -1569,6 +1600,9 @@ template <typename T> static void lu_factor_t(beat_b200_ctx *c, int nb, int spli
         if (fused_stage) tc_stage_u_buffers(c, k, nb, &bhi, &blo, &bsc);
         if (crit && narrow)
             trsm_narrow_kernel<T, WF><<<(cols + NC - 1) / NC, 256, trsm_narrow_smem<T, WF>(nb / W), st>>>(
+                A, ld, k, nb / W, dinv + (size_t)(k / W) * W * W, c_lo, c_hi, bhi, blo, bsc, k + nb, split_terms);
+        else if (wide)
+            trsm_narrow_kernel<T, WF, NCS><<<(cols + NCS - 1) / NCS, 256, trsm_narrow_smem<T, WF, NCS>(nb / W), st>>>(
                 A, ld, k, nb / W, dinv + (size_t)(k / W) * W * W, c_lo, c_hi, bhi, blo, bsc, k + nb, split_terms);
         else if (blocked)
             trsm_blocked_kernel<T, WF><<<(cols + TB_COLS - 1) / TB_COLS, 256, tb_smem, st>>>(
