@@ -89,6 +89,12 @@ __device__ __forceinline__ void sincos_t(float x, float *s, float *c) {
     r = fmaf(-n, -1.7484555314695172e-07f, r);
     __sincosf(r, s, c);
 }
+// The same phase given in revolutions, t = x / (2 pi): t - rint(t) is exact,
+// so the reduction to [-1/2, 1/2] costs one rounding and one subtraction; the
+// rounding of t itself (the phase's relative 2^-24) stays the dominant error.
+__device__ __forceinline__ void sincos_rev(float t, float *s, float *c) {
+    __sincosf((t - rintf(t)) * 6.2831854820251465f, s, c);
+}
 __device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
 __device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
 
@@ -108,6 +114,11 @@ __device__ __forceinline__ void up2(F2 v, float &lo, float &hi) {
 __device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) {
     F2 d;
     asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ F2 mul2(F2 a, F2 b) {
+    F2 d;
+    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
     return d;
 }
 __device__ __forceinline__ F2 add2(F2 a, F2 b) {
@@ -605,6 +616,7 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
     }
 
     const T k = g.k, eta = g.eta;
+    const T kr = k * T(0.15915494309189535);  // k / (2 pi): the phase k r in revolutions
     const T inv4pi = T(0.07957747154594767);  // 1 / (4 pi)
     for (int p = tid; p < SYM_F * SYM_F; p += REG_THREADS) {
         const int ti = p / SYM_F, sj = p % SYM_F;  // a warp: one tau, every sigma
@@ -620,87 +632,108 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
         const T nsx = yn[sj], nsy = yn[SYM_F + sj], nsz = yn[2 * SYM_F + sj];
         const T k2n = eta * g.k2 * (ntx * nsx + nty * nsy + ntz * nsz);
         const T dtau = xp[ti], dsig = yp[sj];
-        T L1[9][2], L2[9][2], R1[3][2], U2[Q][2], cr = T(0), ci = T(0);
+        // r . n_tau = y . n_tau - x . n_tau is the same for every test point x
+        // on the flat face tau: one value per trial point
+        T ync[Q];
+#pragma unroll
+        for (int qs = 0; qs < Q; ++qs)
+            ync[qs] = yq[(qs * 3) * SYM_F + sj] * ntx + yq[(qs * 3 + 1) * SYM_F + sj] * nty +
+                      yq[(qs * 3 + 2) * SYM_F + sj] * ntz - dtau;
+        // L1 / L2: the two orders' 3 x 3 blocks; R1: order 1's right-hand-side
+        // 3-vector; TC_b: sum over both faces' points of w phi_b(y) G, which
+        // gives the Green sum of the curl term and order 2's right-hand side
+        T L1[9][2], L2[9][2], R1[3][2], TC[3][2];
 #pragma unroll
         for (int i = 0; i < 9; ++i) L1[i][0] = L1[i][1] = L2[i][0] = L2[i][1] = T(0);
 #pragma unroll
-        for (int i = 0; i < 3; ++i) R1[i][0] = R1[i][1] = T(0);
-#pragma unroll
-        for (int i = 0; i < Q; ++i) U2[i][0] = U2[i][1] = T(0);
+        for (int i = 0; i < 3; ++i) R1[i][0] = R1[i][1] = TC[i][0] = TC[i][1] = T(0);
 #pragma unroll 1
         for (int qt = 0; qt < Q; ++qt) {
             const T x0 = xq[(ti * Q + qt) * 3], x1 = xq[(ti * Q + qt) * 3 + 1], x2 = xq[(ti * Q + qt) * 3 + 2];
             const T wt = RuleRef<T>::w(RI, qt) * inv4pi;
             const T xns = dsig - (x0 * nsx + x1 * nsy + x2 * nsz);  // r . n_sigma for every y on sigma
-            // order 1 sums over the trial points S_b, order 2 sums P_b, the green
-            // sum G and -W (W = sum of c dG/dr), each a packed (re, im) pair
-            F2 S0 = 0, S1 = 0, S2 = 0, P0 = 0, P1 = 0, P2 = 0, G2 = 0, NW = 0;
-            const T nxns = -xns;
+            // Per trial point (the test point's weight wt applied below):
+            //   g = w_s exp(ikr) / r,  h = g (ik - 1/r) / r  (dG/dr / r),
+            //   C_b += phi_b(y) g,  H_b += phi_b(y) h,  P_b += phi_b(y) (r . n_tau) h.
+            // Order 1's kernel value -g' (r . n_sigma) / r - i k2n g sums to
+            // -xns H_b - i k2n C_b, order 2's (r . n_tau) g' / r - i k2n g to
+            // P_b - i k2n C_b; each sum a packed (re, im) pair.
+            F2 C0 = 0, C1 = 0, C2 = 0, H0 = 0, H1 = 0, H2 = 0, P0 = 0, P1 = 0, P2 = 0;
 #pragma unroll
             for (int qs = 0; qs < Q; ++qs) {
-                const T y0 = yq[(qs * 3) * SYM_F + sj], y1 = yq[(qs * 3 + 1) * SYM_F + sj],
-                        y2 = yq[(qs * 3 + 2) * SYM_F + sj];
-                const T rx = y0 - x0, ry = y1 - x1, rz = y2 - x2;
+                const T rx = yq[(qs * 3) * SYM_F + sj] - x0, ry = yq[(qs * 3 + 1) * SYM_F + sj] - x1,
+                        rz = yq[(qs * 3 + 2) * SYM_F + sj] - x2;
                 const T r2 = rx * rx + ry * ry + rz * rz;
                 const T ir = rsqrt_t(r2);
                 T sn_, cs_;
-                sincos_t(k * (r2 * ir), &sn_, &cs_);
-                const T scl = ir * (wt * RuleRef<T>::w(RI, qs));
+                sincos_rev(kr * (r2 * ir), &sn_, &cs_);
+                const T scl = ir * RuleRef<T>::w(RI, qs);
                 const T gr = cs_ * scl, gi = sn_ * scl;
-                const T gsr = -gr * ir - gi * k;
-                const T gsi = gr * k - gi * ir;
-                const T na = nxns * ir;                                        // -r . n_sigma / r
-                const T nc = ((y0 * ntx + y1 * nty + y2 * ntz) - dtau) * ir;  // r . n_tau / r
-                const F2 g2 = pk2(gr, gi), gs = pk2(gsr, gsi);
-                const F2 kk = pk2(k2n * gi, -(k2n * gr));
-                const F2 l1 = fma2(pk2(na, na), gs, kk);  // order 1: -i k2n g - grad*dn_s
-                const F2 l2 = fma2(pk2(nc, nc), gs, kk);  // order 2: dn_s = c
-                G2 = add2(G2, g2);
-                NW = fma2(pk2(nc, nc), gs, NW);
+                const T hr = (-gr * ir - gi * k) * ir;
+                const T hi = (gr * k - gi * ir) * ir;
+                const F2 g2 = pk2(gr, gi), h2 = pk2(hr, hi);
                 const F2 b0 = rule_b2(RI, qs, 0), b1 = rule_b2(RI, qs, 1), b2 = rule_b2(RI, qs, 2);
-                S0 = fma2(b0, l1, S0);
-                S1 = fma2(b1, l1, S1);
-                S2 = fma2(b2, l1, S2);
-                P0 = fma2(b0, l2, P0);
-                P1 = fma2(b1, l2, P1);
-                P2 = fma2(b2, l2, P2);
-                const T ea = -eta * na;
-                U2[qs][0] += ea * gsi - gr;  // -g - i eta grad*dn_t with dn_t = a
-                U2[qs][1] -= ea * gsr + gi;
+                C0 = fma2(b0, g2, C0);
+                C1 = fma2(b1, g2, C1);
+                C2 = fma2(b2, g2, C2);
+                H0 = fma2(b0, h2, H0);
+                H1 = fma2(b1, h2, H1);
+                H2 = fma2(b2, h2, H2);
+                const F2 p2 = mul2(pk2(ync[qs], ync[qs]), h2);
+                P0 = fma2(b0, p2, P0);
+                P1 = fma2(b1, p2, P1);
+                P2 = fma2(b2, p2, P2);
             }
-            T S0r, S0i, S1r, S1i, S2r, S2i, P0r, P0i, P1r, P1i, P2r, P2i, Gr, Gi, Wr, Wi;
-            up2(S0, S0r, S0i);
-            up2(S1, S1r, S1i);
-            up2(S2, S2r, S2i);
-            up2(P0, P0r, P0i);
-            up2(P1, P1r, P1i);
-            up2(P2, P2r, P2i);
-            up2(G2, Gr, Gi);
-            up2(NW, Wr, Wi);
-            Wr = -Wr;
-            Wi = -Wi;
-            const T Ur = -Gr + eta * Wi, Ui = -Gi - eta * Wr;
-            cr += Gr;
-            ci += Gi;
+            T Cr[3], Ci[3], Hr[3], Hi[3], Pr[3], Pi[3];
+            up2(C0, Cr[0], Ci[0]);
+            up2(C1, Cr[1], Ci[1]);
+            up2(C2, Cr[2], Ci[2]);
+            up2(H0, Hr[0], Hi[0]);
+            up2(H1, Hr[1], Hi[1]);
+            up2(H2, Hr[2], Hi[2]);
+            up2(P0, Pr[0], Pi[0]);
+            up2(P1, Pr[1], Pi[1]);
+            up2(P2, Pr[2], Pi[2]);
+            // order 1's right-hand-side value -G + i eta W, W = sum (r . n_tau) g' / r
+            const T Gr = Cr[0] + Cr[1] + Cr[2], Gi = Ci[0] + Ci[1] + Ci[2];
+            const T Wr = Pr[0] + Pr[1] + Pr[2], Wi = Pi[0] + Pi[1] + Pi[2];
+            const T Ur = -Gr - eta * Wi, Ui = -Gi + eta * Wr;
+            T Sr[3], Si[3];
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                Sr[b] = -xns * Hr[b] + k2n * Ci[b];
+                Si[b] = -xns * Hi[b] - k2n * Cr[b];
+                Pr[b] += k2n * Ci[b];
+                Pi[b] -= k2n * Cr[b];
+                TC[b][0] += wt * Cr[b];
+                TC[b][1] += wt * Ci[b];
+            }
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-                const T ba = RuleRef<T>::b(RI, qt, a);
-                L1[3 * a + 0][0] += ba * S0r;
-                L1[3 * a + 0][1] += ba * S0i;
-                L1[3 * a + 1][0] += ba * S1r;
-                L1[3 * a + 1][1] += ba * S1i;
-                L1[3 * a + 2][0] += ba * S2r;
-                L1[3 * a + 2][1] += ba * S2i;
+                const T ba = RuleRef<T>::b(RI, qt, a) * wt;
+#pragma unroll
+                for (int b = 0; b < 3; ++b) {
+                    L1[3 * a + b][0] += ba * Sr[b];
+                    L1[3 * a + b][1] += ba * Si[b];
+                    // order 2: row = test vertex of sigma (b), column = trial vertex of tau (a)
+                    L2[3 * b + a][0] += ba * Pr[b];
+                    L2[3 * b + a][1] += ba * Pi[b];
+                }
                 R1[a][0] += ba * Ur;
                 R1[a][1] += ba * Ui;
-                // order 2: row = test vertex of sigma (P index), column = trial vertex of tau (a)
-                L2[0 * 3 + a][0] += ba * P0r;
-                L2[0 * 3 + a][1] += ba * P0i;
-                L2[1 * 3 + a][0] += ba * P1r;
-                L2[1 * 3 + a][1] += ba * P1i;
-                L2[2 * 3 + a][0] += ba * P2r;
-                L2[2 * 3 + a][1] += ba * P2i;
             }
+        }
+        // Order 2's right-hand-side value at (x, y) is -(1 + eta k2n) g + i eta
+        // times order 1's kernel value, so its sum against phi_b(y) is
+        // -(1 + eta k2n) TC_b + i eta sum_a L1[a][b] (the test basis sums to 1).
+        const T cr = TC[0][0] + TC[1][0] + TC[2][0], ci = TC[0][1] + TC[1][1] + TC[2][1];
+        const T ce = -(T(1) + eta * k2n);
+        T R2[3][2];
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const T lr = L1[b][0] + L1[3 + b][0] + L1[6 + b][0], li = L1[b][1] + L1[3 + b][1] + L1[6 + b][1];
+            R2[b][0] = ce * TC[b][0] - eta * li;
+            R2[b][1] = ce * TC[b][1] + eta * lr;
         }
         // hypersingular curl term: eta * sum(g w) * curl_test . curl_trial (same sum for both orders)
         const T ccr = -eta * ci, cci = eta * cr;
@@ -733,17 +766,10 @@ __global__ void __launch_bounds__(REG_THREADS, 2) sym_pairs_kernel(RegArgs<float
             val[13] = R1[a][1] * jac;
             // tau's other elements in flight on other warps may share vertex a
             batch_add<14>(acc_re, off, val);
-            T r2r = T(0), r2i = T(0);
-#pragma unroll
-            for (int qs = 0; qs < Q; ++qs) {
-                const T bq = RuleRef<T>::b(RI, qs, a);
-                r2r += bq * U2[qs][0];
-                r2i += bq * U2[qs][1];
-            }
             // (sigma slot a, face tau) belongs to this element pair alone: a plain store
             const int e2 = SYM_D2 + (a * SYM_F + sj) * SYM_BS + ti;
-            acc_re[e2] = r2r * jac;
-            acc_im[e2] = r2i * jac;
+            acc_re[e2] = R2[a][0] * jac;
+            acc_im[e2] = R2[a][1] * jac;
         }
     }
     __syncthreads();
