@@ -97,6 +97,17 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def wait_first_sample(self, limit_s: float = 3.0):
+        """Blocks until nvidia-smi has written its first row (or limit_s has
+        passed), so that its start-up (driver queries, NVML set-up) falls
+        before the timed region rather than inside it."""
+        t0 = time.time()
+        while self.proc is not None and time.time() - t0 < limit_s:
+            self.fh.flush()
+            if os.path.getsize(self.path) > 0:
+                return
+            time.sleep(0.02)
+
     def __exit__(self, *exc):
         if self.proc is not None:
             self.proc.terminate()
@@ -332,6 +343,7 @@ def timed(stream, fn, clocks_device=None):
     sampler = ClockSampler(clocks_device) if clocks_device is not None else None
     if sampler:
         sampler.__enter__()
+        sampler.wait_first_sample()
     try:
         torch.cuda.synchronize()
         e0.record(stream)
@@ -689,11 +701,11 @@ def measured_peaks():
 
 
 # DRAM traffic of sym_pairs_kernel<6> (the mixed form's element-pair kernel) measured by ncu on
-# the F = 5,120 icosphere: 158.99 MB read + 119.64 MB written per launch, against an algorithmic
+# the F = 5,120 icosphere: 158.83 MB read + 117.60 MB written per launch, against an algorithmic
 # output of A (N^2 c64) + B (N x F c64) = 157.4 MB at N = 2,562.  Traffic grows with the output
 # written (the zeroed A and B are read back by the red.global.add flush), so a launch on another
 # mesh is scaled by its output bytes.
-SYM_TRAFFIC_F5120 = {"bytes": 158.986496e6 + 119.639296e6, "output_bytes": 2562 * 2562 * 8 + 2562 * 5120 * 8}
+SYM_TRAFFIC_F5120 = {"bytes": 158.8288e6 + 117.59616e6, "output_bytes": 2562 * 2562 * 8 + 2562 * 5120 * 8}
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # FP32 FMA lanes x 2 flops x max SM clock
 
 
