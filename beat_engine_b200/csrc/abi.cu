@@ -886,7 +886,6 @@ int32_t beat_b200_adjoint_shape(beat_b200_ctx *c, double k_signed, int32_t M, co
         BB_REQUIRE(dirs && p && q && g && gX_out, BEAT_B200_INVALID_ARG, "adjoint: null pointer");
         BB_REQUIRE(c->F > 0, BEAT_B200_STATE, "no mesh: call beat_b200_set_mesh first");
         BB_REQUIRE(M >= 1 && R >= 1, BEAT_B200_INVALID_ARG, "adjoint: M and R must be >= 1");
-        BB_REQUIRE(c->nimg == 0, BEAT_B200_STATE, "shape gradient: symmetry images are not supported");
         const beat_b200_opts o = resolve_opts(opts);
         const int N = c->V, F = c->F;
         const size_t np = (size_t)N * R, ng = (size_t)M * R, nw = (size_t)F * R;

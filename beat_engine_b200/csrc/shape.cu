@@ -28,7 +28,22 @@
 // pass maps the normal, curls and area to the vertices by forward-mode
 // derivatives of the face geometry (normal = e1 x e2 / |e1 x e2|, area, and
 // curl_i = n x grad phi_i through the Gram inverse, as the assembly's set-up
-// computes them).  FP64 throughout; symmetry images are not supported.
+// computes them).  FP64 throughout.
+//
+// Symmetry images.  Each image pass of the assembly integrates every
+// (test, reflected trial) element pair by the regular rule, touching or not;
+// the reflected trial element has its points and normal times the image's
+// signs s and its curls times det s.  The touching image pairs then add the
+// Duffy integral minus that regular one.  The reverse passes repeat both on the
+// same reflected geometry, and map the trial face's adjoints back through the
+// reflection (positions and normal times s, curls times det s: s is its own
+// inverse).  The far field's image sources (reflected positions and normals,
+// the same densities) are mapped back the same way.  The rows of vertices on a
+// symmetry plane are weighted after assembly, so every test-vertex row of the
+// adjoint z is taken times that weight.  In the x and xy modes a vertex on a
+// symmetry plane must stay on it, so its gradient's component normal to that
+// plane is returned as zero (the ground mode's plane has no weights and no
+// such constraint).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -169,21 +184,32 @@ __device__ __forceinline__ double2 curl_term(const double2 (&W)[3][3], const dou
     return S2;
 }
 
-// adds a pair's adjoints (times jac) to the two face records
+// The trial element of an image pass is reflected: positions and normal
+// times s, curls times det s (on = 0: the mesh itself, s = 1, det = 1).
+struct ShapeImage {
+    int on;
+    double s[3];
+    double det;
+};
+__host__ __device__ inline ShapeImage no_image() { return ShapeImage{0, {1.0, 1.0, 1.0}, 1.0}; }
+
+// adds a pair's adjoints (times jac) to the two face records; the trial
+// face's adjoints, taken with respect to its reflected copy im, are mapped
+// back to the face itself
 __device__ __forceinline__ void pair_records(const PairAdj &acc, const double2 (&W)[3][3], const double *ct,
                                              const double *cs, double jac, double at, double as, double eta,
-                                             double *rt, double *rs) {
+                                             double *rt, double *rs, const ShapeImage &im) {
 #pragma unroll
     for (int v = 0; v < 3; ++v)
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             atomicAdd(&rt[SG_V + 3 * v + d], jac * acc.xbar[v][d]);
-            atomicAdd(&rs[SG_V + 3 * v + d], jac * acc.ybar[v][d]);
+            atomicAdd(&rs[SG_V + 3 * v + d], jac * acc.ybar[v][d] * im.s[d]);
         }
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         atomicAdd(&rt[SG_N + d], jac * acc.ntbar[d]);
-        atomicAdd(&rs[SG_N + d], jac * acc.nsbar[d]);
+        atomicAdd(&rs[SG_N + d], jac * acc.nsbar[d] * im.s[d]);
     }
     // curls: d phi / d curl_t[i] = jac Gamma sum_j W_ij curl_s[j], Gamma = eta sum w G
     const double2 gam = times_i_eta(acc.gsum, eta);
@@ -198,7 +224,7 @@ __device__ __forceinline__ void pair_records(const PairAdj &acc, const double2 (
                 ss = cadd(ss, cscale(W[j][i], ct[3 * j + d]));
             }
             atomicAdd(&rt[SG_C + 3 * i + d], jac * cmul(gam, st).x);
-            atomicAdd(&rs[SG_C + 3 * i + d], jac * cmul(gam, ss).x);
+            atomicAdd(&rs[SG_C + 3 * i + d], jac * cmul(gam, ss).x * im.det * im.s[d]);
         }
     // jac = 4 A_t A_s
     atomicAdd(&rt[SG_A], jac * acc.phi.x / at);
@@ -214,6 +240,7 @@ struct ShapeTileArgs {
     int N, F, R, r0;
     double k, eta;
     ShapeRule rule;
+    ShapeImage img;                             // the pass's reflection of the trial elements
     double *rec;                                // F x SG_REC
 };
 
@@ -268,14 +295,20 @@ __global__ void __launch_bounds__(SG_THREADS, 1) shape_pairs_kernel(ShapeTileArg
     for (int i = tid; i < ns; i += SG_THREADS) sa[i] = g.area[s0 + i];
     for (int i = tid; i < (SG_TT + SG_TS) * SG_REC; i += SG_THREADS) rt[i] = 0.0;
     __syncthreads();
+    if (g.img.on) {  // an image pass: the trial tile reflected
+        for (int i = tid; i < ns * Q * 3; i += SG_THREADS) sq[i] *= g.img.s[i % 3];
+        for (int i = tid; i < ns * 3; i += SG_THREADS) sn[i] *= g.img.s[i % 3];
+        for (int i = tid; i < ns * 9; i += SG_THREADS) sc[i] *= g.img.det * g.img.s[i % 3];
+        __syncthreads();
+    }
 
     for (int pr = tid; pr < SG_TT * SG_TS; pr += SG_THREADS) {
         const int tl = pr / SG_TS, sl = pr % SG_TS;
         if (tl >= nt || sl >= ns) continue;
         const int *tv = tgv + 3 * tl, *sv = sgv + 3 * sl;
-        if (tv[0] == sv[0] || tv[0] == sv[1] || tv[0] == sv[2] || tv[1] == sv[0] || tv[1] == sv[1] ||
-            tv[1] == sv[2] || tv[2] == sv[0] || tv[2] == sv[1] || tv[2] == sv[2])
-            continue;  // touching: the Duffy pass
+        if (!g.img.on && (tv[0] == sv[0] || tv[0] == sv[1] || tv[0] == sv[2] || tv[1] == sv[0] || tv[1] == sv[1] ||
+                          tv[1] == sv[2] || tv[2] == sv[0] || tv[2] == sv[1] || tv[2] == sv[2]))
+            continue;  // touching: the Duffy pass (an image pass keeps every pair, as the assembly does)
         double2 W[3][3], U[3];
         pair_weights(zt + tlv[3 * tl] * SG_RC, zt + tlv[3 * tl + 1] * SG_RC, zt + tlv[3 * tl + 2] * SG_RC,
                      ps + slv[3 * sl] * SG_RC, ps + slv[3 * sl + 1] * SG_RC, ps + slv[3 * sl + 2] * SG_RC,
@@ -299,7 +332,7 @@ __global__ void __launch_bounds__(SG_THREADS, 1) shape_pairs_kernel(ShapeTileArg
             }
         }
         const double jac = 4.0 * ta[tl] * sa[sl];
-        pair_records(acc, W, ct, cs, jac, ta[tl], sa[sl], g.eta, rt + tl * SG_REC, rs + sl * SG_REC);
+        pair_records(acc, W, ct, cs, jac, ta[tl], sa[sl], g.eta, rt + tl * SG_REC, rs + sl * SG_REC, g.img);
     }
     __syncthreads();
     for (int i = tid; i < nt * SG_REC; i += SG_THREADS) {
@@ -320,6 +353,9 @@ template <int Q> static size_t shape_pairs_smem() {
 
 struct ShapeSingArgs {
     const int *test, *trial, *rule;
+    const int *img;           // touching image pairs: the image of each pair (NULL: the mesh's own pairs)
+    ShapeImage xf[3];         // the images' reflections
+    ShapeRule reg;            // the regular rule an image pass applied to the pair
     const int *rule_start;
     const double *rule_data;  // per point: test xi, eta, trial xi, eta, weight
     const double *verts, *normals, *curls, *areas;
@@ -332,12 +368,17 @@ struct ShapeSingArgs {
 };
 
 // touching pairs: one warp per pair, Duffy points over the lanes, then the
-// lanes' adjoints summed and added to the two face records
+// lanes' adjoints summed and added to the two face records.  A touching image
+// pair (test t, trial s reflected) takes the Duffy points on the reflected
+// trial element minus the regular rule's points there (the part the image
+// pass integrated), and maps the trial face's adjoints back through the
+// reflection.
 __global__ void __launch_bounds__(256) shape_singular_kernel(ShapeSingArgs g) {
     const int lane = threadIdx.x & 31;
     const int64_t pair = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     if (pair >= g.npairs) return;
     const int t = g.test[pair], s = g.trial[pair], ru = g.rule[pair];
+    const ShapeImage im = g.img ? g.xf[g.img[pair]] : no_image();
     const int *ft = g.faces + 3 * t, *fs = g.faces + 3 * s;
     double tv[3][3], sv[3][3];
 #pragma unroll
@@ -345,10 +386,10 @@ __global__ void __launch_bounds__(256) shape_singular_kernel(ShapeSingArgs g) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             tv[a][c] = g.verts[3 * ft[a] + c];
-            sv[a][c] = g.verts[3 * fs[a] + c];
+            sv[a][c] = im.s[c] * g.verts[3 * fs[a] + c];
         }
     const double nT[3] = {g.normals[3 * t], g.normals[3 * t + 1], g.normals[3 * t + 2]};
-    const double nS[3] = {g.normals[3 * s], g.normals[3 * s + 1], g.normals[3 * s + 2]};
+    const double nS[3] = {im.s[0] * g.normals[3 * s], im.s[1] * g.normals[3 * s + 1], im.s[2] * g.normals[3 * s + 2]};
     const double nn = nT[0] * nS[0] + nT[1] * nS[1] + nT[2] * nS[2];
     double2 W[3][3], U[3];
 #pragma unroll
@@ -371,7 +412,10 @@ __global__ void __launch_bounds__(256) shape_singular_kernel(ShapeSingArgs g) {
             }
         }
     }
-    const double *ct = g.curls + 9 * t, *cs = g.curls + 9 * s;
+    const double *ct = g.curls + 9 * t;
+    double cs[9];  // the trial curls, reflected with the element
+#pragma unroll
+    for (int i = 0; i < 9; ++i) cs[i] = im.det * im.s[i % 3] * g.curls[9 * s + i];
     const double2 S2 = curl_term(W, ct, cs);
     PairAdj acc;
     pair_adj_zero(acc);
@@ -386,6 +430,20 @@ __global__ void __launch_bounds__(256) shape_singular_kernel(ShapeSingArgs g) {
             y[c] = bs[0] * sv[0][c] + bs[1] * sv[1][c] + bs[2] * sv[2][c];
         }
         reverse_point(x, y, bt, bs, d[4], nT, nS, nn, g.k, g.eta, W, U, S2, acc);
+    }
+    if (g.img) {  // minus the regular rule's points, which the image pass added
+        for (int pq = lane; pq < g.reg.n * g.reg.n; pq += 32) {
+            const int qt = pq / g.reg.n, qs = pq % g.reg.n;
+            const double bt[3] = {g.reg.b[qt][0], g.reg.b[qt][1], g.reg.b[qt][2]};
+            const double bs[3] = {g.reg.b[qs][0], g.reg.b[qs][1], g.reg.b[qs][2]};
+            double x[3], y[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                x[c] = bt[0] * tv[0][c] + bt[1] * tv[1][c] + bt[2] * tv[2][c];
+                y[c] = bs[0] * sv[0][c] + bs[1] * sv[1][c] + bs[2] * sv[2][c];
+            }
+            reverse_point(x, y, bt, bs, -g.reg.w[qt] * g.reg.w[qs], nT, nS, nn, g.k, g.eta, W, U, S2, acc);
+        }
     }
     // sum over the lanes
 #pragma unroll
@@ -410,7 +468,7 @@ __global__ void __launch_bounds__(256) shape_singular_kernel(ShapeSingArgs g) {
     if (lane == 0) {
         const double at = g.areas[t], as = g.areas[s];
         pair_records(acc, W, ct, cs, 4.0 * at * as, at, as, g.eta, g.rec + (size_t)t * SG_REC,
-                     g.rec + (size_t)s * SG_REC);
+                     g.rec + (size_t)s * SG_REC, im);
     }
 }
 
@@ -443,21 +501,40 @@ __global__ void shape_identity_kernel(const int *faces, const double *areas, int
     atomicAdd(&rec[(size_t)f * SG_REC + SG_A], phi.x);
 }
 
-// far field: p_inf(d) = sum_src w e(d) [(-ik)(d . n) p_src - q], e = exp(-ik d.y) / (4 pi)
+// the mesh itself and its symmetry images (signs of x, y, z per copy)
+struct ShapeCopies {
+    int n;
+    double s[4][3];
+};
+
+// far field: p_inf(d) = sum_src w e(d) [(-ik)(d . n) p_src - q], e = exp(-ik d.y) / (4 pi),
+// the sources being the mesh's and, with symmetry images, their reflections
+// (position and normal times the signs, the same densities)
 __global__ void shape_farfield_kernel(const double *qpts, const double *normals, const double *areas,
                                       const int *faces, int F, int Q, ShapeRule rule, int N, const double *dirs,
                                       int M, const double2 *g, int R, double k, const double2 *p, const double2 *q,
-                                      double *rec) {
+                                      ShapeCopies copies, double *rec) {
     const int sidx = blockIdx.x * blockDim.x + threadIdx.x;
     if (sidx >= F * Q) return;
     const int f = sidx / Q, qi = sidx % Q;
     const double w = rule.w[qi] * 2.0 * areas[f];
-    const double y[3] = {qpts[3 * (size_t)sidx], qpts[3 * (size_t)sidx + 1], qpts[3 * (size_t)sidx + 2]};
-    const double n[3] = {normals[3 * f], normals[3 * f + 1], normals[3 * f + 2]};
+    const double y0[3] = {qpts[3 * (size_t)sidx], qpts[3 * (size_t)sidx + 1], qpts[3 * (size_t)sidx + 2]};
+    const double n0[3] = {normals[3 * f], normals[3 * f + 1], normals[3 * f + 2]};
     const int *fc = faces + 3 * f;
     double ybar[3] = {0, 0, 0}, nbar[3] = {0, 0, 0};
     double2 phi = make_double2(0.0, 0.0);
-    for (int m = 0; m < M; ++m) {
+    for (int mc = 0; mc < M * copies.n; ++mc) {
+        const int m = mc / copies.n, ix = mc % copies.n;
+        double sg[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {  // copies.s[ix] by selects (no local-memory copy of the parameter)
+            sg[c] = copies.s[0][c];
+#pragma unroll
+            for (int j = 1; j < 4; ++j)
+                if (ix == j) sg[c] = copies.s[j][c];
+        }
+        const double y[3] = {sg[0] * y0[0], sg[1] * y0[1], sg[2] * y0[2]};
+        const double n[3] = {sg[0] * n0[0], sg[1] * n0[1], sg[2] * n0[2]};
         double d[3] = {dirs[3 * m], dirs[3 * m + 1], dirs[3 * m + 2]};
         const double dl = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
         d[0] /= dl;
@@ -484,9 +561,9 @@ __global__ void shape_farfield_kernel(const double *qpts, const double *normals,
         // d/dy: e (-ik d) h;  d/dn: e (-ik) hp d
         const double dy = cmul(make_double2(0.0, -k), eh).x;
         const double dnr = cmul(make_double2(0.0, -k), cmul(e, hp)).x;
-        for (int c = 0; c < 3; ++c) {
-            ybar[c] += dy * d[c];
-            nbar[c] += dnr * d[c];
+        for (int c = 0; c < 3; ++c) {  // back through the reflection
+            ybar[c] += dy * d[c] * sg[c];
+            nbar[c] += dnr * d[c] * sg[c];
         }
     }
     double *rf = rec + (size_t)f * SG_REC;
@@ -557,6 +634,28 @@ __global__ void shape_vertices_kernel(const double *verts, const int *faces, int
         }
 }
 
+// z with the rows of the vertices on a symmetry plane times their orbit
+// weights (the weights the assembly gives those rows of A and B); zw holds a
+// copy of z, and the weighted rows are rewritten from z
+__global__ void shape_scale_rows_kernel(const double2 *z, double2 *zw, int N, int R, const int *wv,
+                                        const double *ww, int nw) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)nw * R) return;
+    const int v = (int)(i % nw), r = (int)(i / nw);
+    const size_t e = (size_t)r * N + wv[v];
+    zw[e] = make_double2(z[e].x * ww[v], z[e].y * ww[v]);
+}
+
+// a vertex on a symmetry plane stays on it: its gradient's component normal
+// to that plane (coordinate exactly 0 after the set-up's snapping) is zero
+__global__ void shape_plane_project_kernel(const double *verts, const int *wv, int nw, int axes, double *gX) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nw) return;
+    const int u = wv[v];
+    for (int a = 0; a < 3; ++a)
+        if ((axes >> a & 1) && verts[3 * (size_t)u + a] == 0.0) gX[3 * (size_t)u + a] = 0.0;
+}
+
 static ShapeRule shape_rule(const std::vector<double> &pts, const std::vector<double> &w) {
     ShapeRule r{};
     r.n = (int)w.size();
@@ -581,18 +680,37 @@ template <int Q> static void launch_shape_pairs(beat_b200_ctx *c, ShapeTileArgs 
 void shape_gradient(beat_b200_ctx *c, double k, double eta, int M, const double *dirs_dev, int R,
                     const double *p_dev, const double *q_dev, const double *g_dev, const double *z_dev,
                     double *gX_dev) {
-    BB_REQUIRE(c->nimg == 0, BEAT_B200_STATE, "shape gradient: symmetry images are not supported");
     BB_REQUIRE(c->test_tiles.tile_faces <= SG_TT && c->test_tiles.tile_verts <= SG_VT &&
                    c->trial_tiles.tile_faces <= SG_TS && c->trial_tiles.tile_verts <= SG_VS,
                BEAT_B200_STATE, "shape gradient: unexpected tiling");
     const int N = c->V, F = c->F, Q = c->Q;
-    DevBuf &rec = c->ws.grad;
-    rec.alloc(sizeof(double) * (size_t)F * SG_REC);
-    BB_CUDA(cudaMemsetAsync(rec.p, 0, sizeof(double) * (size_t)F * SG_REC, c->stream));
+    // the face records, then (with weighted rows) the row-weighted copy of z
+    const size_t rec_bytes = sizeof(double) * (size_t)F * SG_REC;
+    const size_t zw_off = (rec_bytes + 255) / 256 * 256;
+    const bool weighted = c->nweighted > 0;
+    DevBuf &buf = c->ws.grad;
+    buf.alloc(zw_off + (weighted ? sizeof(double2) * (size_t)N * R : 0));
+    double *rec = buf.as<double>();
+    BB_CUDA(cudaMemsetAsync(rec, 0, rec_bytes, c->stream));
     BB_CUDA(cudaMemsetAsync(gX_dev, 0, sizeof(double) * 3 * (size_t)N, c->stream));
     const ShapeRule rule = shape_rule(c->rule_pts, c->rule_w);
-    const double2 *z = reinterpret_cast<const double2 *>(z_dev), *p = reinterpret_cast<const double2 *>(p_dev),
-                  *q = reinterpret_cast<const double2 *>(q_dev);
+    const double2 *p = reinterpret_cast<const double2 *>(p_dev), *q = reinterpret_cast<const double2 *>(q_dev);
+    const double2 *z = reinterpret_cast<const double2 *>(z_dev);
+    if (weighted) {
+        double2 *zw = reinterpret_cast<double2 *>(static_cast<char *>(buf.p) + zw_off);
+        BB_CUDA(cudaMemcpyAsync(zw, z, sizeof(double2) * (size_t)N * R, cudaMemcpyDeviceToDevice, c->stream));
+        const int64_t n = (int64_t)c->nweighted * R;
+        shape_scale_rows_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
+            z, zw, N, R, c->rw_vert.as<int>(), c->rw_weight.as<double>(), c->nweighted);
+        BB_CUDA(cudaGetLastError());
+        z = zw;
+    }
+    ShapeImage xf[3] = {no_image(), no_image(), no_image()};
+    for (int ix = 0; ix < c->nimg; ++ix) {
+        xf[ix].on = 1;
+        for (int i = 0; i < 3; ++i) xf[ix].s[i] = c->img_sign[ix][i];
+        xf[ix].det = c->img_det[ix];
+    }
     ShapeTileArgs a;
     a.qpts = c->pos_qpts64.as<double>();
     a.normal = c->pos_normal64.as<double>();
@@ -618,47 +736,76 @@ void shape_gradient(beat_b200_ctx *c, double k, double eta, int M, const double 
     a.k = k;
     a.eta = eta;
     a.rule = rule;
-    a.rec = rec.as<double>();
-    switch (Q) {
-        case 1: launch_shape_pairs<1>(c, a); break;
-        case 3: launch_shape_pairs<3>(c, a); break;
-        default: launch_shape_pairs<6>(c, a); break;
+    a.rec = rec;
+    for (int img = -1; img < c->nimg; ++img) {  // the mesh itself, then one pass per symmetry image
+        a.img = img < 0 ? no_image() : xf[img];
+        switch (Q) {
+            case 1: launch_shape_pairs<1>(c, a); break;
+            case 3: launch_shape_pairs<3>(c, a); break;
+            default: launch_shape_pairs<6>(c, a); break;
+        }
     }
+    ShapeSingArgs s;
+    s.rule_start = c->rule_start.as<int>();
+    s.rule_data = c->rule_data.as<double>();
+    s.verts = c->d_verts.as<double>();
+    s.normals = c->d_normals.as<double>();
+    s.curls = c->d_curls.as<double>();
+    s.areas = c->d_areas.as<double>();
+    s.faces = c->d_faces.as<int>();
+    s.z = z;
+    s.p = p;
+    s.q = q;
+    s.N = N;
+    s.F = F;
+    s.R = R;
+    s.k = k;
+    s.eta = eta;
+    s.rec = rec;
+    s.reg = rule;
+    for (int ix = 0; ix < 3; ++ix) s.xf[ix] = xf[ix];
     if (c->npairs > 0) {
-        ShapeSingArgs s;
         s.test = c->sp_test.as<int>();
         s.trial = c->sp_trial.as<int>();
         s.rule = c->sp_rule.as<int>();
-        s.rule_start = c->rule_start.as<int>();
-        s.rule_data = c->rule_data.as<double>();
-        s.verts = c->d_verts.as<double>();
-        s.normals = c->d_normals.as<double>();
-        s.curls = c->d_curls.as<double>();
-        s.areas = c->d_areas.as<double>();
-        s.faces = c->d_faces.as<int>();
-        s.z = z;
-        s.p = p;
-        s.q = q;
-        s.N = N;
-        s.F = F;
-        s.R = R;
+        s.img = nullptr;
         s.npairs = c->npairs;
-        s.k = k;
-        s.eta = eta;
-        s.rec = rec.as<double>();
         shape_singular_kernel<<<(unsigned)((c->npairs + 7) / 8), 256, 0, c->stream>>>(s);
         BB_CUDA(cudaGetLastError());
     }
+    if (c->nimg_pairs > 0) {  // touching image pairs: Duffy minus the image pass's regular rule
+        s.test = c->ip_test.as<int>();
+        s.trial = c->ip_trial.as<int>();
+        s.rule = c->ip_rule.as<int>();
+        s.img = c->ip_img.as<int>();
+        s.npairs = c->nimg_pairs;
+        shape_singular_kernel<<<(unsigned)((c->nimg_pairs + 7) / 8), 256, 0, c->stream>>>(s);
+        BB_CUDA(cudaGetLastError());
+    }
     shape_identity_kernel<<<(F + 255) / 256, 256, 0, c->stream>>>(c->d_faces.as<int>(), c->d_areas.as<double>(), F,
-                                                                   N, R, rule, eta, z, p, q, rec.as<double>());
+                                                                   N, R, rule, eta, z, p, q, rec);
     BB_CUDA(cudaGetLastError());
+    ShapeCopies copies;
+    copies.n = 1 + c->nimg;
+    for (int i = 0; i < 3; ++i) copies.s[0][i] = 1.0;
+    for (int ix = 0; ix < c->nimg; ++ix)
+        for (int i = 0; i < 3; ++i) copies.s[1 + ix][i] = c->img_sign[ix][i];
     shape_farfield_kernel<<<(F * Q + 127) / 128, 128, 0, c->stream>>>(
         c->d_qpts.as<double>(), c->d_normals.as<double>(), c->d_areas.as<double>(), c->d_faces.as<int>(), F, Q,
-        rule, N, dirs_dev, M, reinterpret_cast<const double2 *>(g_dev), R, k, p, q, rec.as<double>());
+        rule, N, dirs_dev, M, reinterpret_cast<const double2 *>(g_dev), R, k, p, q, copies, rec);
     BB_CUDA(cudaGetLastError());
     shape_vertices_kernel<<<(F + 127) / 128, 128, 0, c->stream>>>(c->d_verts.as<double>(), c->d_faces.as<int>(), F,
-                                                                  rec.as<double>(), gX_dev);
+                                                                  rec, gX_dev);
     BB_CUDA(cudaGetLastError());
+    if (weighted) {  // the planes are those the images reflect across (a sign of -1)
+        int axes = 0;
+        for (int ix = 0; ix < c->nimg; ++ix)
+            for (int i = 0; i < 3; ++i)
+                if (c->img_sign[ix][i] < 0) axes |= 1 << i;
+        shape_plane_project_kernel<<<(c->nweighted + 127) / 128, 128, 0, c->stream>>>(
+            c->d_verts.as<double>(), c->rw_vert.as<int>(), c->nweighted, axes, gX_dev);
+        BB_CUDA(cudaGetLastError());
+    }
 }
 
 }  // namespace bb

@@ -359,8 +359,11 @@ int32_t beat_b200_adjoint(beat_b200_ctx *ctx, double k_signed, int32_t M, const 
  * assembly (regular and Duffy element pairs, identity), the far field and,
  * with an admittance, its Neumann term.  q is the Neumann data (F x R) of the
  * last solve, which the shape derivative needs besides p; w_out and ga_out
- * are as in beat_b200_adjoint and may be NULL.  Symmetry images are not
- * supported (BEAT_B200_STATE).  No counterpart in the reference. */
+ * are as in beat_b200_adjoint and may be NULL.  With symmetry images the
+ * image passes, touching image pairs and image far-field sources are
+ * differentiated too; in the x and xy modes a vertex on a symmetry plane must
+ * stay on it, so the component of its gradient normal to that plane is zero.
+ * No counterpart in the reference. */
 int32_t beat_b200_adjoint_shape(beat_b200_ctx *ctx, double k_signed, int32_t M, const double *dirs,
                                 int32_t R, const double *p, const double *q, const double *g,
                                 const beat_b200_opts *opts, double *w_out, double *ga_out,

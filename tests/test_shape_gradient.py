@@ -93,14 +93,86 @@ def test_mixed_form_agrees_with_fp64(problem):
     assert np.abs(g32 - g64).max() <= 1e-5 * np.abs(g64).max()
 
 
-def test_symmetry_is_refused():
-    m = M.uv_sphere_patch(0.1, 6, 6, -np.pi / 2, np.pi / 2)
-    dirs = M.fibonacci_sphere(5, 1.0)
-    q = np.ones((m.num_faces, 1), complex)
+def _symmetric_problem(mode, seed):
+    """A fundamental-domain mesh of the given symmetry (x >= 0, x, y >= 0 or
+    y >= 0 sphere patches), its vertices perturbed off the sphere while those
+    on a symmetry plane stay on it, with seeded data."""
+    patch = {"x": (-np.pi / 2, np.pi / 2, 8), "xy": (0.0, np.pi / 2, 4), "ground": (0.0, np.pi, 8)}[mode]
+    m = M.uv_sphere_patch(0.1, 6, patch[2], patch[0], patch[1])
+    rng = np.random.default_rng(seed)
+    v = np.asarray(m.vertices) * (1.0 + 0.02 * rng.standard_normal((m.num_vertices, 1)))
+    planes = {"x": (0,), "xy": (0, 1), "ground": (1,)}[mode]
+    for ax in planes:
+        v[np.asarray(m.vertices)[:, ax] == 0.0, ax] = 0.0
+    mesh = M.BoundaryMesh(v, np.asarray(m.faces), np.asarray(m.physical_tags))
+    F, R = mesh.num_faces, 2
+    dirs = M.fibonacci_sphere(7, 1.0)
+    q0 = rng.standard_normal((F, R)) + 1j * rng.standard_normal((F, R))
+    a = 0.3 * (rng.standard_normal(F) + 1j * rng.standard_normal(F))
+    t = rng.standard_normal((dirs.shape[0], R)) + 1j * rng.standard_normal((dirs.shape[0], R))
+    return mesh, planes, q0, a, t, dirs
+
+
+def _gpu_objective(c, verts, faces, q0, a, t, dirs, with_admittance):
+    c.set_mesh(verts, faces, 4, 4)  # the context's symmetry mode applies
+    if with_admittance:
+        c.set_admittance(a)
+    p, _ = c.solve(K, 1.0 / K, q0, _lib.Context.opts(_lib.FP64, flags=_lib.FLAG_RHS_CACHED))
+    return float(np.sum(np.abs(c.farfield(K, dirs, p, q0) - t) ** 2))
+
+
+@pytest.mark.parametrize("mode,with_admittance", [("x", False), ("x", True), ("xy", False), ("ground", False)])
+def test_symmetry_images_gradient_matches_central_differences(mode, with_admittance):
+    """With symmetry images the vertex gradient and the Neumann-data gradient
+    match central differences (h = 1e-6) of the FP64 forward model with the
+    same images (the GPU's, whose images are pinned to mirrored full meshes
+    and to the oracle by the symmetry tests), within 1e-6 of the largest
+    entry.  In the x and xy modes a vertex on a symmetry plane stays on it, so
+    its gradient's component normal to the plane is zero.  The ground mode has
+    no such constraint (as in the reference, its plane has no orbit weights);
+    there the hemisphere rests on the plane, so its touching image pairs are
+    exercised, and moving a vertex off the plane would end that contact, so
+    the differences move plane vertices within the plane only."""
+    mesh, planes, q0, a, t, dirs = _symmetric_problem(mode, 11)
+    faces = np.asarray(mesh.faces)
+    v0 = np.asarray(mesh.vertices)
     with _lib.Context(0) as c:
-        c.set_mesh(m.vertices, m.faces, 4, 4)
-        c.set_symmetry("x")
-        p, _ = c.solve(K, 1.0 / K, q, _lib.Context.opts(_lib.FP64, flags=_lib.FLAG_RHS_CACHED))
-        with pytest.raises(_lib.BeatB200Error) as e:
-            c.adjoint_shape(K, dirs, p, q, np.ones((dirs.shape[0], 1), complex))
-        assert e.value.status == _lib.STATE
+        c.set_mesh(v0, faces, 4, 4)
+        c.set_symmetry(mode)
+        if with_admittance:
+            c.set_admittance(a)
+        opts = _lib.Context.opts(_lib.FP64, flags=_lib.FLAG_RHS_CACHED)
+        p, _ = c.solve(K, 1.0 / K, q0, opts)
+        g = c.farfield(K, dirs, p, q0) - t
+        w, _, gx = c.adjoint_shape(K, dirs, p, q0, g, opts)
+        on_plane = np.zeros(v0.shape, dtype=bool)
+        for ax in planes:
+            on_plane[v0[:, ax] == 0.0, ax] = True
+        assert on_plane.any()
+        if mode != "ground":
+            assert np.all(gx[on_plane] == 0.0)
+        scale = np.abs(gx).max()
+        rng = np.random.default_rng(5)
+        free = np.argwhere(~on_plane)
+        # plane vertices (in-plane components) and others
+        plane_rows = np.argwhere(on_plane.any(axis=1)[:, None] & ~on_plane)
+        picks = [tuple(free[i]) for i in rng.choice(len(free), 8, replace=False)]
+        picks += [tuple(plane_rows[i]) for i in rng.choice(len(plane_rows), 4, replace=False)]
+        for v, d in picks:
+            js = []
+            for sgn in (1.0, -1.0):
+                vv = v0.copy()
+                vv[v, d] += sgn * H
+                js.append(_gpu_objective(c, vv, faces, q0, a, t, dirs, with_admittance))
+            fd = (js[0] - js[1]) / (2 * H)
+            assert abs(fd - gx[v, d]) <= 1e-6 * scale, (mode, v, d, fd, gx[v, d], scale)
+        # the Neumann-data gradient: dJ = 2 Re sum conj(w) dq0 along a seeded
+        # direction; J is quadratic in q0, so a central difference is exact at
+        # any step, and a step of 1e-3 keeps J's rounding out of it
+        dq = rng.standard_normal(q0.shape) + 1j * rng.standard_normal(q0.shape)
+        hq = 1e-3
+        jp = _gpu_objective(c, v0, faces, q0 + hq * dq, a, t, dirs, with_admittance)
+        jm = _gpu_objective(c, v0, faces, q0 - hq * dq, a, t, dirs, with_admittance)
+        fdq = (jp - jm) / (2 * hq)
+        dj = 2.0 * np.real(np.sum(np.conj(w) * dq))
+        assert abs(fdq - dj) <= 1e-6 * abs(dj), (mode, fdq, dj)
