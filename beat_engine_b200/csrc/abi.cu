@@ -71,11 +71,6 @@ static int rhs_request(const beat_b200_opts &o) {
     return BEAT_B200_RHS_AUTO;
 }
 
-__global__ void f32_to_f64_copy(const float2 *src, double2 *dst, size_t n) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) dst[i] = make_double2(src[i].x, src[i].y);
-}
-
 // row-major (ld) -> column-major N x N FP64
 template <typename T>
 __global__ void export_matrix_kernel(const Cx<T> *A, int64_t ld, int n, double2 *out) {
