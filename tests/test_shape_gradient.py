@@ -176,3 +176,23 @@ def test_symmetry_images_gradient_matches_central_differences(mode, with_admitta
         fdq = (jp - jm) / (2 * hq)
         dj = 2.0 * np.real(np.sum(np.conj(w) * dq))
         assert abs(fdq - dj) <= 1e-6 * abs(dj), (mode, fdq, dj)
+
+
+@pytest.mark.parametrize("mode", ["x", "xy"])
+def test_symmetry_images_mixed_form_agrees_with_fp64(mode):
+    """With symmetry images, the mixed form's gradients (adjoint solve on the
+    FP32 factors with FP64 refinement) agree with the FP64 form's within
+    1e-5 of the largest entry."""
+    mesh, _, q0, _, t, dirs = _symmetric_problem(mode, 12)
+    out = {}
+    for precision in (_lib.FP64, _lib.MIXED_FP32_IR):
+        with _lib.Context(0) as c:
+            c.set_mesh(mesh.vertices, mesh.faces, 4, 4)
+            c.set_symmetry(mode)
+            opts = _lib.Context.opts(precision, flags=_lib.FLAG_RHS_CACHED)
+            p, _ = c.solve(K, 1.0 / K, q0, opts)
+            g = c.farfield(K, dirs, p, q0) - t
+            out[precision] = c.adjoint_shape(K, dirs, p, q0, g, opts)
+    (w64, _, gx64), (w32, _, gx32) = out[_lib.FP64], out[_lib.MIXED_FP32_IR]
+    assert np.abs(gx32 - gx64).max() <= 1e-5 * np.abs(gx64).max()
+    assert np.abs(w32 - w64).max() <= 1e-5 * np.abs(w64).max()
