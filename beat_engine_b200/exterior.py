@@ -109,19 +109,43 @@ def evaluate_far_field_b200(directions, mesh: BoundaryMesh, pressure, q, wavenum
     return out[:, 0] if np.asarray(pressure).ndim == 1 else out
 
 
+def rigid_translation_axis(motion_axis, symmetry_mode: str = "off") -> np.ndarray:
+    """The unit direction of a rigid-translation source, checked as the
+    reference checks it (``prescribed_motion_axis``,
+    ``BeatEngineCompiledDriver.jl:728-770``): three finite numbers, not all
+    zero, scaled by the largest magnitude and then normalised (an axis gives a
+    direction, not a speed), and lying in every active symmetry plane (x: no x
+    component; xy: no x or y component) to 1e-8.  Violations raise
+    ``ValueError`` with the reference's messages."""
+    raw = list(motion_axis) if isinstance(motion_axis, (list, tuple, np.ndarray)) else None
+    if raw is None or len(raw) != 3:
+        raise ValueError("Rigid-translation source requires a three-component motion_axis.")
+    if not all(isinstance(v, (int, float, np.integer, np.floating)) and not isinstance(v, (bool, np.bool_))
+               and np.isfinite(v) for v in raw):
+        raise ValueError("Rigid-translation source motion_axis must contain three finite numbers.")
+    ax = np.asarray(raw, dtype=np.float64)
+    scale = float(np.max(np.abs(ax)))
+    if not scale > 0.0:
+        raise ValueError("Rigid-translation source motion_axis must be finite and nonzero.")
+    ax = ax / scale
+    ax = ax / np.linalg.norm(ax)
+    planes = {"x": (0,), "xy": (0, 1)}.get(str(symmetry_mode).lower(), ())
+    if any(abs(ax[c]) > 1e-8 for c in planes):
+        raise ValueError("Rigid-translation source motion_axis must lie in the physical symmetry planes.")
+    return ax
+
+
 def exterior_neumann(mesh: BoundaryMesh, tags, amplitudes, density: float, omega: float,
-                     phasor_convention: str = NEGATIVE_TIME_PHASOR, motion_axis=None):
+                     phasor_convention: str = NEGATIVE_TIME_PHASOR, motion_axis=None, symmetry_mode: str = "off"):
     """Per-face Neumann data ``q_f = neumann_scale(rho, omega) * amplitude``
     on faces carrying one of ``tags`` (times ``n_f . axis`` for a rigid
-    translation), zero elsewhere."""
+    translation, the axis checked and normalised by
+    :func:`rigid_translation_axis`), zero elsewhere."""
     values = np.zeros(mesh.num_faces, dtype=np.complex128)
     scale = neumann_scale(density, omega, phasor_convention)
     factor = np.ones(mesh.num_faces)
     if motion_axis is not None:
-        ax = np.asarray(motion_axis, dtype=np.float64)
-        ax = ax / np.max(np.abs(ax))
-        ax = ax / np.linalg.norm(ax)
-        factor = mesh.normals @ ax
+        factor = mesh.normals @ rigid_translation_axis(motion_axis, symmetry_mode)
     for tag, amp in zip(tags, amplitudes):
         sel = mesh.physical_tags == tag
         values[sel] = scale * amp * factor[sel]
