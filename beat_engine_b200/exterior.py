@@ -52,6 +52,35 @@ class ExteriorB200Cache:
         self.ctx.close()
 
 
+def exterior_assembly_selection(options: dict) -> dict:
+    """The solver-option checks of ``solve_exterior_request``
+    (``BeatEngineCompiledDriver.jl:1055-1076``) with ``b200_direct`` added to
+    the allowed ``burton_miller_assembly`` values: ``precision`` float32 or
+    float64 (default float32), ``bem_backend`` cpu / cuda / rocm / metal
+    (default cpu), ``burton_miller_assembly`` direct_system / operator_matrices
+    / b200_direct (default direct_system), all case-insensitive.  This path
+    runs when the backend is cuda and the assembly b200_direct; b200_direct on
+    another backend is refused.  Violations raise ``ValueError`` with the
+    reference's messages (the assembly one lists the new value).  Returns the
+    normalised choices, ``b200_assembly`` and, when it is set, the precision
+    form of ``b200_precision``."""
+    precision_name = str(options.get("precision", "float32")).lower()
+    if precision_name not in ("float32", "float64"):
+        raise ValueError("Exterior precision must be float32 or float64.")
+    backend = str(options.get("bem_backend", "cpu")).lower()
+    if backend not in ("cpu", "cuda", "rocm", "metal"):
+        raise ValueError("Exterior BEM backend must be cpu, cuda, rocm, or metal.")
+    requested = str(options.get("burton_miller_assembly", "direct_system")).lower()
+    if requested not in ("direct_system", "operator_matrices", BURTON_MILLER_ASSEMBLY):
+        raise ValueError("Exterior burton_miller_assembly must be direct_system, operator_matrices, or "
+                         f"{BURTON_MILLER_ASSEMBLY}.")
+    b200 = requested == BURTON_MILLER_ASSEMBLY
+    if b200 and backend != "cuda":
+        raise ValueError(f"Exterior burton_miller_assembly = {BURTON_MILLER_ASSEMBLY} needs bem_backend = cuda.")
+    return {"precision": precision_name, "bem_backend": backend, "burton_miller_assembly": requested,
+            "b200_assembly": b200, "b200_precision": solver_options_precision(options) if b200 else None}
+
+
 def solver_options_precision(options: dict) -> int:
     """``b200_precision`` solver option -> precision form (default mixed)."""
     name = str(options.get("b200_precision", "mixed_fp32_ir")).lower()

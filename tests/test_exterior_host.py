@@ -4,7 +4,9 @@ Neumann data of tag-driven and explicit-velocity excitations
 (``exterior_neumann``, BeatEngineCompiledDriver.jl:825-839), the
 rigid-translation axis and its checks (``prescribed_motion_axis``,
 BeatEngineCompiledDriver.jl:728-770; ``exterior_motion_factor``,
-compiled_ground_contract.jl:47-50), and the ``b200_precision`` solver option.
+compiled_ground_contract.jl:47-50), the ``b200_precision`` solver option, and
+the solver-option checks that select this path
+(BeatEngineCompiledDriver.jl:1055-1076 with ``b200_direct`` added).
 """
 import numpy as np
 import pytest
@@ -88,3 +90,31 @@ def test_explicit_velocity_neumann():
     assert np.allclose(E.bem_normal_velocity_neumann(v, rho, omega), neumann_scale(rho, omega) * v)
     assert np.allclose(E.bem_normal_velocity_neumann(v, rho, omega, POSITIVE_TIME_PHASOR),
                        neumann_scale(rho, omega, POSITIVE_TIME_PHASOR) * v)
+
+
+def test_assembly_selection():
+    sel = E.exterior_assembly_selection({"bem_backend": "CUDA", "burton_miller_assembly": "B200_direct"})
+    assert sel["b200_assembly"] and sel["b200_precision"] == _lib.MIXED_FP32_IR
+    assert sel["precision"] == "float32" and sel["bem_backend"] == "cuda"
+    sel = E.exterior_assembly_selection({"bem_backend": "cuda", "burton_miller_assembly": "b200_direct",
+                                         "b200_precision": "float64", "precision": "float64"})
+    assert sel["b200_assembly"] and sel["b200_precision"] == _lib.FP64
+    # the reference's own values keep their paths
+    for assembly in ("direct_system", "operator_matrices"):
+        for backend in ("cpu", "cuda", "rocm", "metal"):
+            sel = E.exterior_assembly_selection({"bem_backend": backend, "burton_miller_assembly": assembly})
+            assert not sel["b200_assembly"] and sel["b200_precision"] is None
+    assert E.exterior_assembly_selection({})["burton_miller_assembly"] == "direct_system"
+
+
+@pytest.mark.parametrize("options,message", [
+    ({"precision": "float16"}, "precision must be float32 or float64"),
+    ({"bem_backend": "opencl"}, "backend must be cpu, cuda, rocm, or metal"),
+    ({"burton_miller_assembly": "hmatrix"}, "must be direct_system, operator_matrices, or b200_direct"),
+    ({"burton_miller_assembly": "b200_direct"}, "needs bem_backend = cuda"),
+    ({"burton_miller_assembly": "b200_direct", "bem_backend": "metal"}, "needs bem_backend = cuda"),
+    ({"burton_miller_assembly": "b200_direct", "bem_backend": "cuda", "b200_precision": "bf16"}, "b200_precision"),
+])
+def test_assembly_selection_rejects(options, message):
+    with pytest.raises(ValueError, match=message):
+        E.exterior_assembly_selection(options)
