@@ -38,6 +38,20 @@ EXPORTS = (
 SYMMETRY_MODES = {"off": 0, "x": 1, "xy": 2, "ground": 3}
 
 
+def symmetry_mode(mode) -> int:
+    """A symmetry mode name, trimmed and case-insensitive as the reference
+    normalises it (``normalized_symmetry_mode``, src/BeatEngineCore.jl:448-454),
+    or its number 0..3, as the C ABI's mode number.  An unknown name raises
+    ``ValueError`` with the reference's message; numbers are checked by the
+    library."""
+    if isinstance(mode, str):
+        key = mode.strip().lower()
+        if key not in SYMMETRY_MODES:
+            raise ValueError(f"Unsupported image mode: {mode}. Expected off, x, xy, or ground.")
+        return SYMMETRY_MODES[key]
+    return int(mode)
+
+
 class Opts(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("ir_restart", ctypes.c_int32), ("ir_max_iters", ctypes.c_int32),
                 ("lu_split_terms", ctypes.c_int32), ("ir_rtol", ctypes.c_double), ("lu_block", ctypes.c_int32),
@@ -365,8 +379,7 @@ class Context:
 
     def set_symmetry(self, mode):
         """Symmetry images: "off", "x", "xy" or "ground" (or 0..3)."""
-        m = SYMMETRY_MODES[mode] if isinstance(mode, str) else int(mode)
-        self._check(self.lib.beat_b200_set_symmetry(self.handle, m))
+        self._check(self.lib.beat_b200_set_symmetry(self.handle, symmetry_mode(mode)))
 
     def set_admittance(self, a=None):
         """Per-face admittance coefficients a (F complex): later solves use

@@ -118,3 +118,10 @@ def test_assembly_selection():
 def test_assembly_selection_rejects(options, message):
     with pytest.raises(ValueError, match=message):
         E.exterior_assembly_selection(options)
+
+
+def test_symmetry_mode_names():
+    assert _lib.symmetry_mode(" XY ") == 2 and _lib.symmetry_mode("Ground") == 3 and _lib.symmetry_mode("off") == 0
+    assert _lib.symmetry_mode(1) == 1
+    with pytest.raises(ValueError, match="Unsupported image mode: yz. Expected off, x, xy, or ground."):
+        _lib.symmetry_mode("yz")
