@@ -488,8 +488,9 @@ void set_mesh(beat_b200_ctx *c, int V, const double *verts, int F, const int32_t
     upload(c->d_curls, curls);
     upload(c->d_qpts, qpts);
 
-    // touching pairs, grouped by test element, trial candidates in the
-    // vertex -> element order of adjacent_trial_indices_by_test
+    // touching pairs, found per test element with the trial candidates in the
+    // vertex -> element order of adjacent_trial_indices_by_test (reordered by
+    // rule size once the rules are built, below)
     std::vector<int> vstart(V + 1, 0), vlist(3 * (size_t)F), fill(V, 0);
     for (int f = 0; f < F; ++f)
         for (int a = 0; a < 3; ++a) vstart[c->faces[3 * f + a] + 1]++;
@@ -632,12 +633,6 @@ void set_mesh(beat_b200_ctx *c, int V, const double *verts, int F, const int32_t
         }
     }
     c->nimg_pairs = (int64_t)ip_t.size();
-    upload(c->ip_test, ip_t);
-    upload(c->ip_trial, ip_s);
-    upload(c->ip_rule, ip_r);
-    upload(c->ip_img, ip_x);
-    upload(c->ip_jac, ip_j);
-    upload(c->ip_nn, ip_n);
     c->nrules = (int)keys.size();
     std::vector<DuffyPt> base[4];
     for (int k = 1; k <= 3; ++k) base[k] = duffy(sing_order, k);
@@ -653,6 +648,39 @@ void set_mesh(beat_b200_ctx *c, int V, const double *verts, int F, const int32_t
         }
         rstart.push_back(rstart.back() + (int)b.size());
     }
+    // Pairs in increasing order of their rule's point count (vertex, edge,
+    // coincident at the same order), stably: the Duffy kernels give each pair
+    // one warp, and a CTA's warps then hold pairs of one size and finish
+    // together instead of idling beside its longest pair.  Increasing, so that
+    // the mixed form's FP32 entries take their small vertex- and edge-pair
+    // terms before the large self terms.
+    auto by_rule_size = [&](std::vector<int> &t, std::vector<int> &s, std::vector<int> &r, std::vector<double> &j,
+                            std::vector<double> &n, std::vector<int> *x) {
+        std::vector<size_t> order(t.size());
+        std::iota(order.begin(), order.end(), size_t(0));
+        std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+            return rstart[r[a] + 1] - rstart[r[a]] < rstart[r[b] + 1] - rstart[r[b]];
+        });
+        auto apply = [&](auto &v) {
+            auto w = v;
+            for (size_t i = 0; i < order.size(); ++i) w[i] = v[order[i]];
+            v.swap(w);
+        };
+        apply(t);
+        apply(s);
+        apply(r);
+        apply(j);
+        apply(n);
+        if (x) apply(*x);
+    };
+    by_rule_size(sp_t, sp_s, sp_r, sp_j, sp_n, nullptr);
+    by_rule_size(ip_t, ip_s, ip_r, ip_j, ip_n, &ip_x);
+    upload(c->ip_test, ip_t);
+    upload(c->ip_trial, ip_s);
+    upload(c->ip_rule, ip_r);
+    upload(c->ip_img, ip_x);
+    upload(c->ip_jac, ip_j);
+    upload(c->ip_nn, ip_n);
     upload(c->sp_test, sp_t);
     upload(c->sp_trial, sp_s);
     upload(c->sp_rule, sp_r);
